@@ -1,0 +1,143 @@
+"""Recipe that builds the reference oracle ``oracle/_ref/<grid>/libsimson_ref.so``.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/f77c.py``).  The product never loads it.
+
+It reads the reference's Fortran sources where they lie (``$SIMSON_REFERENCE``,
+default the read-only reference checkout), edits only the compile-time grid
+in ``par.f`` exactly as the reference's own instructions say to do per case
+(nx, ny, nz, nthread, pressure=0), translates the hot-path units to C with
+``oracle/f77c.py`` and compiles them, together with ``oracle/ref_harness.c``,
+with ``gcc -O3 -fopenmp``.  Nothing derived from the reference is written
+outside ``oracle/_ref/`` (git-ignored).
+
+Translated units (reference file: what it contributes):
+  bla/bla.f         declarations of the driver state + these statement ranges:
+                    849 rkcoeff call, 1080-1082 preprbl call, 1466-1478 first-step
+                    RK factors, 1562-1569 prhs call, 1622-1662 channel px/mflux init,
+                    1796-1797 substep time, 1819-1826 box shift, 2251-2288 the
+                    nonlinbl plane loop (OpenMP), 2349-2351 wcflbl, 2384-2397 RK
+                    weights, 2433-2475 the linearbl plane loop (OpenMP), 2598 it=it+1
+  bla/nonlinbl.f advection.f boxcfl.f fft2db.f fft2df.f getxz.f putxz.f   (step 2)
+  bla/linearbl.f getxy.f putxy.f setmacrhs.f trid.f dcheb.f evald.f evalbc.f
+                 solvbc.f                                                  (step 3)
+  bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
+Everything else those units call (LES filters, forcing, MPI, timers, ...) is
+emitted as a stub that aborts if reached; the timers ``ctim``/``wall_time``
+are no-ops.  The channel configuration never reaches a stub.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from f77c import translate  # noqa: E402
+
+REF_ROOT = os.environ.get("SIMSON_REFERENCE", "/root/reference")
+REF_BLA = os.path.join(REF_ROOT, "bla")
+OUT_ROOT = os.path.join(HERE, "_ref")
+
+UNIT_FILES = [
+    "nonlinbl.f", "advection.f", "boxcfl.f", "fft2db.f", "fft2df.f", "getxz.f", "putxz.f",
+    "linearbl.f", "getxy.f", "putxy.f", "setmacrhs.f", "trid.f", "dcheb.f", "evald.f",
+    "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f",
+]
+
+MAIN_RANGES = [
+    ("bla_rkcoeff", 849, 849),
+    ("bla_preprbl", 1080, 1082),
+    ("bla_firststep", 1466, 1478),
+    ("bla_prhs", 1562, 1569),
+    ("bla_pxinit", 1622, 1662),
+    ("bla_substep_time", 1796, 1797),
+    ("bla_boxshift", 1819, 1826),
+    ("bla_nonlin", 2251, 2288),
+    ("bla_cfl", 2349, 2351),
+    ("bla_rkweights", 2384, 2397),
+    ("bla_linear", 2433, 2475),
+    ("bla_itinc", 2598, 2598),
+]
+
+NOOP_STUBS = ("ctim", "wall_time", "fft_identify")
+NTHREAD = 64  # compile-time thread slots (par.f nthread); the harness never runs more
+
+
+def par_text(nx: int, ny: int, nz: int, nthread: int = NTHREAD) -> str:
+    with open(os.path.join(REF_BLA, "par.f")) as f:
+        txt = f.read()
+    txt, n1 = re.subn(r"parameter \(nx=\d+,ny=\d+,nz=\d+\)",
+                      f"parameter (nx={nx},ny={ny},nz={nz})", txt)
+    txt, n2 = re.subn(r"parameter \(nthread=\d+\)", f"parameter (nthread={nthread})", txt)
+    txt, n3 = re.subn(r"parameter \(pressure=\d\)", "parameter (pressure=0)", txt)
+    if (n1, n2, n3) != (1, 1, 1):
+        raise RuntimeError("par.f layout not recognised")
+    return txt
+
+
+def generate_c(nx: int, ny: int, nz: int) -> str:
+    sources = []
+    for fn in UNIT_FILES:
+        with open(os.path.join(REF_BLA, fn)) as f:
+            sources.append((fn, f.read()))
+    with open(os.path.join(REF_BLA, "bla.f")) as f:
+        sources.append(("bla.f", f.read()))
+    return translate(sources, par_text(nx, ny, nz), defines={"OPENMP"},
+                     main_ranges=MAIN_RANGES, stubs_noop=NOOP_STUBS,
+                     skip_units=("fft_identify",), provided=("stopnow",))
+
+
+def lib_path(nx: int, ny: int, nz: int) -> str:
+    return os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}", "libsimson_ref.so")
+
+
+def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False) -> str:
+    """Translate + compile the reference for one grid; returns the .so path."""
+    out_dir = os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}")
+    so = os.path.join(out_dir, "libsimson_ref.so")
+    harness = os.path.join(HERE, "ref_harness.c")
+    translator = os.path.join(HERE, "f77c.py")
+    stamp = hashlib.sha256()
+    for p in (harness, translator, __file__):
+        with open(p, "rb") as f:
+            stamp.update(f.read())
+    stamp = stamp.hexdigest()[:16]
+    stamp_file = os.path.join(out_dir, "stamp")
+    if not force and os.path.exists(so) and os.path.exists(stamp_file):
+        with open(stamp_file) as f:
+            if f.read().strip() == stamp:
+                return so
+    if not os.path.isdir(REF_BLA):
+        if os.path.exists(so):
+            return so
+        raise FileNotFoundError(f"reference sources not found at {REF_BLA} and no prebuilt {so}")
+    os.makedirs(out_dir, exist_ok=True)
+    csrc = generate_c(nx, ny, nz)
+    gen = os.path.join(out_dir, "ref_gen.c")
+    with open(gen, "w") as f:
+        f.write(csrc)
+    cmd = ["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", "-w", "-std=gnu11",
+           "-fno-fast-math", "-ffp-contract=off", "-I", out_dir,
+           "-o", so + ".tmp", harness, "-lm"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(so + ".tmp", so)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    return so
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("grid", nargs="*", default=["48x65x48"], help="NXxNYxNZ")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    for g in a.grid:
+        nx, ny, nz = (int(v) for v in g.split("x"))
+        print(build(nx, ny, nz, force=a.force, verbose=True))

@@ -1,0 +1,136 @@
+/* Harness around the translated reference (oracle/_ref/<grid>/ref_gen.c).
+ *
+ * TEST INFRASTRUCTURE ONLY: loaded by tests/, bench.py's CPU-baseline arm and
+ * __graft_entry__.smoke() as the checker, never by the product.
+ *
+ * It plays the part of the reference driver bla/bla.f for the temporal channel
+ * (fltype=1, nst=3 RK3/CN, fixed dt, ibc=0, tau method, constant mass flux,
+ * no LES, no scalar, nproc=1): it sets the bla.i-level scalars that the
+ * channel case uses, then runs the translated statement ranges of bla.f in the
+ * order the reference time loop does (bla/bla.f:1790-2610).  The translated
+ * ranges are the reference's own statements; only the glue (parameter values,
+ * slot copies, the full-step time update bla/bla.f:2600-2607) is written here.
+ */
+#include "ref_gen.c"
+
+#include <string.h>
+
+void f77_stop(int code) {
+  fprintf(stderr, "oracle: reference STOP %d\n", code);
+  abort();
+}
+
+void f_stopnow(int *code) {
+  fprintf(stderr, "oracle: reference stopnow(%d)\n", *code);
+  abort();
+}
+
+static int sref_threads = 1;
+
+/* dims[0..11] = nx ny nz nxp nyp nzp memnx memny memnz memnxyz nthread nby */
+void sref_dims(int *dims) {
+  dims[0] = v_nx; dims[1] = v_ny; dims[2] = v_nz;
+  dims[3] = v_nxp; dims[4] = v_nyp; dims[5] = v_nzp;
+  dims[6] = v_memnx; dims[7] = v_memny; dims[8] = v_memnz; dims[9] = v_memnxyz;
+  dims[10] = v_nthread; dims[11] = v_nby;
+}
+
+/* Sets up the channel case; mirrors what rparambl/bla.f would leave in place
+ * for a bla.i with: fltype=1, nst=3, fixed dt, ibc=0, cim=.false., cflux,
+ * icfl=nst, iamp=iext=ixys=0 (disabled), iles=0, rot=0. */
+int sref_setup(double re, double xl, double zl, double dt, int cflux, int icfl, int nthreads) {
+  static int allocated = 0;
+  if (allocated) f77_main_free();
+  f77_main_alloc();
+  allocated = 1;
+  sref_threads = nthreads < 1 ? 1 : (nthreads > v_nthread ? v_nthread : nthreads);
+#ifdef _OPENMP
+  omp_set_num_threads(sref_threads);
+#endif
+  v_re = re; v_xl = xl; v_zl = zl;
+  v_dtn = dt; v_dtmax = 1.0e30; v_vart = 0;
+  v_nst = 3; v_fltype = 1; v_pert = 0; v_lin = 0; v_spat = 0;
+  v_cflux = cflux ? 1 : 0;
+  v_ibc = 0; v_cim = 0; v_icorr = 0;
+  v_icfl = icfl; v_iamp = -1000000; v_iext = -1000000; v_ixys = -1000000;
+  v_iles = 0; v_isfd = 0; v_imhd = 0; v_wbci = 0; v_loctyp = 0; v_tripf = 0;
+  v_osmod = 0; v_streak = 0; v_bf3 = 0; v_do_press_nl = 0; v_do_press = 0;
+  v_rot = 0.0; v_dstar = 1.0; v_my_node = 0;
+  v_u0low = 0.0; v_u0upp = 0.0; v_w0low = 0.0; v_w0upp = 0.0; v_du0upp = 0.0;
+  v_vsuc = 0.0; v_x0 = 0.0; v_cdev = 0.0; v_xs = 0.0; v_zs = 0.0; v_t = 0.0;
+  bla_rkcoeff();
+  bla_preprbl();
+  bla_firststep();
+  return 0;
+}
+
+static long slot_size(void) { return (long)v_memnx * v_memny * v_memnz; }
+
+void sref_set_slot(int slot, const double *re_part, const double *im_part) {
+  long n = slot_size();
+  memcpy(v_ur + (long)(slot - 1) * n, re_part, n * sizeof(double));
+  memcpy(v_ui + (long)(slot - 1) * n, im_part, n * sizeof(double));
+}
+
+void sref_get_slot(int slot, double *re_part, double *im_part) {
+  long n = slot_size();
+  memcpy(re_part, v_ur + (long)(slot - 1) * n, n * sizeof(double));
+  memcpy(im_part, v_ui + (long)(slot - 1) * n, n * sizeof(double));
+}
+
+/* Startup: partial right-hand side from the velocities (bla/bla.f:1562) and
+ * the channel pressure-gradient / mass-flux initialisation (:1622-1662). */
+void sref_start(void) {
+#ifdef _OPENMP
+  omp_set_num_threads(sref_threads);
+#endif
+  bla_prhs();
+  bla_pxinit();
+  v_it = 1;
+}
+
+/* One RK substep: step 2 (nonlinbl over xz-planes), CFL, RK weights, step 3
+ * (linearbl over xy-planes), iteration counter and full-step time update. */
+void sref_substep(void) {
+#ifdef _OPENMP
+  omp_set_num_threads(sref_threads);
+#endif
+  bla_substep_time();
+  bla_boxshift();
+  bla_nonlin();
+  bla_cfl();
+  bla_rkweights();
+  bla_linear();
+  bla_itinc();
+  if ((v_it - 1) % v_nst == 0) v_t = v_t + v_dtn;
+}
+
+/* Only step 2 or only step 3 (for per-kernel parity tests). */
+void sref_nonlin_only(void) {
+  bla_substep_time();
+  bla_boxshift();
+  bla_nonlin();
+}
+void sref_linear_only(void) {
+  bla_cfl();
+  bla_rkweights();
+  bla_linear();
+  bla_itinc();
+  if ((v_it - 1) % v_nst == 0) v_t = v_t + v_dtn;
+}
+
+/* scalars: 0 px, 1 mflux, 2 t, 3 cfl, 4 an, 5 bn, 6 anp1, 7 bnp1, 8 cnp1, 9 it, 10 tc, 11 dtn */
+void sref_scalars(double *s) {
+  s[0] = v_px; s[1] = v_mflux; s[2] = v_t; s[3] = v_cfl;
+  s[4] = v_an; s[5] = v_bn; s[6] = v_anp1; s[7] = v_bnp1; s[8] = v_cnp1;
+  s[9] = v_it; s[10] = v_tc; s[11] = v_dtn;
+}
+
+/* partial RHS of the mean flow, puw(ny, 2) */
+void sref_get_puw(double *p) { memcpy(p, v_puw, (size_t)v_ny * 2 * sizeof(double)); }
+
+/* Gauss-Lobatto points and integration weights from preprbl. */
+void sref_grid(double *eta, double *wint) {
+  memcpy(eta, v_eta, (size_t)v_nyp * sizeof(double));
+  memcpy(wint, v_wint, (size_t)v_nyp * sizeof(double));
+}

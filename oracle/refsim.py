@@ -1,0 +1,108 @@
+"""ctypes wrapper around the translated reference ``bla`` (oracle/_ref).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, bench.py's CPU-baseline arm and
+``__graft_entry__.smoke()`` as the checker; never by the product path.
+
+Field layout at this interface is the reference's main storage,
+``ur(memnx, memny, memnz, slot)`` (bla/par.f:111-120), seen from numpy as a
+complex array of shape ``(nz, nyp, nx//2)`` per slot (kx fastest).  Slots:
+1-3 u, v, w (Fourier x/z, physical y); 4-5 omega_x, omega_z; 6-7 the partial
+right-hand sides p_v, p_omega_y (Chebyshev y).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _lib(nx, ny, nz, build=True):
+    import sys
+    sys.path.insert(0, HERE)
+    from build_ref import build as _build, lib_path
+    path = _build(nx, ny, nz) if build else lib_path(nx, ny, nz)
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    lib = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.sref_setup.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int] * 3
+    lib.sref_set_slot.argtypes = [ctypes.c_int, dp, dp]
+    lib.sref_get_slot.argtypes = [ctypes.c_int, dp, dp]
+    lib.sref_scalars.argtypes = [dp]
+    lib.sref_get_puw.argtypes = [dp]
+    lib.sref_grid.argtypes = [dp, dp]
+    lib.sref_dims.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class RefSim:
+    """The reference channel time stepper (temporal channel, RK3/CN, cflux)."""
+
+    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True):
+        self.lib = _lib(nx, ny, nz, build)
+        dims = (ctypes.c_int * 12)()
+        self.lib.sref_dims(dims)
+        self.dims = list(dims)
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nyp = self.dims[4]
+        self.lib.sref_setup(re, xl, zl, dt, int(cflux), int(icfl), int(threads))
+        self.shape = (nz, self.nyp, nx // 2)
+
+    def set_slot(self, slot, field):
+        f = np.ascontiguousarray(field, dtype=np.complex128).reshape(self.shape)
+        re_ = np.ascontiguousarray(f.real)
+        im_ = np.ascontiguousarray(f.imag)
+        self.lib.sref_set_slot(slot, _dp(re_), _dp(im_))
+
+    def get_slot(self, slot):
+        re_ = np.empty(self.shape)
+        im_ = np.empty(self.shape)
+        self.lib.sref_get_slot(slot, _dp(re_), _dp(im_))
+        return re_ + 1j * im_
+
+    def set_velocity(self, u, v, w):
+        for k, f in enumerate((u, v, w), start=1):
+            self.set_slot(k, f)
+
+    def start(self):
+        self.lib.sref_start()
+
+    def substep(self):
+        self.lib.sref_substep()
+
+    def step(self, n=1):
+        for _ in range(3 * n):
+            self.lib.sref_substep()
+
+    def nonlin_only(self):
+        self.lib.sref_nonlin_only()
+
+    def linear_only(self):
+        self.lib.sref_linear_only()
+
+    def scalars(self):
+        s = np.empty(12)
+        self.lib.sref_scalars(_dp(s))
+        keys = ("px", "mflux", "t", "cfl", "an", "bn", "anp1", "bnp1", "cnp1", "it", "tc", "dtn")
+        return dict(zip(keys, s))
+
+    def puw(self):
+        p = np.empty((2, self.ny))
+        self.lib.sref_get_puw(_dp(p))
+        return p
+
+    def grid(self):
+        eta = np.empty(self.nyp)
+        wint = np.empty(self.nyp)
+        self.lib.sref_grid(_dp(eta), _dp(wint))
+        return eta, wint
+
+    def state(self):
+        return [self.get_slot(k) for k in range(1, 8)]

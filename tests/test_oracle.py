@@ -1,0 +1,86 @@
+"""The reference oracle (the reference's own Fortran, translated to C) against
+known answers.  CPU only."""
+import numpy as np
+import pytest
+
+from simson_b200.fields import cc_weights, channel_field, gl_points
+
+
+def test_grid_and_weights(need_ref):
+    need_ref(16, 17, 16)
+    from refsim import RefSim
+    r = RefSim(16, 17, 16, 4200.0, 4 * np.pi, 2 * np.pi, 0.01)
+    eta, wint = r.grid()
+    assert np.array_equal(eta, gl_points(17))
+    np.testing.assert_allclose(wint, cc_weights(17), atol=1e-15)
+    assert abs(wint.sum() - 2.0) < 1e-14
+
+
+def test_laminar_poiseuille_is_fixed_point(need_ref):
+    """U = 1 - y^2 with constant flux is a discrete steady state."""
+    need_ref(16, 17, 16)
+    from refsim import RefSim
+    r = RefSim(16, 17, 16, 4200.0, 4 * np.pi, 2 * np.pi, 0.01)
+    u, v, w = channel_field(16, 17, 16, 4 * np.pi, 2 * np.pi, 0.0, 1)
+    r.set_velocity(u, v, w)
+    r.start()
+    r.step(10)
+    assert np.abs(r.get_slot(1) - u).max() < 1e-12
+    assert np.abs(r.get_slot(2)).max() < 1e-12
+    s = r.scalars()
+    assert abs(s["px"] + 2.0 / 4200.0) < 1e-12
+    assert abs(s["t"] - 0.1) < 1e-12
+
+
+def test_orr_sommerfeld_orszag_1971(need_ref):
+    """A small Tollmien-Schlichting mode grows at Orszag's published rate:
+    Re = 10000, alpha = 1, c = 0.23752649 + 0.00373967 i."""
+    need_ref(4, 65, 4)
+    from os_modes import least_stable_mode
+    from refsim import RefSim
+    n, re, alpha = 64, 10000.0, 1.0
+    c, v, dv = least_stable_mode(n, re, alpha)
+    assert abs(c - (0.23752649 + 0.00373967j)) < 1e-8
+    r = RefSim(4, n + 1, 4, re, 2 * np.pi / alpha, 2 * np.pi, 0.01)
+    eps = 1e-7
+    U = np.zeros((4, n + 1, 2), complex)
+    V = np.zeros_like(U)
+    y = gl_points(n + 1)
+    U[0, :, 0] = 1 - y * y
+    V[0, :, 1] = eps * v
+    U[0, :, 1] = 1j * eps * dv / alpha
+    r.set_velocity(U, V, np.zeros_like(U))
+    r.start()
+    r.step(500)
+    T = r.scalars()["t"]
+    vt = r.get_slot(2)[0, :, 1]
+    ratio = np.vdot(v, vt) / np.vdot(v, v) / eps
+    c_meas = 1j * np.log(ratio) / (alpha * T)
+    assert abs(c_meas.real - 0.23752649) < 2e-8
+    assert abs(c_meas.imag - 0.00373967) < 2e-8
+    pred = eps * v * np.exp(-1j * alpha * c * T)
+    assert np.abs(vt - pred).max() / np.abs(pred).max() < 1e-7
+
+
+def test_seeded_field_is_divergence_free_and_scaled():
+    nx, ny, nz = 16, 17, 16
+    xl, zl = 4 * np.pi, 2 * np.pi
+    u, v, w = channel_field(nx, ny, nz, xl, zl, 0.02, 7, laminar=False)
+    from simson_b200.fields import wavenumbers
+    from os_modes import cheb
+    D, _ = cheb(ny - 1)
+    alfa, beta = wavenumbers(nx, nz, xl, zl)
+    div = 1j * alfa[None, None, :] * u + np.einsum("ij,zjx->zix", D, v) + 1j * beta[:, None, None] * w
+    assert np.abs(div).max() < 1e-12
+    wy = cc_weights(ny)
+    e = 0.0
+    for f in (u, v, w):
+        m = np.abs(f) ** 2
+        m[:, :, 1:] *= 2
+        e += np.einsum("zyx,y->", m, wy) / 2
+    assert abs(np.sqrt(e / 3) - 0.02) < 1e-14
+    for f in (u, v, w):  # no-slip
+        assert np.abs(f[:, 0, :]).max() < 1e-15 and np.abs(f[:, -1, :]).max() < 1e-15
+    # Hermitian kx = 0 column
+    for kz in range(1, 7):
+        assert np.allclose(v[kz, :, 0], np.conj(v[nz - kz, :, 0]))
