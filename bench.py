@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the channel time step: RK3 steps/s at 384x193x384.
+
+Workload (the production-DNS configuration the headline metric is quoted on):
+temporal channel, 384x193x384 modes (3/2-rule grid 576x193x576), box
+2pi x 2 x pi, Re_cl = 9000, constant flow rate, dt = 0.002, seeded
+divergence-free perturbation of rms 0.1 on laminar Poiseuille flow.  One
+"step" is one full RK3 step (three substeps of nonlinear step 2 + implicit
+step 3).  The state (1.6 GB in FP64) is far larger than L2, so no flush is
+needed between steps.
+
+Arms:
+  own (default)   the CUDA step through the C ABI, state resident in HBM;
+                  ``e2e`` repeats it through the same ABI with the whole state
+                  uploaded from pinned host memory and downloaded every step.
+  --impl reference  the reference's own CPU implementation of the step (the
+                  translated Fortran, oracle/_ref) on all host cores, OpenMP.
+
+Multi-GPU: the step runs as independent replicas, one per rank (weak scaling);
+the path is not sharded across GPUs in this build.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(nx=384, ny=193, nz=384, re=9000.0, xl=2 * np.pi, zl=np.pi, dt=0.002, rms=0.1, seed=3)
+METRIC = "RK3 steps/s at 384x193x384"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def substep_bytes(nc, s_bytes):
+    # algorithmic main-storage traffic of one substep: step 2 reads 5 fields and
+    # writes 3, step 3 reads 5 and writes 7 (20 field passes)
+    return 20 * nc * s_bytes
+
+
+def kernel_bytes(name, w):
+    """Algorithmic (compulsory) HBM bytes of one launch of each kernel, FP64."""
+    nx2, ny, nz = w["nx"] // 2, w["ny"], w["nz"]
+    nzp = nz + nz // 2
+    c = 16
+    fld = nx2 * ny * nz * c          # one spectral field
+    fine = nx2 * ny * nzp * c        # one z-transformed field on the 3/2 z grid
+    return {
+        "zinv": 5 * fld + 6 * fine,
+        "xpass": 6 * fine + 3 * fine,
+        "zfwd": 3 * fine + 3 * fld,
+        "cheb_fwd": 3 * fld + 3 * fld,
+        "cheb_inv": 5 * fld + 5 * fld,
+    }.get(name)
+
+
+def own_arm(args, rank, world):
+    from simson_b200.bla import Channel, PinnedArray, FP64, MIXED
+    from simson_b200.fields import channel_field
+    import ctypes
+
+    w = WORKLOAD
+    prec = MIXED if args.precision == "mixed" else FP64
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], precision=prec, device=dev)
+    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"] + rank)
+    ch.set_velocity(u, v, wv)
+    ch.prhs()
+    for _ in range(args.warmup):
+        ch.step(1)
+    ch.sync()
+    dist_barrier(world)
+    clk = ClockSampler(dev)
+    clk.start()
+    l0 = ch.launches()
+    ch.record(0)
+    ch.step(args.steps)
+    ch.record(1)
+    ms = ch.elapsed_ms(0, 1)
+    launches = ch.launches() - l0
+    clocks = clk.stop()
+    ms = dist_max(ms, world)
+    sc = ch.scalars()
+    # per-kernel times (a separate, profiled run of 2 steps)
+    ch.profile(True)
+    ch.step(2)
+    prof = ch.profile_read()
+    ch.profile(False)
+    # end-to-end through the public API with host buffers
+    nslots = 7
+    shape = (nslots, w["nz"], w["ny"], w["nx"] // 2)
+    hr = PinnedArray(shape)
+    hi = PinnedArray(shape)
+    ch.download_raw(hr.ptr, hi.ptr, nslots)
+    e2e_steps = max(2, min(args.steps, 10))
+    ch.sync()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ch.upload_raw(hr.ptr, hi.ptr, nslots)
+        ch.step(1)
+        ch.download_raw(hr.ptr, hi.ptr, nslots)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(e2e_s * 1000.0, world) / 1000.0
+    nbytes = int(np.prod(shape)) * 8 * 2
+    hr.free()
+    hi.free()
+    finite = bool(np.isfinite(sc["px"]))
+    ch.close()
+    return dict(ms=ms, launches=launches, clocks=clocks, prof=prof, e2e_s=e2e_s, e2e_steps=e2e_steps,
+                e2e_bytes=nbytes, scalars=sc, finite=finite)
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_max(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(steps, threads, sample_note):
+    """Time the reference's own implementation (translated Fortran) on host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from refsim import RefSim
+    from simson_b200.fields import channel_field
+    w = WORKLOAD
+    ref = RefSim(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], threads=threads,
+                 build=os.path.isdir(os.environ.get("SIMSON_REFERENCE", "/root/reference")))
+    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"])
+    ref.set_velocity(u, v, wv)
+    ref.start()
+    ref.substep()  # warm-up substep (page faults, caches)
+    t0 = time.perf_counter()
+    ref.substep()
+    ref.substep()
+    ref.substep()
+    dt = time.perf_counter() - t0
+    return dict(value=1.0 / dt, unit="steps/s", cores=threads, kind="reference",
+                sample=f"{sample_note}: 1 full RK3 step (3 substeps) after 1 warm-up substep, "
+                       f"translated reference bla (gcc -O3 -fopenmp), {threads} threads")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    threads = os.cpu_count() or 1
+    w = WORKLOAD
+    config = {"workload": "temporal channel 384x193x384 (576x193x576 dealiased), box 2pi x 2 x pi, Re_cl 9000, "
+                          "cflux, dt 0.002, seeded rms 0.1 perturbation", "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
+              "precision": args.precision, "l2": "state 1.6 GB > L2, no flush needed",
+              "parallelism": f"replicas x{args.gpus}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        try:
+            r = cpu_reference(args.steps, threads, "per step")
+        except Exception as e:  # pragma: no cover
+            print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {e}"}))
+            return
+        line = {"metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": args.gpus, "steps": 1,
+                "warmup": 1, "ms_per_step": 1000.0 / r["value"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": r, "e2e": {"value": r["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    res = own_arm(args, rank, world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    steps_per_s = args.steps / (res["ms"] / 1000.0) * args.gpus
+    ms_step = res["ms"] / args.steps
+    hbm, peak_kind = peaks()
+    nc = (w["nx"] // 2) * w["ny"] * w["nz"]
+    prof = res["prof"]
+    # dominant kernel by measured time
+    dom = max((k for k in prof if k not in ("other",) and prof[k][1] > 0), key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / prof[dom][1]
+    dom_bytes = kernel_bytes(dom, w)
+    roof = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
+            "traffic": None, "launch_ms": dom_ms}
+    if dom_bytes:
+        ach = dom_bytes / (dom_ms / 1000.0) / 1e9
+        roof.update(achieved=ach, frac=ach / hbm, algorithmic_bytes=dom_bytes)
+    else:
+        roof.update(achieved=None, frac=None, algorithmic_bytes=None)
+    stage_bytes = substep_bytes(nc, 16)
+    step_ach = 3 * stage_bytes / (ms_step / 1000.0) / 1e9
+    line = {
+        "metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": config,
+        "grid_point_stages_per_s": w["nx"] * w["ny"] * w["nz"] * 3 * steps_per_s,
+        "roofline": roof,
+        "step_roofline": {"bound": "hbm", "bytes_per_substep": stage_bytes, "achieved": step_ach, "peak": hbm,
+                          "frac": step_ach / hbm, "unit": "GB/s"},
+        "kernel_ms_per_substep": {k: (v[0] / max(v[1], 1)) for k, v in prof.items() if v[1]},
+        "e2e": {"value": res["e2e_steps"] / res["e2e_s"] * args.gpus, "unit": "steps/s",
+                "h2d_bytes_per_step": res["e2e_bytes"], "d2h_bytes_per_step": res["e2e_bytes"]},
+        "gpu_launches": res["launches"],
+        "clocks": res["clocks"],
+        "finite": res["finite"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference(1, threads, "bounded sample")
+        except Exception as e:  # pragma: no cover
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+/* simson_b200: B200-native time step of Simson's bla (temporal channel).
+ *
+ * C ABI of the drop-in for the two plane loops of the reference driver:
+ *   bla/bla.f:2251-2290  do ybp: call nonlinbl(...)   -> sgpu_nonlin
+ *   bla/bla.f:2433-2476  do zbp: call linearbl(...)   -> sgpu_linear
+ * plus the startup partial right-hand side bla/bla.f:1562 (prhs) -> sgpu_prhs.
+ *
+ * Calling convention: plain C, every entry returns 0 on success or a negative
+ * SGPU_E* code (the Fortran shim maps non-zero to stopnow(code)).  Arrays use
+ * the reference's main-storage layout ur(memnx,memny,memnz,slot), 0-based
+ * index x + memnx*(y + memny*(z + memnz*slot)), split real/imaginary double
+ * arrays exactly as bla keeps them (bla/bla.f:67, bla/par.f:111-120).  Slots:
+ * 0-2 u,v,w and 3-4 omega_x,omega_z (Fourier x/z, physical y), 5-6 the partial
+ * right-hand sides p_v, p_omega_y (Chebyshev y).
+ *
+ * Ownership: the device owns the state between upload and download; one
+ * context per process, not re-entrant, called from one host thread.
+ */
+#ifndef SIMSON_B200_H
+#define SIMSON_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGPU_OK 0
+#define SGPU_E_PARAM (-1)      /* invalid parameters (grid, nst, dt, ...) */
+#define SGPU_E_CUDA (-2)       /* CUDA runtime error (allocation, launch)  */
+#define SGPU_E_STATE (-3)      /* call out of order (no state uploaded)    */
+#define SGPU_E_CFL (-4)        /* CFL*dt > 10: the reference stops (wcflbl.f:93) */
+#define SGPU_E_NAN (-5)        /* non-finite value detected in the state   */
+
+#define SGPU_FP64 0            /* every transform and solve in FP64 */
+#define SGPU_MIXED 1           /* FP32 FFTs/products/Chebyshev transforms, FP64 solves */
+
+typedef struct sgpu_ctx sgpu_ctx;
+
+/* The subset of par.f and bla.i that the channel step reads. */
+typedef struct sgpu_params {
+  int nx, ny, nz;   /* par.f nx, ny, nz (nfxd = nfzd = 1, nfyd = 0) */
+  double re;        /* bla.i re (centreline Reynolds number) */
+  double xl, zl;    /* box length in x and z */
+  double dt;        /* fixed time step (bla.i dt > 0) */
+  int nst;          /* RK stages: 3 (bla.i nst) */
+  int cflux;        /* 1: constant mass flux (bla.i cflux); 0: fixed px */
+  double mflux;     /* target flux under cflux (bla.f:1629 sets 4/3) */
+  double px;        /* pressure gradient; first guess under cflux (-2/re) */
+  double rot;       /* bla.i rot */
+  int icfl;         /* CFL every icfl substeps (bla.i icfl, rounded as rparambl.f:1862) */
+  int precision;    /* SGPU_FP64 or SGPU_MIXED */
+  int device;       /* CUDA device ordinal */
+} sgpu_params;
+
+/* bla/bla.f:709-1082 subset: allocate the resident state and tables.
+ * Replaces the preprbl/rkcoeff set-up for the device path. */
+int sgpu_init(const sgpu_params* prm, sgpu_ctx** ctx);
+int sgpu_finalize(sgpu_ctx* ctx);
+
+/* Host <-> device state in the reference layout (bla/par.f:111-120).
+ * nslots = number of leading slots transferred (3: velocities only). */
+int sgpu_upload_state(sgpu_ctx* ctx, const double* ur, const double* ui, int nslots);
+int sgpu_download_state(sgpu_ctx* ctx, double* ur, double* ui, int nslots);
+/* Mean-flow partial right-hand side puw(ny,2) (linearbl.f argument puw). */
+int sgpu_upload_puw(sgpu_ctx* ctx, const double* puw);
+int sgpu_download_puw(sgpu_ctx* ctx, double* puw);
+
+/* bla/prhs.f, called at bla/bla.f:1562: from u,v,w (slots 0-2) build
+ * omega_x, omega_z, p_v, p_omega and puw for the first stage; also resets the
+ * RK bookkeeping to the first substep (bla/bla.f:1464-1478, 1622-1662). */
+int sgpu_prhs(sgpu_ctx* ctx);
+
+/* One RK substep, split like the reference driver:
+ * sgpu_nonlin replaces the nonlinbl plane loop (bla/bla.f:2251-2290,
+ * bla/nonlinbl.f:9-32) including boxcfl (CFL partial maxima);
+ * sgpu_linear replaces the RK-weight update (bla/bla.f:2384-2397) and the
+ * linearbl plane loop (bla/bla.f:2433-2476, bla/linearbl.f:9-27), including
+ * the constant-flux px correction, and advances it/t (bla/bla.f:2598-2607). */
+int sgpu_nonlin(sgpu_ctx* ctx);
+int sgpu_linear(sgpu_ctx* ctx);
+/* nsub consecutive substeps (nonlin + linear), enqueued without host syncs. */
+int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
+
+/* Scalars, in this order: px, mflux, t, cfl (CFL*dt of the last evaluated
+ * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises. */
+int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
+
+/* Stream-ordered timing on the library's stream: record event slot (0..15),
+ * elapsed milliseconds between two recorded slots (synchronises on b). */
+int sgpu_event_record(sgpu_ctx* ctx, int slot);
+int sgpu_event_elapsed(sgpu_ctx* ctx, int a, int b, float* ms);
+int sgpu_sync(sgpu_ctx* ctx);
+
+/* Per-kernel timing for profiling runs: enable, run substeps, read the
+ * milliseconds and launch counts per kernel id (0 zinv, 1 xpass, 2 zfwd,
+ * 3 Chebyshev forward, 4 pencil solve, 5 mean flow, 6 Chebyshev inverse,
+ * 7 other).  Adds an event record per launch; not for timed runs. */
+int sgpu_profile(sgpu_ctx* ctx, int enable);
+int sgpu_profile_read(sgpu_ctx* ctx, double* ms, int* count, int n);
+
+/* Page-locked host buffers for the host<->device state copies (cudaHostAlloc):
+ * a Fortran host can keep ur/ui in them to get full-bandwidth transfers. */
+int sgpu_host_alloc(unsigned long long bytes, void** ptr);
+int sgpu_host_free(void* ptr);
+
+/* Device kernels launched by this context so far (launch accounting). */
+long long sgpu_launch_count(sgpu_ctx* ctx);
+const char* sgpu_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,228 @@
+"""Python host side of the B200 channel step (ctypes over the C ABI).
+
+The reference's interface for this path is the pair of plane-loop calls in the
+``bla`` driver (``nonlinbl`` over xz-planes, ``linearbl`` over xy-planes,
+bla/bla.f:2251-2290 and 2433-2476) plus the startup ``prhs`` (bla/bla.f:1562).
+:class:`Channel` mirrors that driver for the temporal channel: the same
+``bla.i`` parameters, the same main-storage layout and slot numbering, and the
+same substep bookkeeping.  The state lives on the GPU; ``get_slot`` /
+``set_slot`` copy it in the reference layout.
+
+There is no CPU fallback: constructing a :class:`Channel` without the CUDA
+library (or without a GPU) raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+FP64 = 0
+MIXED = 1
+
+
+class SgpuParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("re", ctypes.c_double), ("xl", ctypes.c_double), ("zl", ctypes.c_double),
+        ("dt", ctypes.c_double), ("nst", ctypes.c_int), ("cflux", ctypes.c_int),
+        ("mflux", ctypes.c_double), ("px", ctypes.c_double), ("rot", ctypes.c_double),
+        ("icfl", ctypes.c_int), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class SimsonError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def load_library(build: bool = True):
+    """Load (building if needed) ``simson_b200/_lib/libsimson_b200.so``."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.build() if build else _build.LIB
+    if not os.path.exists(path):
+        raise SimsonError(f"CUDA library missing: {path}")
+    lib = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    vp = ctypes.c_void_p
+    lib.sgpu_init.argtypes = [ctypes.POINTER(SgpuParams), ctypes.POINTER(vp)]
+    lib.sgpu_finalize.argtypes = [vp]
+    lib.sgpu_upload_state.argtypes = [vp, dp, dp, ctypes.c_int]
+    lib.sgpu_download_state.argtypes = [vp, dp, dp, ctypes.c_int]
+    lib.sgpu_upload_puw.argtypes = [vp, dp]
+    lib.sgpu_download_puw.argtypes = [vp, dp]
+    for fn in ("sgpu_prhs", "sgpu_nonlin", "sgpu_linear", "sgpu_sync"):
+        getattr(lib, fn).argtypes = [vp]
+    lib.sgpu_step_rk.argtypes = [vp, ctypes.c_int]
+    lib.sgpu_get_scalars.argtypes = [vp, dp, ctypes.c_int]
+    lib.sgpu_event_record.argtypes = [vp, ctypes.c_int]
+    lib.sgpu_event_elapsed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    lib.sgpu_launch_count.argtypes = [vp]
+    lib.sgpu_launch_count.restype = ctypes.c_longlong
+    lib.sgpu_error_string.restype = ctypes.c_char_p
+    lib.sgpu_host_alloc.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
+    lib.sgpu_host_free.argtypes = [vp]
+    lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
+    lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    _LIB = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+SCALARS = ("px", "mflux", "t", "cfl", "an", "bn", "anp1", "bnp1", "cnp1", "it", "tc", "dt")
+
+
+class Channel:
+    """Temporal channel (fltype=1, RK3/CN, tau, ibc=0) resident on one GPU."""
+
+    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, mflux=4.0 / 3.0, px=None,
+                 rot=0.0, icfl=3, precision=FP64, device=0):
+        self.lib = load_library()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.shape = (nz, ny, nx // 2)
+        if px is None:
+            px = -2.0 / re  # bla/bla.f:1630 first guess under cflux
+        prm = SgpuParams(nx, ny, nz, re, xl, zl, dt, 3, int(cflux), mflux, px, rot, icfl, precision, device)
+        self._ctx = ctypes.c_void_p()
+        self._check(self.lib.sgpu_init(ctypes.byref(prm), ctypes.byref(self._ctx)), "sgpu_init")
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise SimsonError(f"{what}: {self.lib.sgpu_error_string(rc).decode()} ({rc})")
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self.lib.sgpu_finalize(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- state in the reference layout ---------------------------------
+    def set_state(self, slots):
+        """slots: list of complex arrays (nz, ny, nx//2) for slots 1..k."""
+        k = len(slots)
+        a = np.ascontiguousarray(np.stack([np.asarray(s, np.complex128).reshape(self.shape) for s in slots]))
+        re_ = np.ascontiguousarray(a.real)
+        im_ = np.ascontiguousarray(a.imag)
+        self._check(self.lib.sgpu_upload_state(self._ctx, _dp(re_), _dp(im_), k), "upload")
+
+    def set_velocity(self, u, v, w):
+        self.set_state([u, v, w])
+
+    def state(self, nslots=7):
+        re_ = np.empty((nslots,) + self.shape)
+        im_ = np.empty((nslots,) + self.shape)
+        self._check(self.lib.sgpu_download_state(self._ctx, _dp(re_), _dp(im_), nslots), "download")
+        return list(re_ + 1j * im_)
+
+    def get_slot(self, slot):
+        return self.state(slot)[slot - 1]
+
+    def puw(self):
+        p = np.empty((2, self.ny))
+        self._check(self.lib.sgpu_download_puw(self._ctx, _dp(p)), "puw")
+        return p
+
+    # --- the reference's call sequence ----------------------------------
+    def prhs(self):
+        self._check(self.lib.sgpu_prhs(self._ctx), "prhs")
+
+    start = prhs
+
+    def nonlinbl(self):
+        """Step 2 of the substep for all xz-planes (bla/nonlinbl.f)."""
+        self._check(self.lib.sgpu_nonlin(self._ctx), "nonlin")
+
+    def linearbl(self):
+        """Step 3 of the substep for all xy-planes (bla/linearbl.f)."""
+        self._check(self.lib.sgpu_linear(self._ctx), "linear")
+
+    def substep(self):
+        self.nonlinbl()
+        self.linearbl()
+
+    def step(self, n=1):
+        """n full RK3 steps (3 substeps each), no host synchronisation."""
+        self._check(self.lib.sgpu_step_rk(self._ctx, 3 * n), "step")
+
+    def substeps(self, n):
+        self._check(self.lib.sgpu_step_rk(self._ctx, n), "step")
+
+    def sync(self):
+        self._check(self.lib.sgpu_sync(self._ctx), "sync")
+
+    def scalars(self):
+        s = np.empty(12)
+        self._check(self.lib.sgpu_get_scalars(self._ctx, _dp(s), 12), "scalars")
+        return dict(zip(SCALARS, s))
+
+    def record(self, slot):
+        self._check(self.lib.sgpu_event_record(self._ctx, slot), "event")
+
+    def elapsed_ms(self, a, b):
+        ms = ctypes.c_float()
+        self._check(self.lib.sgpu_event_elapsed(self._ctx, a, b, ctypes.byref(ms)), "elapsed")
+        return ms.value
+
+    def upload_raw(self, re_ptr, im_ptr, nslots):
+        """Upload from caller-owned host buffers (e.g. pinned), reference layout."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.sgpu_upload_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
+                    "upload")
+
+    def download_raw(self, re_ptr, im_ptr, nslots):
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.sgpu_download_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
+                    "download")
+
+    KERNELS = ("zinv", "xpass", "zfwd", "cheb_fwd", "pencil", "mean", "cheb_inv", "other")
+
+    def profile(self, enable=True):
+        self._check(self.lib.sgpu_profile(self._ctx, int(enable)), "profile")
+
+    def profile_read(self):
+        n = len(self.KERNELS)
+        ms = np.zeros(n)
+        cnt = (ctypes.c_int * n)()
+        self._check(self.lib.sgpu_profile_read(self._ctx, _dp(ms), cnt, n), "profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNELS)}
+
+    def launches(self):
+        return int(self.lib.sgpu_launch_count(self._ctx))
+
+
+class PinnedArray:
+    """A numpy view of page-locked host memory allocated by the library."""
+
+    def __init__(self, shape, dtype=np.float64):
+        lib = load_library()
+        self.lib = lib
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = ctypes.c_void_p()
+        rc = lib.sgpu_host_alloc(n, ctypes.byref(self.ptr))
+        if rc != 0:
+            raise SimsonError("sgpu_host_alloc failed")
+        buf = (ctypes.c_char * n).from_address(self.ptr.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.lib.sgpu_host_free(self.ptr)
+            self.ptr = None

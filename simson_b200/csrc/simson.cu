@@ -1,0 +1,535 @@
+// Host side of the C ABI declared in include/simson_b200.h: the resident
+// device state, the transform plans and tables, and the launch sequence of one
+// RK3/CN substep.  The RK bookkeeping mirrors the reference driver
+// (bla/bla.f:1464-1478 first stage, 2382-2397 weights, 2598-2607 time).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/simson_b200.h"
+#include "fft.cuh"
+#include "layout.cuh"
+#include "step2.cuh"
+#include "step3.cuh"
+
+using namespace sb;
+
+namespace {
+
+const double ANRK[3] = {8. / 15., 5. / 12., 3. / 4.};
+const double BNRK[3] = {0., -17. / 60., -5. / 12.};
+const double CNRK[3] = {0., 8. / 15., 2. / 3.};
+
+struct Tw {
+  double2* d = nullptr;
+  float2* f = nullptr;
+  FFTPlan plan{};
+};
+
+}  // namespace
+
+struct sgpu_ctx {
+  sgpu_params prm{};
+  Dims g{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[16] = {};
+  // resident state
+  double2* st = nullptr;     // [7][nyp][NP]
+  double* puw = nullptr;     // [2][ny]
+  double* scal = nullptr;    // [0] px, [1] mflux
+  unsigned long long* cfl_bits = nullptr;
+  double* alfa = nullptr;
+  double* beta = nullptr;
+  double* dyi = nullptr;
+  // step-2 buffers
+  double2* zb = nullptr;     // [6][nyp][nzp][nx2]
+  double2* xb = nullptr;     // [3][nyp][nzp][nx2]
+  // step-3 scratch
+  double2* cz = nullptr;     // complex scratch columns, [ncz][nyp][NP]
+  int ncz = 0;
+  double* rz = nullptr;      // real scratch columns, [nrz][nyp][NP]
+  int nrz = 0;
+  double* mscr = nullptr;    // mean-flow scratch
+  double* stage = nullptr;   // host<->device staging (split re/im)
+  Tw twz, twx, twy;
+  // RK bookkeeping (host mirror of the reference driver scalars)
+  double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
+  int it = 1;
+  double cfl = 0.0;
+  bool cfl_pending = false;
+  bool have_state = false;
+  long long launches = 0;
+  int kb = 8, rb = 2, pb = 8;
+  // optional per-kernel timing (sgpu_profile): event pairs around each launch
+  bool prof = false;
+  std::vector<cudaEvent_t> pev;
+  std::vector<int> pid;
+  int pnext = 0;
+};
+
+enum KernelId { K_ZINV = 0, K_XPASS, K_ZFWD, K_CHEB_FWD, K_PENCIL, K_MEAN, K_CHEB_INV, K_OTHER, K_COUNT };
+
+static void prof_mark(sgpu_ctx* c, int id) {
+  if (!c->prof) return;
+  if (c->pnext + 1 >= (int)c->pev.size()) return;
+  cudaEventRecord(c->pev[c->pnext], c->stream);
+  c->pid[c->pnext] = id;
+  c->pnext++;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  if (e != cudaSuccess) {
+    fprintf(stderr, "simson_b200: %s: %s\n", where, cudaGetErrorString(e));
+    return SGPU_E_CUDA;
+  }
+  return SGPU_OK;
+}
+#define CK(x)                                        \
+  do {                                               \
+    int _r = cuda_fail((x), #x);                     \
+    if (_r) return _r;                               \
+  } while (0)
+
+static FFTPlan make_plan(int n) {
+  FFTPlan p{};
+  p.n = n;
+  int m = n, k = 0;
+  while (m % 4 == 0) { p.radix[k++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.radix[k++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.radix[k++] = 3; m /= 3; }
+  while (m % 5 == 0) { p.radix[k++] = 5; m /= 5; }
+  p.npass = (m == 1) ? k : -1;
+  return p;
+}
+
+static int make_tw(Tw& t, int n) {
+  t.plan = make_plan(n);
+  if (t.plan.npass < 0) return SGPU_E_PARAM;
+  std::vector<double2> hd(n);
+  std::vector<float2> hf(n);
+  for (int m = 0; m < n; ++m) {
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+    hd[m] = double2{(double)cosl(ang), (double)sinl(ang)};
+    hf[m] = float2{(float)cosl(ang), (float)sinl(ang)};
+  }
+  CK(cudaMalloc(&t.d, n * sizeof(double2)));
+  CK(cudaMalloc(&t.f, n * sizeof(float2)));
+  CK(cudaMemcpy(t.d, hd.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(t.f, hf.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+  return SGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion between the reference's split arrays and the device state
+// ---------------------------------------------------------------------------
+__global__ void k_from_ref(const double* __restrict__ re, const double* __restrict__ im, double2* __restrict__ st,
+                           Dims g, int nslots) {
+  const size_t tot = (size_t)nslots * g.nyp * g.NP;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    // i indexes the reference layout x + nx2*(y + nyp*(z + nz*s))
+    size_t r = i;
+    const int x = r % g.nx2; r /= g.nx2;
+    const int y = r % g.nyp; r /= g.nyp;
+    const int z = r % g.nz; r /= g.nz;
+    const int s = (int)r;
+    st[((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x] = double2{re[i], im[i]};
+  }
+}
+
+__global__ void k_to_ref(const double2* __restrict__ st, double* __restrict__ re, double* __restrict__ im, Dims g,
+                         int nslots) {
+  const size_t tot = (size_t)nslots * g.nyp * g.NP;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    size_t r = i;
+    const int x = r % g.nx2; r /= g.nx2;
+    const int y = r % g.nyp; r /= g.nyp;
+    const int z = r % g.nz; r /= g.nz;
+    const int s = (int)r;
+    const double2 v = st[((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x];
+    re[i] = v.x;
+    im[i] = v.y;
+  }
+}
+
+__global__ void k_cfl_reset(unsigned long long* c) { *c = 0ull; }
+
+// ---------------------------------------------------------------------------
+
+extern "C" const char* sgpu_error_string(int code) {
+  switch (code) {
+    case SGPU_OK: return "ok";
+    case SGPU_E_PARAM: return "invalid parameters";
+    case SGPU_E_CUDA: return "CUDA error";
+    case SGPU_E_STATE: return "call out of order";
+    case SGPU_E_CFL: return "CFL*dt above 10";
+    case SGPU_E_NAN: return "non-finite state";
+    default: return "unknown error";
+  }
+}
+
+static size_t smem_fft(int n, int cols, size_t elem) { return 2 * (size_t)n * cols * elem; }
+
+extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
+  if (!prm || !out) return SGPU_E_PARAM;
+  *out = nullptr;
+  const sgpu_params& P = *prm;
+  if (P.nx < 4 || P.nz < 4 || P.nx % 4 || P.nz % 2 || P.ny < 9 || (P.ny % 2) == 0 || P.nst != 3 || !(P.dt > 0) ||
+      !(P.re > 0) || !(P.xl > 0) || !(P.zl > 0) || P.precision != SGPU_FP64)
+    return SGPU_E_PARAM;
+  sgpu_ctx* c = new sgpu_ctx();
+  c->prm = P;
+  Dims& g = c->g;
+  g.nx = P.nx; g.ny = P.ny; g.nz = P.nz;
+  g.nx2 = P.nx / 2; g.nyp = P.ny;
+  g.nxp = P.nx + P.nx / 2; g.nzp = P.nz + P.nz / 2;
+  g.NP = P.nz * g.nx2; g.zodd = P.nz / 2;
+  int rc = SGPU_OK;
+  auto fail = [&](int r) { sgpu_finalize(c); return r; };
+  if (cudaSetDevice(P.device) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(SGPU_E_CUDA);
+  for (int i = 0; i < 16; ++i)
+    if (cudaEventCreate(&c->ev[i]) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if ((rc = make_tw(c->twz, g.nzp)) || (rc = make_tw(c->twx, g.nxp)) || (rc = make_tw(c->twy, 2 * (g.nyp - 1))))
+    return fail(rc);
+  const size_t fld = (size_t)g.nyp * g.NP;
+  c->ncz = 23;
+  c->nrz = 5;
+  if (cudaMalloc(&c->st, 7 * fld * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&c->puw, 2 * g.ny * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->scal, 4 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->cfl_bits, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&c->alfa, g.nx2 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->beta, g.nz * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->dyi, g.nyp * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->zb, 6 * (size_t)g.nyp * g.nzp * g.nx2 * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&c->xb, 3 * (size_t)g.nyp * g.nzp * g.nx2 * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&c->cz, (size_t)c->ncz * fld * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&c->rz, (size_t)c->nrz * fld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess)
+    return fail(SGPU_E_CUDA);
+  cudaMemset(c->st, 0, 7 * fld * sizeof(double2));
+  cudaMemset(c->puw, 0, 2 * g.ny * sizeof(double));
+  // wavenumbers (bla/preprbl.f:36-43) and CFL grid spacing (bla/boxcfl.f:25-56)
+  const double pi = 3.1415926535897932385;
+  std::vector<double> alfa(g.nx2), beta(g.nz, 0.0), dyi(g.nyp), eta(g.nyp), deta(g.nyp);
+  for (int x = 0; x < g.nx2; ++x) alfa[x] = 2. * pi / P.xl * (double)x;
+  for (int z = 1; z <= g.nz / 2; ++z) {
+    beta[z] = 2. * pi / P.zl * (double)z;
+    beta[g.nz - z] = -2. * pi / P.zl * (double)z;
+  }
+  for (int y = 0; y < g.nyp; ++y) eta[y] = cos(pi * (double)y / (double)(g.nyp - 1));
+  deta[0] = 1. - eta[1];
+  deta[g.nyp - 1] = deta[0];
+  for (int y = 1; y < g.nyp - 1; ++y) deta[y] = (eta[y - 1] - eta[y + 1]) * .5;
+  for (int y = 0; y < g.nyp; ++y) {
+    double d = (double)(g.ny - 1) / (double)(g.nyp - 1) / deta[y];
+    if (g.ny >= 17) d = fmin(d, (double)(g.ny - 1) * (double)(g.ny - 1) / 10. / 3.14);
+    dyi[y] = d;
+  }
+  cudaMemcpy(c->alfa, alfa.data(), g.nx2 * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->beta, beta.data(), g.nz * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->dyi, dyi.data(), g.nyp * sizeof(double), cudaMemcpyHostToDevice);
+  double sc[4] = {P.px, P.mflux, 0, 0};
+  cudaMemcpy(c->scal, sc, sizeof(sc), cudaMemcpyHostToDevice);
+  // shared-memory opt-in
+  const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
+  const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
+  const size_t s_y = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
+  if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024) return fail(SGPU_E_PARAM);
+  cudaFuncSetAttribute(k_zinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zfwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_xpass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
+  cudaFuncSetAttribute(k_cheb<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_y);
+  c->dtn = P.dt;
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
+  *out = c;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_finalize(sgpu_ctx* c) {
+  if (!c) return SGPU_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->st, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+                  c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < 16; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (auto& e : c->pev) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_upload_state(sgpu_ctx* c, const double* ur, const double* ui, int nslots) {
+  if (!c || !ur || !ui || nslots < 1 || nslots > 7) return SGPU_E_PARAM;
+  const size_t n = (size_t)nslots * c->g.nyp * c->g.NP;
+  CK(cudaMemcpyAsync(c->stage, ur, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->stage + n, ui, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_from_ref<<<592, 256, 0, c->stream>>>(c->stage, c->stage + n, c->st, c->g, nslots);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_state = true;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_download_state(sgpu_ctx* c, double* ur, double* ui, int nslots) {
+  if (!c || !ur || !ui || nslots < 1 || nslots > 7) return SGPU_E_PARAM;
+  const size_t n = (size_t)nslots * c->g.nyp * c->g.NP;
+  k_to_ref<<<592, 256, 0, c->stream>>>(c->st, c->stage, c->stage + n, c->g, nslots);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ur, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(ui, c->stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_upload_puw(sgpu_ctx* c, const double* puw) {
+  if (!c || !puw) return SGPU_E_PARAM;
+  CK(cudaMemcpyAsync(c->puw, puw, 2 * c->g.ny * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_download_puw(sgpu_ctx* c, double* puw) {
+  if (!c || !puw) return SGPU_E_PARAM;
+  CK(cudaMemcpyAsync(puw, c->puw, 2 * c->g.ny * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+static double2* czf(sgpu_ctx* c, int k) { return c->cz + (size_t)k * c->g.nyp * c->g.NP; }
+static double* rzf(sgpu_ctx* c, int k) { return c->rz + (size_t)k * c->g.nyp * c->g.NP; }
+static double2* slot(sgpu_ctx* c, int s) { return c->st + (size_t)s * c->g.nyp * c->g.NP; }
+
+static void launch_cheb(sgpu_ctx* c, const double2* in, size_t in_fs, double2* out, size_t out_fs, int nfields,
+                        int inverse, double scale, int skip_oddball) {
+  const Dims& g = c->g;
+  dim3 grid((g.NP + c->pb - 1) / c->pb, nfields);
+  const size_t sm = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
+  k_cheb<double><<<grid, 256, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse, scale, c->twy.plan, c->twy.d,
+                                              c->pb, skip_oddball);
+  c->launches++;
+}
+
+extern "C" int sgpu_prhs(sgpu_ctx* c) {
+  if (!c) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  const Dims& g = c->g;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  // first-stage RK factors (bla/bla.f:1466-1478) and cflux px (:1622-1633)
+  c->dtn = c->prm.dt;
+  c->an = c->dtn * ANRK[0];
+  c->cnp1 = 0.0;
+  c->anp1 = c->an;
+  c->bnp1 = 0.0;
+  c->bn = 0.0;
+  c->it = 1;
+  c->t = 0.0;
+  c->tc = 0.0;
+  // Chebyshev coefficients of u, v, w
+  launch_cheb(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0, 0);
+  PrhsBufs B;
+  B.U1 = czf(c, 0); B.U2 = czf(c, 1); B.U3 = czf(c, 2);
+  B.OMY = czf(c, 3); B.OX = czf(c, 4); B.OZ = czf(c, 5); B.PHI = czf(c, 6); B.T1 = czf(c, 7); B.T2 = czf(c, 8);
+  B.PV = slot(c, 5); B.PW = slot(c, 6); B.puw = c->puw;
+  k_prhs<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, c->prm.re, c->anp1);
+  c->launches++;
+  // omega_x, omega_z back to physical y into slots 3, 4
+  launch_cheb(c, czf(c, 4), fld, slot(c, 3), fld, 2, 1, 1.0, 0);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+static int enqueue_nonlin(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const sgpu_params& P = c->prm;
+  c->tc = c->t + c->cnp1;
+  // CFL partial maxima only on the substeps the reference evaluates them
+  // (nonlinbl.f: mod(it-1,icfl) == 0); the device word keeps the last one.
+  const bool do_cfl = (P.icfl > 0) && ((c->it - 1) % P.icfl == 0);
+  if (do_cfl) {
+    prof_mark(c, K_OTHER);
+    k_cfl_reset<<<1, 1, 0, c->stream>>>(c->cfl_bits);
+    c->launches++;
+  }
+  dim3 gz((g.nx2 + c->kb - 1) / c->kb, g.nyp);
+  const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
+  prof_mark(c, K_ZINV);
+  k_zinv<double><<<gz, 256, s_z, c->stream>>>(c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta, c->kb);
+  dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
+  const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
+  const double dxi = (double)(g.nx - 2) / P.xl;
+  const double dzi = (double)(g.nz - 2) / P.zl;
+  prof_mark(c, K_XPASS);
+  k_xpass<double><<<gx, 256, s_x, c->stream>>>(c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot,
+                                               c->rb, do_cfl ? c->cfl_bits : nullptr);
+  prof_mark(c, K_ZFWD);
+  k_zfwd<double><<<gz, 256, s_z, c->stream>>>(c->xb, c->st, g, c->twz.plan, c->twz.d, c->kb);
+  c->launches += 3;
+  if (do_cfl) c->cfl_pending = true;
+  return cuda_fail(cudaGetLastError(), "nonlin launch");
+}
+
+static int enqueue_linear(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const sgpu_params& P = c->prm;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  // RK weights (bla/bla.f:2384-2397)
+  c->an = c->anp1;
+  c->bn = c->bnp1;
+  const int k = c->it % 3;
+  c->anp1 = c->dtn * ANRK[k];
+  c->bnp1 = c->dtn * BNRK[k];
+  c->cnp1 = c->dtn * CNRK[k];
+  RKc rk{c->an, c->bn, c->anp1, c->bnp1};
+  // Chebyshev transform of H, normalised by 1/(nxp nzp) (linearbl.f:262-273)
+  prof_mark(c, K_CHEB_FWD);
+  launch_cheb(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0 / ((double)g.nxp * (double)g.nzp), 0);
+  PencilBufs B;
+  B.H1 = czf(c, 0); B.H2 = czf(c, 1); B.H3 = czf(c, 2);
+  B.PV = slot(c, 5); B.PW = slot(c, 6);
+  B.G = czf(c, 3); B.DG = czf(c, 4); B.HV = czf(c, 5); B.HOM = czf(c, 6); B.FV = czf(c, 7); B.FW = czf(c, 8);
+  B.PHI = czf(c, 9); B.OM = czf(c, 10); B.V = czf(c, 11); B.DV = czf(c, 12); B.DOM = czf(c, 13);
+  B.T1 = czf(c, 14); B.T2 = czf(c, 15);
+  B.OU = czf(c, 16); B.OV = czf(c, 17); B.OW = czf(c, 18); B.OX = czf(c, 19); B.OZ = czf(c, 20);
+  B.PHIH = rzf(c, 0); B.VH = rzf(c, 1); B.DVH = rzf(c, 2); B.CP = rzf(c, 3); B.WT = rzf(c, 4);
+  prof_mark(c, K_PENCIL);
+  k_pencil<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+  MeanArgs M;
+  M.H1 = B.H1; M.H3 = B.H3; M.puw = c->puw; M.scal = c->scal; M.scr = c->mscr;
+  M.OU = B.OU; M.OV = B.OV; M.OW = B.OW; M.OX = B.OX; M.OZ = B.OZ; M.PV = B.PV; M.PW = B.PW;
+  M.cflux = P.cflux;
+  prof_mark(c, K_MEAN);
+  k_mean<<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
+  // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
+  prof_mark(c, K_CHEB_INV);
+  launch_cheb(c, B.OU, fld, slot(c, 0), fld, 5, 1, 1.0, 1);
+  prof_mark(c, K_OTHER);
+  c->launches += 2;
+  // bla/bla.f:2598-2607
+  c->it += 1;
+  if ((c->it - 1) % 3 == 0) c->t = c->t + c->dtn;
+  return cuda_fail(cudaGetLastError(), "linear launch");
+}
+
+static int collect_cfl(sgpu_ctx* c) {
+  if (!c->cfl_pending) return SGPU_OK;
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double m;
+  memcpy(&m, &bits, sizeof(m));
+  const double pi = 3.1415926535897932385;
+  c->cfl = (m * pi + 2. * fabs(c->prm.rot)) * c->dtn;  // bla/wcflbl.f:87
+  c->cfl_pending = false;
+  if (!(c->cfl <= 10.)) return std::isnan(c->cfl) ? SGPU_E_NAN : SGPU_E_CFL;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_nonlin(sgpu_ctx* c) {
+  if (!c) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  int r = enqueue_nonlin(c);
+  if (r) return r;
+  return collect_cfl(c);
+}
+
+extern "C" int sgpu_linear(sgpu_ctx* c) {
+  if (!c) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  return enqueue_linear(c);
+}
+
+extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
+  if (!c || nsub < 0) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  for (int s = 0; s < nsub; ++s) {
+    // the CFL word is read back lazily (sgpu_get_scalars): no host sync per substep
+    int r = enqueue_nonlin(c);
+    if (r) return r;
+    r = enqueue_linear(c);
+    if (r) return r;
+  }
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_get_scalars(sgpu_ctx* c, double* out, int n) {
+  if (!c || !out) return SGPU_E_PARAM;
+  int r = collect_cfl(c);
+  double sc[4];
+  CK(cudaMemcpyAsync(sc, c->scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const double v[12] = {sc[0], sc[1], c->t, c->cfl, c->an, c->bn, c->anp1, c->bnp1, c->cnp1, (double)c->it, c->tc, c->dtn};
+  for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
+  return r;
+}
+
+extern "C" int sgpu_event_record(sgpu_ctx* c, int slot_) {
+  if (!c || slot_ < 0 || slot_ >= 16) return SGPU_E_PARAM;
+  CK(cudaEventRecord(c->ev[slot_], c->stream));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_event_elapsed(sgpu_ctx* c, int a, int b, float* ms) {
+  if (!c || !ms || a < 0 || b < 0 || a >= 16 || b >= 16) return SGPU_E_PARAM;
+  CK(cudaEventSynchronize(c->ev[b]));
+  CK(cudaEventElapsedTime(ms, c->ev[a], c->ev[b]));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_sync(sgpu_ctx* c) {
+  if (!c) return SGPU_E_PARAM;
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+extern "C" long long sgpu_launch_count(sgpu_ctx* c) { return c ? c->launches : -1; }
+
+extern "C" int sgpu_host_alloc(unsigned long long bytes, void** ptr) {
+  if (!ptr) return SGPU_E_PARAM;
+  *ptr = nullptr;
+  CK(cudaHostAlloc(ptr, (size_t)bytes, cudaHostAllocDefault));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_host_free(void* ptr) {
+  if (ptr) CK(cudaFreeHost(ptr));
+  return SGPU_OK;
+}
+
+// Per-kernel timing: when enabled, an event is recorded before every launch
+// and the time to the next event is attributed to that kernel.
+extern "C" int sgpu_profile(sgpu_ctx* c, int enable) {
+  if (!c) return SGPU_E_PARAM;
+  if (enable && c->pev.empty()) {
+    c->pev.resize(8192);
+    c->pid.resize(8192);
+    for (auto& e : c->pev) CK(cudaEventCreate(&e));
+  }
+  c->prof = enable != 0;
+  c->pnext = 0;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_profile_read(sgpu_ctx* c, double* ms, int* count, int n) {
+  if (!c || !ms || !count) return SGPU_E_PARAM;
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) { ms[i] = 0.0; count[i] = 0; }
+  for (int i = 0; i + 1 < c->pnext; ++i) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->pev[i], c->pev[i + 1]));
+    const int id = c->pid[i];
+    if (id < n) { ms[id] += t; count[id] += 1; }
+  }
+  c->pnext = 0;
+  return SGPU_OK;
+}

@@ -1,0 +1,207 @@
+// Step 2 of the RK substep: the nonlinear term H = u x omega in physical space
+// (the work bla/nonlinbl.f does plane by plane).
+//
+//   k_zinv : per xz-plane and block of kx columns: read u, v, w, omega_x,
+//            omega_z (and form omega_y = i beta u - i alpha w) from the
+//            spectral state, zero-pad kz 2/3 -> 3/2 grid (pad folded into the
+//            load: the zero band and the oddball mode are never read), inverse
+//            complex FFT over z.
+//   k_xpass: per xz-plane and block of z rows: Hermitian-complete two fields
+//            per complex FFT (u+iv, w+i omega_x, omega_y+i omega_z), inverse
+//            FFT over x, form H and the CFL number in registers, forward FFT
+//            of (H1+iH2) and H3, split the spectra and keep kx < nx/2.
+//   k_zfwd : forward complex FFT over z, keep the nz stored kz modes
+//            (truncation folded into the store) and write H into state slots
+//            1-3, exactly where the reference's putxz puts it.
+//
+// Normalisation follows the reference: synthesis and analysis are both
+// unnormalised, so H carries the factor nxp*nzp that the Chebyshev transform
+// of step 3 removes.
+#pragma once
+#include "fft.cuh"
+#include "layout.cuh"
+
+namespace sb {
+
+template <class T>
+__global__ void k_zinv(const double2* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
+                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
+                       const double* __restrict__ alfa, const double* __restrict__ beta, int KB) {
+  typedef typename C2<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* b0 = reinterpret_cast<V*>(smem_raw);
+  V* b1 = b0 + (size_t)g.nzp * KB;
+  const int y = blockIdx.y;
+  const int kx0 = blockIdx.x * KB;
+  const int nzh = g.nz / 2;
+  const size_t slot = (size_t)g.nyp * g.NP;
+  // fine-grid fields: 0 u, 1 v, 2 w, 3 omega_x, 4 omega_y, 5 omega_z
+  const int src_slot[6] = {0, 1, 2, 3, -1, 4};
+  for (int f = 0; f < 6; ++f) {
+    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int b = t - m * KB;
+      const int kx = kx0 + b;
+      int iz = -1;
+      if (m < nzh)
+        iz = m;
+      else if (m > g.nzp - nzh)
+        iz = m - (g.nzp - g.nz);
+      V val = V{(T)0, (T)0};
+      if (iz >= 0 && kx < g.nx2) {
+        const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
+        if (f == 4) {
+          const double2 u = st[off];
+          const double2 w = st[2 * slot + off];
+          const double a = alfa[kx], be = beta[iz];
+          val = V{(T)(-be * u.y + a * w.y), (T)(be * u.x - a * w.x)};
+        } else {
+          const double2 q = st[src_slot[f] * slot + off];
+          val = V{(T)q.x, (T)q.y};
+        }
+      }
+      b0[t] = val;
+    }
+    __syncthreads();
+    V* res = fft_columns<T>(b0, b1, KB, plan, tw, +1);
+    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int b = t - m * KB;
+      const int kx = kx0 + b;
+      if (kx < g.nx2) zb[(((size_t)f * g.nyp + y) * g.nzp + m) * g.nx2 + kx] = res[t];
+    }
+    __syncthreads();
+  }
+}
+
+// CFL accumulator: non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <class T>
+__global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb,
+                        Dims g, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
+                        const double* __restrict__ dyi, double dxi, double dzi, double rot, int RB,
+                        unsigned long long* __restrict__ cfl_bits) {
+  typedef typename C2<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int B = 3 * RB;
+  V* bA = reinterpret_cast<V*>(smem_raw);
+  V* bB = bA + (size_t)g.nxp * B;
+  const int y = blockIdx.y;
+  const int m0 = blockIdx.x * RB;
+  const int n = g.nxp;
+  // Hermitian completion of two half spectra into one complex spectrum
+  for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
+    const int k = t / B;
+    const int c = t - k * B;
+    const int r = c / 3, q = c - 3 * (c / 3);
+    const int m = m0 + r;
+    V z = V{(T)0, (T)0};
+    if (m < g.nzp) {
+      const size_t f0 = (((size_t)(2 * q) * g.nyp + y) * g.nzp + m) * g.nx2;
+      const size_t f1 = (((size_t)(2 * q + 1) * g.nyp + y) * g.nzp + m) * g.nx2;
+      if (k == 0) {
+        z = V{zb[f0].x, zb[f1].x};
+      } else if (k < g.nx2) {
+        const V a = zb[f0 + k], b = zb[f1 + k];
+        z = V{a.x - b.y, a.y + b.x};
+      } else if (k > n - g.nx2) {
+        const int kk = n - k;
+        const V a = zb[f0 + kk], b = zb[f1 + kk];
+        z = V{a.x + b.y, b.x - a.y};
+      }
+    }
+    bA[t] = z;
+  }
+  __syncthreads();
+  V* res = fft_columns<T>(bA, bB, B, plan, tw, +1);
+  V* oth = (res == bA) ? bB : bA;
+  // products in physical space, H into (H1 + i H2, H3 + 0i), CFL
+  const int B2 = 2 * RB;
+  double cmax = 0.0;
+  const double dy = dyi[y];
+  const T r2 = (T)(2.0 * rot);
+  for (int t = threadIdx.x; t < n * RB; t += blockDim.x) {
+    const int j = t / RB;
+    const int r = t - j * RB;
+    const V z0 = res[j * B + 3 * r + 0];
+    const V z1 = res[j * B + 3 * r + 1];
+    const V z2 = res[j * B + 3 * r + 2];
+    const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
+    const T h1 = v * (oz + r2) - w * oy;
+    const T h2 = w * ox - u * (oz + r2);
+    const T h3 = u * oy - v * ox;
+    oth[j * B2 + 2 * r + 0] = V{h1, h2};
+    oth[j * B2 + 2 * r + 1] = V{h3, (T)0};
+    if (m0 + r < g.nzp) {
+      const double cl = fabs((double)u) * dxi + fabs((double)v) * dy + fabs((double)w) * dzi;
+      cmax = fmax(cmax, cl);
+    }
+  }
+  __syncthreads();
+  V* fres = fft_columns<T>(oth, res, B2, plan, tw, -1);
+  for (int t = threadIdx.x; t < g.nx2 * RB; t += blockDim.x) {
+    const int k = t / RB;
+    const int r = t - k * RB;
+    const int m = m0 + r;
+    if (m >= g.nzp) continue;
+    const V a = fres[k * B2 + 2 * r];
+    const V b = fres[((n - k) % n) * B2 + 2 * r];
+    const V h3 = fres[k * B2 + 2 * r + 1];
+    const V h1 = V{(a.x + b.x) * (T)0.5, (a.y - b.y) * (T)0.5};
+    const V h2 = V{(a.y + b.y) * (T)0.5, (b.x - a.x) * (T)0.5};
+    const size_t o = ((size_t)y * g.nzp + m) * g.nx2 + k;
+    const size_t fs = (size_t)g.nyp * g.nzp * g.nx2;
+    xb[o] = h1;
+    xb[fs + o] = h2;
+    xb[2 * fs + o] = h3;
+  }
+  // block max of the CFL number
+  for (int off = 16; off > 0; off >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
+  __shared__ double wmax[32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = cmax;
+  __syncthreads();
+  if (threadIdx.x == 0 && cfl_bits != nullptr) {
+    double mx = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) mx = fmax(mx, wmax[i]);
+    atomic_max_nonneg(cfl_bits, mx);
+  }
+}
+
+template <class T>
+__global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, double2* __restrict__ st, Dims g,
+                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw, int KB) {
+  typedef typename C2<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* b0 = reinterpret_cast<V*>(smem_raw);
+  V* b1 = b0 + (size_t)g.nzp * KB;
+  const int y = blockIdx.y;
+  const int kx0 = blockIdx.x * KB;
+  const int nzh = g.nz / 2;
+  const size_t fs = (size_t)g.nyp * g.nzp * g.nx2;
+  const size_t slot = (size_t)g.nyp * g.NP;
+  for (int f = 0; f < 3; ++f) {
+    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int b = t - m * KB;
+      const int kx = kx0 + b;
+      b0[t] = (kx < g.nx2) ? xb[f * fs + ((size_t)y * g.nzp + m) * g.nx2 + kx] : V{(T)0, (T)0};
+    }
+    __syncthreads();
+    V* res = fft_columns<T>(b0, b1, KB, plan, tw, -1);
+    for (int t = threadIdx.x; t < g.nz * KB; t += blockDim.x) {
+      const int iz = t / KB;
+      const int b = t - iz * KB;
+      const int kx = kx0 + b;
+      if (kx >= g.nx2) continue;
+      const int m = (iz < nzh) ? iz : iz + (g.nzp - g.nz);
+      const V h = res[m * KB + b];
+      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = double2{(double)h.x, (double)h.y};
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace sb

@@ -1,0 +1,447 @@
+// Step 3 of the RK substep: implicit Chebyshev-tau solves per (kx,kz) pencil
+// (the work bla/linearbl.f does per xy-plane), plus the startup partial
+// right-hand side (bla/prhs.f).
+//
+// Chebyshev transforms (k_cheb): physical <-> Chebyshev along y as a DCT-I of
+// length N+1 (N = ny-1), computed as a complex FFT of the even extension of
+// length 2N in shared memory over a tile of PB pencils.  Conventions are the
+// reference's (bla/cvecfft_acc.f vchbf/vchbb with the normalisation of
+// linearbl.f:262): a_k = 2/(N cbar_k) sum_j u_j cos(pi jk/N)/cbar_j,
+// u_j = sum_k a_k cos(pi jk/N), cbar_0 = cbar_N = 2, else 1.
+//
+// Pencil algebra (k_pencil, one thread per complex pencil, columns strided by
+// NP so a warp's accesses coalesce): the tau method of Canuto et al. for
+// (D^2 - lambda) psi = f (bla/setmacrhs.f, bla/trid.f:120-200), the
+// velocity-vorticity recovery and the next partial right-hand side, in the
+// order linearbl.f:257-1860 uses for the channel (ibc = 0, tau).
+#pragma once
+#include "fft.cuh"
+#include "layout.cuh"
+
+namespace sb {
+
+struct Col {
+  double* a;
+  size_t s;
+  __device__ __forceinline__ double& operator[](int j) const { return a[(size_t)j * s]; }
+};
+
+__device__ __forceinline__ Col col_re(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p, 2 * (size_t)NP}; }
+__device__ __forceinline__ Col col_im(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p + 1, 2 * (size_t)NP}; }
+__device__ __forceinline__ Col col_r(double* arr, int p, int NP) { return Col{arr + p, (size_t)NP}; }
+
+// Chebyshev derivative: b = D a, by the backward recurrence
+// b_j = b_{j+2} + 2(j+1) a_{j+1}, b_{n-1} = 0, b_0 halved (bla/dcheb.f).
+__device__ void cheb_deriv(Col b, Col a, int n) {
+  double bp2 = 2.0 * (double)(n - 1) * a[n - 1];  // b[n-2]
+  double bp1 = 2.0 * (double)(n - 2) * a[n - 2];  // b[n-3]
+  b[n - 2] = bp2;
+  b[n - 3] = bp1;
+  for (int j = n - 4; j >= 0; --j) {
+    const double v = bp2 + 2.0 * (double)(j + 1) * a[j + 1];
+    bp2 = bp1;
+    bp1 = v;
+    b[j] = v;
+  }
+  b[n - 1] = 0.0;
+  b[0] = 0.5 * b[0];
+}
+
+// Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
+// (1-based row index i as in bla/setmacrhs.f).
+__device__ __forceinline__ double tau_c(int i, double lam) {
+  return (i == 1) ? -0.25 * lam : (-0.25 / ((double)i * ((double)i + 1.0))) * lam;
+}
+__device__ __forceinline__ double tau_d(int i, double lam) {
+  return 1.0 + (0.5 / ((double)i * ((double)i + 2.0))) * lam;
+}
+__device__ __forceinline__ double tau_e(int i, double lam) {
+  return (-0.25 / (((double)i + 1.0) * ((double)i + 2.0))) * lam;
+}
+
+// Tau right-hand side of row i (3 <= i <= n, 1-based) from f: the
+// Chebyshev-coefficient form of u'' = f + lam u, truncated at n modes.
+__device__ __forceinline__ double tau_rhs(const Col& f, int i, int n) {
+  if (f.a == nullptr) return 0.0;
+  auto F = [&](int k) { return f[k - 1]; };
+  const double di = (double)i;
+  if (i == 3) return 0.25 * F(1) + F(5) / 24.0 - F(3) / 6.0;
+  double r = (0.25 / ((di - 2.0) * (di - 1.0))) * F(i - 2);
+  if (i <= n - 2) r += (-0.5 / ((di - 2.0) * di)) * F(i);
+  if (i <= n - 4) r += (0.25 / ((di - 1.0) * di)) * F(i + 2);
+  return r;
+}
+
+// Solve (D^2 - lam) x_q = f_q, q < m, by the Chebyshev tau method with the
+// boundary rows  sum_{k even} x_k = bc1[q],  sum_{k odd} x_k = bc2[q]
+// (i.e. x(+1) = bc1+bc2, x(-1) = bc1-bc2).  Elimination order follows
+// bla/trid.f:120-200: upper off-diagonal from the top, the two full rows
+// through the weights W, then the lower off-diagonal upwards.
+// cp, wt: per-pencil scratch columns (n entries each).
+template <int M>
+__device__ void tau_solve(double lam, int n, const Col* f, const Col* x, const double* bc1, const double* bc2,
+                          Col cp, Col wt) {
+  // setmacrhs: rows 3..n
+  for (int q = 0; q < M; ++q)
+    for (int i = 3; i <= n; ++i) x[q][i - 1] = tau_rhs(f[q], i, n);
+  // factor: wt <- 1/d', cp <- c' = c/d'
+  {
+    const double a5 = 1.0 / tau_d(n - 5, lam);
+    cp[n - 6] = tau_c(n - 5, lam) * a5;
+    wt[n - 6] = a5;
+    const double a4 = 1.0 / tau_d(n - 4, lam);
+    cp[n - 5] = tau_c(n - 4, lam) * a4;
+    wt[n - 5] = a4;
+    for (int i = n - 6; i >= 1; --i) {
+      const double di = 1.0 / (tau_d(i, lam) - cp[i + 1] * tau_e(i, lam));
+      cp[i - 1] = tau_c(i, lam) * di;
+      wt[i - 1] = di;
+    }
+    cp[n - 4] = tau_c(n - 3, lam);
+    cp[n - 3] = tau_c(n - 2, lam);
+  }
+  // eliminate the upper off-diagonal in every right-hand side
+  for (int q = 0; q < M; ++q) {
+    const Col X = x[q];
+    X[n - 4] = X[n - 4] * wt[n - 6];
+    X[n - 3] = X[n - 3] * wt[n - 5];
+    for (int i = n - 4; i >= 3; --i) X[i - 1] = (X[i - 1] - X[i + 1] * tau_e(i - 2, lam)) * wt[i - 3];
+  }
+  // weights of the two full (boundary) rows
+  wt[n - 4] = 1.0 - cp[n - 4];
+  wt[n - 3] = 1.0 - cp[n - 3];
+  for (int i = n - 4; i >= 3; --i) wt[i - 1] = 1.0 - cp[i - 1] * wt[i + 1];
+  const double d1 = 1.0 / (1.0 - cp[0] * wt[2]);
+  const double d2 = 1.0 / (1.0 - cp[1] * wt[3]);
+  for (int q = 0; q < M; ++q) {
+    const Col X = x[q];
+    double x1 = bc1[q] - X[n - 1];
+    double x2 = bc2[q] - X[n - 2];
+    for (int i = 5; i <= n - 2; i += 2) {
+      x1 = x1 - X[i - 1] * wt[i - 1];
+      x2 = x2 - X[i - 2] * wt[i - 2];
+    }
+    X[0] = (x1 - X[2] * wt[2]) * d1;
+    X[1] = x2 * d2;
+    for (int i = 3; i <= n; ++i) X[i - 1] = X[i - 1] - cp[i - 3] * X[i - 3];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Chebyshev transforms over pencils
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __restrict__ out, size_t out_fs,
+                       Dims g, int inverse, double scale, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
+                       int PB, int skip_oddball) {
+  typedef typename C2<T>::type V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = g.nyp;
+  const int N = n - 1;
+  const int L = 2 * N;
+  V* b0 = reinterpret_cast<V*>(smem_raw);
+  V* b1 = b0 + (size_t)L * PB;
+  const int f = blockIdx.y;
+  const int p0 = blockIdx.x * PB;
+  const double2* src = in + f * in_fs;
+  double2* dst = out + f * out_fs;
+  for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
+    const int j = t / PB;
+    const int b = t - j * PB;
+    const int p = p0 + b;
+    double2 v = (p < g.NP) ? src[(size_t)j * g.NP + p] : double2{0.0, 0.0};
+    if (inverse) {
+      const double cb = (j == 0 || j == N) ? 1.0 : 0.5;
+      v.x *= cb;
+      v.y *= cb;
+    }
+    const V w = V{(T)v.x, (T)v.y};
+    b0[j * PB + b] = w;
+    if (j >= 1 && j <= N - 1) b0[(L - j) * PB + b] = w;
+  }
+  __syncthreads();
+  V* res = fft_columns<T>(b0, b1, PB, plan, tw, -1);
+  for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
+    const int k = t / PB;
+    const int b = t - k * PB;
+    const int p = p0 + b;
+    if (p >= g.NP) continue;
+    if (skip_oddball && (p / g.nx2) == g.zodd) continue;
+    const V e = res[k * PB + b];
+    double fac = scale;
+    if (!inverse) fac = scale / ((double)N * ((k == 0 || k == N) ? 2.0 : 1.0));
+    dst[(size_t)k * g.NP + p] = double2{(double)e.x * fac, (double)e.y * fac};
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-pencil solve of one substep (all pencils except kx=kz=0 and the oddball)
+// ---------------------------------------------------------------------------
+struct PencilBufs {
+  double2 *H1, *H2, *H3;          // Chebyshev nonlinear term (normalised)
+  double2 *PV, *PW;               // state slots 6,7 (partial RHS, Chebyshev), updated in place
+  double2 *G, *DG, *HV, *HOM, *FV, *FW, *PHI, *OM, *V, *DV, *DOM, *T1, *T2;
+  double2 *OU, *OV, *OW, *OX, *OZ;  // outputs (Chebyshev)
+  double *PHIH, *VH, *DVH, *CP, *WT;
+};
+
+struct RKc {
+  double an, bn, anp1, bnp1;
+};
+
+__global__ void k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa, const double* __restrict__ beta,
+                         double re, RKc rk) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.NP) return;
+  const int kx = p % g.nx2;
+  const int iz = p / g.nx2;
+  if (iz == g.zodd || p == 0) return;
+  const int n = g.nyp;
+  const int NP = g.NP;
+  const double a = alfa[kx], be = beta[iz];
+  const double k2 = a * a + be * be;
+  const double k2i = 1.0 / k2;
+  const double lam = k2 + 2.0 * re / (rk.an + rk.bn);
+  const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
+  auto at = [&](double2* arr, int j) -> double2& { return arr[(size_t)j * NP + p]; };
+
+  // nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340)
+  for (int j = 0; j < n; ++j) {
+    const double2 h1 = at(B.H1, j), h3 = at(B.H3, j);
+    at(B.G, j) = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
+    const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
+    at(B.HOM, j) = hom;
+    const double2 pw = at(B.PW, j);
+    at(B.FW, j) = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
+  }
+  cheb_deriv(col_re(B.DG, p, NP), col_re(B.G, p, NP), n);
+  cheb_deriv(col_im(B.DG, p, NP), col_im(B.G, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 dg = at(B.DG, j), h2 = at(B.H2, j), pv = at(B.PV, j);
+    const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
+    at(B.HV, j) = hv;
+    at(B.FV, j) = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
+  }
+  // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
+  {
+    const Col f[5] = {col_re(B.FV, p, NP), col_im(B.FV, p, NP), col_re(B.FW, p, NP), col_im(B.FW, p, NP), Col{nullptr, 0}};
+    const Col x[5] = {col_re(B.PHI, p, NP), col_im(B.PHI, p, NP), col_re(B.OM, p, NP), col_im(B.OM, p, NP), col_r(B.PHIH, p, NP)};
+    const double bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
+    tau_solve<5>(lam, n, f, x, bc1, bc2, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
+  }
+  // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001)
+  {
+    const Col f[3] = {col_re(B.PHI, p, NP), col_im(B.PHI, p, NP), col_r(B.PHIH, p, NP)};
+    const Col x[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
+    const double bc1[3] = {0, 0, 0}, bc2[3] = {0, 0, 0};
+    tau_solve<3>(k2, n, f, x, bc1, bc2, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
+  }
+  // dv/dy = 0 at the walls: add the homogeneous solution per parity (linearbl.f:1020-1085)
+  cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
+  cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
+  cheb_deriv(col_r(B.DVH, p, NP), col_r(B.VH, p, NP), n);
+  double cvr[2], cvi[2];
+  for (int is = 0; is < 2; ++is) {
+    double sr = 0.0, si = 0.0, sh = 0.0;
+    for (int j = is; j < n; j += 2) {
+      const double2 dv = at(B.DV, j);
+      sr = sr + dv.x;
+      si = si + dv.y;
+      sh = sh + B.DVH[(size_t)j * NP + p];
+    }
+    const double cinv = 1.0 / sh;
+    cvr[1 - is] = (0.0 - sr) * cinv;
+    cvi[1 - is] = (0.0 - si) * cinv;
+  }
+  for (int j = 0; j < n; ++j) {
+    const double vh = B.VH[(size_t)j * NP + p];
+    const double2 v = at(B.V, j);
+    at(B.V, j) = double2{v.x + cvr[j & 1] * vh, v.y + cvi[j & 1] * vh};
+  }
+  // phi from the final v (tau: phi = D^2 v - k^2 v), derivatives (linearbl.f:1160-1170)
+  cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
+  cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.DV, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.DV, p, NP), n);
+  cheb_deriv(col_re(B.DOM, p, NP), col_re(B.OM, p, NP), n);
+  cheb_deriv(col_im(B.DOM, p, NP), col_im(B.OM, p, NP), n);
+  // u, w, omega_x, omega_z (linearbl.f:1193-1212)
+  for (int j = 0; j < n; ++j) {
+    const double2 v = at(B.V, j), t1 = at(B.T1, j);
+    const double2 phi = double2{t1.x - k2 * v.x, t1.y - k2 * v.y};
+    at(B.PHI, j) = phi;
+    const double2 dv = at(B.DV, j), om = at(B.OM, j), dom = at(B.DOM, j);
+    at(B.OU, j) = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
+    at(B.OW, j) = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
+    at(B.OZ, j) = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
+    at(B.OX, j) = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
+    at(B.OV, j) = v;
+  }
+  // partial right-hand sides of the next stage (linearbl.f:1696-1800, tau branch)
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.PHI, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.PHI, p, NP), n);
+  cheb_deriv(col_re(B.T2, p, NP), col_re(B.T1, p, NP), n);
+  cheb_deriv(col_im(B.T2, p, NP), col_im(B.T1, p, NP), n);
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.DOM, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.DOM, p, NP), n);
+  const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
+  const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
+  const double k2m = k2 - c1n;
+  for (int j = 0; j < n; ++j) {
+    const double2 d2phi = at(B.T2, j), phi = at(B.PHI, j), hv = at(B.HV, j);
+    const double2 d2om = at(B.T1, j), om = at(B.OM, j), hom = at(B.HOM, j);
+    at(B.PV, j) = double2{-d2phi.x + k2m * phi.x - c2 * hv.x, -d2phi.y + k2m * phi.y - c2 * hv.y};
+    at(B.PW, j) = double2{-d2om.x + k2m * om.x - c2 * hom.x, -d2om.y + k2m * om.y - c2 * hom.y};
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kx = kz = 0: mean flow with the constant-flux pressure gradient
+// (linearbl.f:1214-1470 tau branch, ibc = 0; next partial RHS :1712-1733)
+// One thread; FP64.  scratch: 12 columns of n doubles.
+// ---------------------------------------------------------------------------
+struct MeanArgs {
+  double2 *H1, *H3;        // Chebyshev nonlinear term
+  double *puw;             // [2][ny] partial RHS of the mean flow
+  double *scal;            // [0] px, [1] mflux
+  double *scr;             // scratch
+  double2 *OU, *OV, *OW, *OX, *OZ, *PV, *PW;
+  int cflux;
+};
+
+__global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int n = g.nyp;
+  const int NP = g.NP;
+  Col huw1{A.scr + 0 * n, 1}, huw2{A.scr + 1 * n, 1}, fu{A.scr + 2 * n, 1}, fw{A.scr + 3 * n, 1};
+  Col U{A.scr + 4 * n, 1}, W{A.scr + 5 * n, 1}, DU{A.scr + 6 * n, 1}, DW{A.scr + 7 * n, 1};
+  Col cp{A.scr + 8 * n, 1}, wt{A.scr + 9 * n, 1}, t1{A.scr + 10 * n, 1}, t2{A.scr + 11 * n, 1};
+  const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
+  double px = A.scal[0];
+  const double mflux = A.scal[1];
+  for (int j = 0; j < n; ++j) {
+    huw1[j] = A.H1[(size_t)j * NP].x;
+    huw2[j] = A.H3[(size_t)j * NP].x;
+    fu[j] = A.puw[j] - c1 * huw1[j];
+    fw[j] = A.puw[n + j] - c1 * huw2[j];
+  }
+  fu[0] = fu[0] + 2.0 * re * px;
+  const double lam = 0.0 + 2.0 * re / (rk.an + rk.bn);
+  const double bz[1] = {0.0};
+  {
+    const Col f[2] = {fu, fw};
+    const Col x[2] = {U, W};
+    const double b0[2] = {0.0, 0.0};
+    tau_solve<2>(lam, n, f, x, b0, b0, cp, wt);
+  }
+  if (A.cflux) {
+    double m1 = 0.0;
+    for (int j = 0; j < n; j += 2) m1 = m1 - U[j] * 2.0 / (double)(j * j - 1);
+    fu[0] = fu[0] + 2.0 * re * px;
+    tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
+    double m2 = 0.0;
+    for (int j = 0; j < n; j += 2) m2 = m2 - U[j] * 2.0 / (double)(j * j - 1);
+    fu[0] = fu[0] - 4.0 * re * px;
+    px = px * (1.0 + (mflux - m1) / (m2 - m1));
+    fu[0] = fu[0] + 2.0 * re * px;
+    tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
+    A.scal[0] = px;
+  }
+  cheb_deriv(DU, U, n);
+  cheb_deriv(DW, W, n);
+  for (int j = 0; j < n; ++j) {
+    A.OU[(size_t)j * NP] = double2{U[j], 0.0};
+    A.OW[(size_t)j * NP] = double2{W[j], 0.0};
+    A.OV[(size_t)j * NP] = double2{0.0, 0.0};
+    A.OX[(size_t)j * NP] = double2{DW[j], 0.0};
+    A.OZ[(size_t)j * NP] = double2{-DU[j], 0.0};
+    A.PV[(size_t)j * NP] = double2{0.0, 0.0};
+    A.PW[(size_t)j * NP] = double2{0.0, 0.0};
+  }
+  const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
+  const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
+  cheb_deriv(t1, DU, n);
+  cheb_deriv(t2, DW, n);
+  for (int j = 0; j < n; ++j) {
+    A.puw[j] = -t1[j] - c1n * U[j] - c2 * huw1[j];
+    A.puw[n + j] = -t2[j] - c1n * W[j] - c2 * huw2[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// startup partial right-hand side and vorticities (bla/prhs.f), all pencils
+// ---------------------------------------------------------------------------
+struct PrhsBufs {
+  double2 *U1, *U2, *U3;    // Chebyshev velocities
+  double2 *OMY, *OX, *OZ, *PHI, *T1, *T2;
+  double2 *PV, *PW;         // state slots 6,7
+  double *puw;
+};
+
+__global__ void k_prhs(PrhsBufs B, Dims g, const double* __restrict__ alfa, const double* __restrict__ beta,
+                       double re, double an) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.NP) return;
+  const int kx = p % g.nx2;
+  const int iz = p / g.nx2;
+  const int n = g.nyp;
+  const int NP = g.NP;
+  const double a = alfa[kx], be = beta[iz];
+  const double k2 = a * a + be * be;
+  const double lam = k2 - 2.0 * re / an;
+  auto at = [&](double2* arr, int j) -> double2& { return arr[(size_t)j * NP + p]; };
+  for (int j = 0; j < n; ++j) {
+    const double2 u1 = at(B.U1, j), u3 = at(B.U3, j);
+    at(B.OMY, j) = double2{-u1.y * be + u3.y * a, u1.x * be - u3.x * a};
+  }
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.U3, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.U3, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 t = at(B.T1, j), u2 = at(B.U2, j);
+    at(B.OX, j) = double2{t.x + u2.y * be, t.y - u2.x * be};
+  }
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.U1, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.U1, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 t = at(B.T1, j), u2 = at(B.U2, j);
+    at(B.OZ, j) = double2{-t.x - u2.y * a, -t.y + u2.x * a};
+  }
+  // phi = D^2 v - k^2 v
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.U2, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.U2, p, NP), n);
+  cheb_deriv(col_re(B.T2, p, NP), col_re(B.T1, p, NP), n);
+  cheb_deriv(col_im(B.T2, p, NP), col_im(B.T1, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 t = at(B.T2, j), u2 = at(B.U2, j);
+    at(B.PHI, j) = double2{t.x - k2 * u2.x, t.y - k2 * u2.y};
+  }
+  // p_omega = -D^2 omega_y + lam omega_y
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.OMY, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.OMY, p, NP), n);
+  cheb_deriv(col_re(B.T2, p, NP), col_re(B.T1, p, NP), n);
+  cheb_deriv(col_im(B.T2, p, NP), col_im(B.T1, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 t = at(B.T2, j), om = at(B.OMY, j);
+    at(B.PW, j) = double2{-t.x + lam * om.x, -t.y + lam * om.y};
+  }
+  // p_v = -D^2 phi + lam phi
+  cheb_deriv(col_re(B.T1, p, NP), col_re(B.PHI, p, NP), n);
+  cheb_deriv(col_im(B.T1, p, NP), col_im(B.PHI, p, NP), n);
+  cheb_deriv(col_re(B.T2, p, NP), col_re(B.T1, p, NP), n);
+  cheb_deriv(col_im(B.T2, p, NP), col_im(B.T1, p, NP), n);
+  for (int j = 0; j < n; ++j) {
+    const double2 t = at(B.T2, j), ph = at(B.PHI, j);
+    at(B.PV, j) = double2{-t.x + lam * ph.x, -t.y + lam * ph.y};
+  }
+  if (p == 0) {
+    // mean flow partial RHS: -2 Re/an U - D^2 U (prhs.f, zb = 1)
+    cheb_deriv(col_re(B.T1, 0, NP), col_re(B.U1, 0, NP), n);
+    cheb_deriv(col_re(B.T2, 0, NP), col_re(B.T1, 0, NP), n);
+    for (int j = 0; j < n; ++j) B.puw[j] = -2.0 * re / an * at(B.U1, j).x - at(B.T2, j).x;
+    cheb_deriv(col_re(B.T1, 0, NP), col_re(B.U3, 0, NP), n);
+    cheb_deriv(col_re(B.T2, 0, NP), col_re(B.T1, 0, NP), n);
+    for (int j = 0; j < n; ++j) B.puw[n + j] = -2.0 * re / an * at(B.U3, j).x - at(B.T2, j).x;
+  }
+}
+
+}  // namespace sb
