@@ -90,13 +90,18 @@ def generate_c(nx: int, ny: int, nz: int) -> str:
                      skip_units=("fft_identify",), provided=("stopnow",))
 
 
-def lib_path(nx: int, ny: int, nz: int) -> str:
-    return os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}", "libsimson_ref.so")
+def lib_path(nx: int, ny: int, nz: int, fma: bool = False) -> str:
+    return os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}" + ("_fma" if fma else ""), "libsimson_ref.so")
 
 
-def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False) -> str:
-    """Translate + compile the reference for one grid; returns the .so path."""
-    out_dir = os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}")
+def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False, fma: bool = False) -> str:
+    """Translate + compile the reference for one grid; returns the .so path.
+
+    fma=True builds a second copy with fused multiply-add contraction
+    (-mfma -ffp-contract=fast): the same reference with roundoff-level
+    different arithmetic, used to measure how far the reference agrees with
+    itself."""
+    out_dir = os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}" + ("_fma" if fma else ""))
     so = os.path.join(out_dir, "libsimson_ref.so")
     harness = os.path.join(HERE, "ref_harness.c")
     translator = os.path.join(HERE, "f77c.py")
@@ -119,9 +124,9 @@ def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False)
     gen = os.path.join(out_dir, "ref_gen.c")
     with open(gen, "w") as f:
         f.write(csrc)
+    fp = ["-mfma", "-ffp-contract=fast"] if fma else ["-ffp-contract=off"]
     cmd = ["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", "-w", "-std=gnu11",
-           "-fno-fast-math", "-ffp-contract=off", "-I", out_dir,
-           "-o", so + ".tmp", harness, "-lm"]
+           "-fno-fast-math"] + fp + ["-I", out_dir, "-o", so + ".tmp", harness, "-lm"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -19,11 +19,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _lib(nx, ny, nz, build=True):
+def _lib(nx, ny, nz, build=True, fma=False):
     import sys
     sys.path.insert(0, HERE)
     from build_ref import build as _build, lib_path
-    path = _build(nx, ny, nz) if build else lib_path(nx, ny, nz)
+    path = _build(nx, ny, nz, fma=fma) if build else lib_path(nx, ny, nz, fma=fma)
     if not os.path.exists(path):
         raise FileNotFoundError(path)
     lib = ctypes.CDLL(path)
@@ -45,8 +45,8 @@ def _dp(a):
 class RefSim:
     """The reference channel time stepper (temporal channel, RK3/CN, cflux)."""
 
-    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True):
-        self.lib = _lib(nx, ny, nz, build)
+    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True, fma=False):
+        self.lib = _lib(nx, ny, nz, build, fma)
         dims = (ctypes.c_int * 12)()
         self.lib.sref_dims(dims)
         self.dims = list(dims)

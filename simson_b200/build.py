@@ -36,7 +36,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    # The FP64 path is built without FMA contraction: the reference's
+    # arithmetic (gfortran/gcc for x86-64) rounds every product, and the stiff
+    # tau solves (lambda ~ 1e6) amplify the difference between fused and
+    # separate rounding to ~1e-12.  Set SIMSON_FMAD=1 to allow contraction.
+    fmad = "true" if os.environ.get("SIMSON_FMAD") == "1" else "false"
+    cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", f"-fmad={fmad}", "-Xcompiler", "-fPIC", "-shared",
            "--expt-relaxed-constexpr", "-o", LIB + ".tmp"] + SOURCES
     if verbose:
         print(" ".join(cmd))

@@ -1,0 +1,66 @@
+"""Step 2 and step 3 checked one at a time: both sides start each step from
+the oracle's own state, so each kernel chain is compared without the other's
+roundoff feeding in."""
+import numpy as np
+import pytest
+
+from simson_b200.fields import channel_field
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def setup(grid, need_ref, seed=5, rms=0.05):
+    nx, ny, nz = grid
+    need_ref(nx, ny, nz)
+    from refsim import RefSim
+    from simson_b200.bla import Channel
+    xl, zl = 4 * np.pi, 2 * np.pi
+    u, v, w = channel_field(nx, ny, nz, xl, zl, rms, seed)
+    ref = RefSim(nx, ny, nz, 4200.0, xl, zl, 0.01)
+    ref.set_velocity(u, v, w)
+    ref.start()
+    gpu = Channel(nx, ny, nz, 4200.0, xl, zl, 0.01)
+    gpu.set_velocity(u, v, w)
+    gpu.start()
+    return ref, gpu
+
+
+def sync_gpu_to_ref(ref, gpu):
+    gpu.set_state(ref.state())
+    import ctypes
+    p = np.ascontiguousarray(ref.puw())
+    gpu._check(gpu.lib.sgpu_upload_puw(gpu._ctx, p.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "puw")
+
+
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_step2_isolated(grid, need_ref):
+    ref, gpu = setup(grid, need_ref)
+    for k in range(3):
+        sync_gpu_to_ref(ref, gpu)
+        ref.nonlin_only()
+        gpu.nonlinbl()
+        errs = [rel(gpu.get_slot(s), ref.get_slot(s)) for s in (1, 2, 3)]
+        print("step2 substep", k, errs)
+        assert max(errs) < 1e-13, errs
+        ref.linear_only()
+        gpu.linearbl()
+
+
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_step3_isolated(grid, need_ref):
+    ref, gpu = setup(grid, need_ref)
+    for k in range(3):
+        ref.nonlin_only()
+        gpu.nonlinbl()
+        sync_gpu_to_ref(ref, gpu)
+        ref.linear_only()
+        gpu.linearbl()
+        rs, gs = ref.state(), gpu.state()
+        errs = [rel(gs[s], rs[s]) for s in range(7)]
+        print("step3 substep", k, ["%.2e" % e for e in errs], "px", gpu.scalars()["px"] - ref.scalars()["px"])
+        np.testing.assert_allclose(gpu.puw(), ref.puw(), rtol=0, atol=1e-12 * np.abs(ref.puw()).max())
+        assert max(errs) < 1e-12, errs
