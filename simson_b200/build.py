@@ -50,5 +50,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+HOSTCHECK = os.path.join(LIB_DIR, "libsimson_hostcheck.so")
+
+
+def build_hostcheck(force: bool = False) -> str:
+    """Host (CPU) build of the step-3 pencil algebra for the CPU unit tests."""
+    src = os.path.join(HERE, "csrc", "hostcheck.cu")
+    if not force and os.path.exists(HOSTCHECK) and all(
+            os.path.getmtime(d) <= os.path.getmtime(HOSTCHECK) for d in DEPS + [__file__]):
+        return HOSTCHECK
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = [nvcc(), ARCH, "-O2", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
+           "-o", HOSTCHECK + ".tmp", src]
+    subprocess.run(cmd, check=True)
+    os.replace(HOSTCHECK + ".tmp", HOSTCHECK)
+    return HOSTCHECK
+
+
 if __name__ == "__main__":
     print(build(force=True, verbose=True))
+    print(build_hostcheck(force=True))

@@ -34,6 +34,9 @@ struct FFTPlan {
   int n;
   int npass;
   int radix[20];
+  int ns[20];              // sub-transform length before the pass
+  unsigned magic[20];      // ceil(2^32 / ns): j / ns == __umulhi(j, magic) for j*ns < 2^32
+  int tstep[20];           // n / (ns * radix): twiddle stride of the pass
 };
 
 // cos and sin of 2*pi/5 and 4*pi/5 (the radix-5 butterfly)
@@ -79,56 +82,62 @@ __device__ __forceinline__ void dft_small(V* v, int R, int s) {
   }
 }
 
-// One Stockham pass: src -> dst, sub-transform length Ns -> Ns*R.
-template <class T>
+// One Stockham pass: src -> dst, sub-transform length Ns -> Ns*R.  B (the
+// number of interleaved columns) is a compile-time constant so the column
+// index is a mask/shift; the only division left (by Ns) uses a precomputed
+// reciprocal.  The twiddle exponent r*jm*tstep is always below n.
+template <class T, int B, int R>
 __device__ __forceinline__ void stockham_pass(const typename C2<T>::type* __restrict__ src,
-                                              typename C2<T>::type* __restrict__ dst, int n, int B,
-                                              int R, int Ns, const typename C2<T>::type* __restrict__ tw,
-                                              int s) {
+                                              typename C2<T>::type* __restrict__ dst, int n, int Ns,
+                                              unsigned magic, int tstep,
+                                              const typename C2<T>::type* __restrict__ tw, int s) {
   typedef typename C2<T>::type V;
   const int nb = n / R;
-  const int tstep = n / (Ns * R);
   for (int t = threadIdx.x; t < nb * B; t += blockDim.x) {
     const int j = t / B;
     const int b = t - j * B;
-    const int jm = j % Ns;
+    const int jg = (Ns == 1) ? j : (int)__umulhi((unsigned)j, magic);
+    const int jm = j - jg * Ns;
     V v[5];
 #pragma unroll
-    for (int r = 0; r < 5; ++r)
-      if (r < R) v[r] = src[(j + r * nb) * B + b];
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * B + b];
     if (jm != 0) {
       const int e = jm * tstep;
 #pragma unroll
-      for (int r = 1; r < 5; ++r) {
-        if (r < R) {
-          V w = tw[(r * e) % n];
-          if (s > 0) w.y = -w.y;
-          v[r] = cmul(v[r], w);
-        }
+      for (int r = 1; r < R; ++r) {
+        V w = tw[r * e];
+        if (s > 0) w.y = -w.y;
+        v[r] = cmul(v[r], w);
       }
     }
     dft_small<T, V>(v, R, s);
-    const int base = (j / Ns) * Ns * R + jm;
+    const int base = jg * Ns * R + jm;
 #pragma unroll
-    for (int r = 0; r < 5; ++r)
-      if (r < R) dst[(base + r * Ns) * B + b] = v[r];
+    for (int r = 0; r < R; ++r) dst[(base + r * Ns) * B + b] = v[r];
   }
 }
 
 // Full transform of the B interleaved columns held in buf0; buf1 is scratch.
-// Returns the buffer holding the result.  Caller syncs before and after.
-template <class T>
+// Returns the buffer holding the result.  Caller syncs before; the function
+// ends with a barrier.
+template <class T, int B>
 __device__ typename C2<T>::type* fft_columns(typename C2<T>::type* buf0, typename C2<T>::type* buf1,
-                                            int B, const FFTPlan& plan,
-                                            const typename C2<T>::type* __restrict__ tw, int s) {
+                                            const FFTPlan& plan, const typename C2<T>::type* __restrict__ tw,
+                                            int s) {
   typename C2<T>::type* src = buf0;
   typename C2<T>::type* dst = buf1;
-  int Ns = 1;
   for (int p = 0; p < plan.npass; ++p) {
     const int R = plan.radix[p];
-    stockham_pass<T>(src, dst, plan.n, B, R, Ns, tw, s);
+    const int Ns = plan.ns[p];
+    if (R == 4)
+      stockham_pass<T, B, 4>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
+    else if (R == 2)
+      stockham_pass<T, B, 2>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
+    else if (R == 3)
+      stockham_pass<T, B, 3>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
+    else
+      stockham_pass<T, B, 5>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
     __syncthreads();
-    Ns *= R;
     typename C2<T>::type* tmp = src;
     src = dst;
     dst = tmp;

@@ -36,6 +36,8 @@ struct sgpu_ctx {
   sgpu_params prm{};
   Dims g{};
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;      // mean-flow solve, overlapped with the pencils
+  cudaEvent_t fork = nullptr, join = nullptr;
   cudaEvent_t ev[16] = {};
   // resident state
   double2* st = nullptr;     // [7][nyp][NP]
@@ -63,7 +65,7 @@ struct sgpu_ctx {
   bool cfl_pending = false;
   bool have_state = false;
   long long launches = 0;
-  int kb = 8, rb = 2, pb = 8;
+  static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 128;
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
   std::vector<cudaEvent_t> pev;
@@ -103,6 +105,13 @@ static FFTPlan make_plan(int n) {
   while (m % 3 == 0) { p.radix[k++] = 3; m /= 3; }
   while (m % 5 == 0) { p.radix[k++] = 5; m /= 5; }
   p.npass = (m == 1) ? k : -1;
+  int ns = 1;
+  for (int i = 0; i < k; ++i) {
+    p.ns[i] = ns;
+    p.magic[i] = (ns == 1) ? 0u : (unsigned)((((unsigned long long)1 << 32) + ns - 1) / ns);
+    p.tstep[i] = n / (ns * p.radix[i]);
+    ns *= p.radix[i];
+  }
   return p;
 }
 
@@ -191,6 +200,10 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   auto fail = [&](int r) { sgpu_finalize(c); return r; };
   if (cudaSetDevice(P.device) != cudaSuccess) return fail(SGPU_E_CUDA);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if (cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess)
+    return fail(SGPU_E_CUDA);
   for (int i = 0; i < 16; ++i)
     if (cudaEventCreate(&c->ev[i]) != cudaSuccess) return fail(SGPU_E_CUDA);
   if ((rc = make_tw(c->twz, g.nzp)) || (rc = make_tw(c->twx, g.nxp)) || (rc = make_tw(c->twy, 2 * (g.nyp - 1))))
@@ -241,10 +254,10 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
   const size_t s_y = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
   if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024) return fail(SGPU_E_PARAM);
-  cudaFuncSetAttribute(k_zinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_xpass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
-  cudaFuncSetAttribute(k_cheb<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_y);
+  cudaFuncSetAttribute(k_zinv<double, sgpu_ctx::kb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zfwd<double, sgpu_ctx::kb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_xpass<double, sgpu_ctx::rb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
+  cudaFuncSetAttribute(k_cheb<double, sgpu_ctx::pb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_y);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -261,6 +274,9 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   for (int i = 0; i < 16; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (auto& e : c->pev) cudaEventDestroy(e);
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->join) cudaEventDestroy(c->join);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SGPU_OK;
@@ -314,8 +330,8 @@ static void launch_cheb(sgpu_ctx* c, const double2* in, size_t in_fs, double2* o
   const Dims& g = c->g;
   dim3 grid((g.NP + c->pb - 1) / c->pb, nfields);
   const size_t sm = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
-  k_cheb<double><<<grid, 256, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse, scale, c->twy.plan, c->twy.d,
-                                              c->pb, skip_oddball);
+  k_cheb<double, sgpu_ctx::pb><<<grid, sgpu_ctx::fft_threads, sm, c->stream>>>(
+      in, in_fs, out, out_fs, g, inverse, scale, c->twy.plan, c->twy.d, skip_oddball);
   c->launches++;
 }
 
@@ -364,16 +380,18 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   dim3 gz((g.nx2 + c->kb - 1) / c->kb, g.nyp);
   const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
   prof_mark(c, K_ZINV);
-  k_zinv<double><<<gz, 256, s_z, c->stream>>>(c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta, c->kb);
+  k_zinv<double, sgpu_ctx::kb><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->st, c->zb, g, c->twz.plan, c->twz.d,
+                                                                              c->alfa, c->beta);
   dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
   const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
   prof_mark(c, K_XPASS);
-  k_xpass<double><<<gx, 256, s_x, c->stream>>>(c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot,
-                                               c->rb, do_cfl ? c->cfl_bits : nullptr);
+  k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::fft_threads, s_x, c->stream>>>(
+      c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, do_cfl ? c->cfl_bits : nullptr);
   prof_mark(c, K_ZFWD);
-  k_zfwd<double><<<gz, 256, s_z, c->stream>>>(c->xb, c->st, g, c->twz.plan, c->twz.d, c->kb);
+  k_zfwd<double, sgpu_ctx::kb><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->xb, c->st, g, c->twz.plan,
+                                                                              c->twz.d);
   c->launches += 3;
   if (do_cfl) c->cfl_pending = true;
   return cuda_fail(cudaGetLastError(), "nonlin launch");
@@ -402,14 +420,23 @@ static int enqueue_linear(sgpu_ctx* c) {
   B.T1 = czf(c, 14); B.T2 = czf(c, 15);
   B.OU = czf(c, 16); B.OV = czf(c, 17); B.OW = czf(c, 18); B.OX = czf(c, 19); B.OZ = czf(c, 20);
   B.PHIH = rzf(c, 0); B.VH = rzf(c, 1); B.DVH = rzf(c, 2); B.CP = rzf(c, 3); B.WT = rzf(c, 4);
-  prof_mark(c, K_PENCIL);
-  k_pencil<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+  // kx = kz = 0 (mean flow, cflux) on the side stream, concurrent with the pencils
   MeanArgs M;
   M.H1 = B.H1; M.H3 = B.H3; M.puw = c->puw; M.scal = c->scal; M.scr = c->mscr;
   M.OU = B.OU; M.OV = B.OV; M.OW = B.OW; M.OX = B.OX; M.OZ = B.OZ; M.PV = B.PV; M.PW = B.PW;
   M.cflux = P.cflux;
-  prof_mark(c, K_MEAN);
-  k_mean<<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
+  if (c->prof) {
+    prof_mark(c, K_MEAN);
+    k_mean<<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
+  } else {
+    cudaEventRecord(c->fork, c->stream);
+    cudaStreamWaitEvent(c->side, c->fork, 0);
+    k_mean<<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
+    cudaEventRecord(c->join, c->side);
+  }
+  prof_mark(c, K_PENCIL);
+  k_pencil<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+  if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
   launch_cheb(c, B.OU, fld, slot(c, 0), fld, 5, 1, 1.0, 1);

@@ -23,10 +23,10 @@
 
 namespace sb {
 
-template <class T>
+template <class T, int KB>
 __global__ void k_zinv(const double2* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
                        FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       const double* __restrict__ alfa, const double* __restrict__ beta, int KB) {
+                       const double* __restrict__ alfa, const double* __restrict__ beta) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* b0 = reinterpret_cast<V*>(smem_raw);
@@ -63,7 +63,7 @@ __global__ void k_zinv(const double2* __restrict__ st, typename C2<T>::type* __r
       b0[t] = val;
     }
     __syncthreads();
-    V* res = fft_columns<T>(b0, b1, KB, plan, tw, +1);
+    V* res = fft_columns<T, KB>(b0, b1, plan, tw, +1);
     for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
       const int m = t / KB;
       const int b = t - m * KB;
@@ -79,10 +79,10 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-template <class T>
+template <class T, int RB>
 __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb,
                         Dims g, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                        const double* __restrict__ dyi, double dxi, double dzi, double rot, int RB,
+                        const double* __restrict__ dyi, double dxi, double dzi, double rot,
                         unsigned long long* __restrict__ cfl_bits) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -116,7 +116,7 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
     bA[t] = z;
   }
   __syncthreads();
-  V* res = fft_columns<T>(bA, bB, B, plan, tw, +1);
+  V* res = fft_columns<T, 3 * RB>(bA, bB, plan, tw, +1);
   V* oth = (res == bA) ? bB : bA;
   // products in physical space, H into (H1 + i H2, H3 + 0i), CFL
   const int B2 = 2 * RB;
@@ -141,7 +141,7 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
     }
   }
   __syncthreads();
-  V* fres = fft_columns<T>(oth, res, B2, plan, tw, -1);
+  V* fres = fft_columns<T, 2 * RB>(oth, res, plan, tw, -1);
   for (int t = threadIdx.x; t < g.nx2 * RB; t += blockDim.x) {
     const int k = t / RB;
     const int r = t - k * RB;
@@ -170,9 +170,9 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
   }
 }
 
-template <class T>
+template <class T, int KB>
 __global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, double2* __restrict__ st, Dims g,
-                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw, int KB) {
+                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* b0 = reinterpret_cast<V*>(smem_raw);
@@ -190,7 +190,7 @@ __global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, double2* __r
       b0[t] = (kx < g.nx2) ? xb[f * fs + ((size_t)y * g.nzp + m) * g.nx2 + kx] : V{(T)0, (T)0};
     }
     __syncthreads();
-    V* res = fft_columns<T>(b0, b1, KB, plan, tw, -1);
+    V* res = fft_columns<T, KB>(b0, b1, plan, tw, -1);
     for (int t = threadIdx.x; t < g.nz * KB; t += blockDim.x) {
       const int iz = t / KB;
       const int b = t - iz * KB;

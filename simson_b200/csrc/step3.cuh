@@ -20,10 +20,14 @@
 
 namespace sb {
 
+#ifndef SB_HD
+#define SB_HD __host__ __device__
+#endif
+
 struct Col {
   double* a;
   size_t s;
-  __device__ __forceinline__ double& operator[](int j) const { return a[(size_t)j * s]; }
+  SB_HD __forceinline__ double& operator[](int j) const { return a[(size_t)j * s]; }
 };
 
 __device__ __forceinline__ Col col_re(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p, 2 * (size_t)NP}; }
@@ -32,7 +36,7 @@ __device__ __forceinline__ Col col_r(double* arr, int p, int NP) { return Col{ar
 
 // Chebyshev derivative: b = D a, by the backward recurrence
 // b_j = b_{j+2} + 2(j+1) a_{j+1}, b_{n-1} = 0, b_0 halved (bla/dcheb.f).
-__device__ void cheb_deriv(Col b, Col a, int n) {
+SB_HD inline void cheb_deriv(Col b, Col a, int n) {
   double bp2 = 2.0 * (double)(n - 1) * a[n - 1];  // b[n-2]
   double bp1 = 2.0 * (double)(n - 2) * a[n - 2];  // b[n-3]
   b[n - 2] = bp2;
@@ -49,19 +53,19 @@ __device__ void cheb_deriv(Col b, Col a, int n) {
 
 // Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
 // (1-based row index i as in bla/setmacrhs.f).
-__device__ __forceinline__ double tau_c(int i, double lam) {
+SB_HD __forceinline__ double tau_c(int i, double lam) {
   return (i == 1) ? -0.25 * lam : (-0.25 / ((double)i * ((double)i + 1.0))) * lam;
 }
-__device__ __forceinline__ double tau_d(int i, double lam) {
+SB_HD __forceinline__ double tau_d(int i, double lam) {
   return 1.0 + (0.5 / ((double)i * ((double)i + 2.0))) * lam;
 }
-__device__ __forceinline__ double tau_e(int i, double lam) {
+SB_HD __forceinline__ double tau_e(int i, double lam) {
   return (-0.25 / (((double)i + 1.0) * ((double)i + 2.0))) * lam;
 }
 
 // Tau right-hand side of row i (3 <= i <= n, 1-based) from f: the
 // Chebyshev-coefficient form of u'' = f + lam u, truncated at n modes.
-__device__ __forceinline__ double tau_rhs(const Col& f, int i, int n) {
+SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
   if (f.a == nullptr) return 0.0;
   auto F = [&](int k) { return f[k - 1]; };
   const double di = (double)i;
@@ -72,47 +76,59 @@ __device__ __forceinline__ double tau_rhs(const Col& f, int i, int n) {
   return r;
 }
 
-// Solve (D^2 - lam) x_q = f_q, q < m, by the Chebyshev tau method with the
+// Solve (D^2 - lam) x_q = f_q, q < M, by the Chebyshev tau method with the
 // boundary rows  sum_{k even} x_k = bc1[q],  sum_{k odd} x_k = bc2[q]
-// (i.e. x(+1) = bc1+bc2, x(-1) = bc1-bc2).  Elimination order follows
-// bla/trid.f:120-200: upper off-diagonal from the top, the two full rows
-// through the weights W, then the lower off-diagonal upwards.
-// cp, wt: per-pencil scratch columns (n entries each).
+// (i.e. x(+1) = bc1+bc2, x(-1) = bc1-bc2).  The elimination is the one of
+// bla/trid.f:120-200 -- upper off-diagonal from the top, the two full rows
+// through the weights W, then the lower off-diagonal -- with the same rounding
+// of every operation, reorganised into three sweeps whose recurrences run in
+// registers:
+//   1. backward (rows n..3): factor 1/d', c' = c/d'; eliminated right-hand side
+//      x(i) = (rhs(i) - x(i+2) e(i-2)) / d'(i-2); weights W(i) = 1 - c'(i) W(i+2);
+//   2. ascending boundary sums (same summation order as the reference);
+//   3. forward (rows 3..n): x(i) -= c'(i-2) x(i-2).
+// cp, wt: per-pencil scratch columns (n entries each).  f[q].a == nullptr
+// means a zero right-hand side.
 template <int M>
-__device__ void tau_solve(double lam, int n, const Col* f, const Col* x, const double* bc1, const double* bc2,
+SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double* bc1, const double* bc2,
                           Col cp, Col wt) {
-  // setmacrhs: rows 3..n
-  for (int q = 0; q < M; ++q)
-    for (int i = 3; i <= n; ++i) x[q][i - 1] = tau_rhs(f[q], i, n);
-  // factor: wt <- 1/d', cp <- c' = c/d'
-  {
-    const double a5 = 1.0 / tau_d(n - 5, lam);
-    cp[n - 6] = tau_c(n - 5, lam) * a5;
-    wt[n - 6] = a5;
-    const double a4 = 1.0 / tau_d(n - 4, lam);
-    cp[n - 5] = tau_c(n - 4, lam) * a4;
-    wt[n - 5] = a4;
-    for (int i = n - 6; i >= 1; --i) {
-      const double di = 1.0 / (tau_d(i, lam) - cp[i + 1] * tau_e(i, lam));
-      cp[i - 1] = tau_c(i, lam) * di;
-      wt[i - 1] = di;
+  double xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
+  double q1 = 0.0, q2 = 0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
+  double w1 = 0.0, w2 = 0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
+#pragma unroll
+  for (int q = 0; q < M; ++q) xa[q] = xb[q] = 0.0;
+  for (int i = n; i >= 3; --i) {
+    double dinv = 1.0, cnew = 0.0, wnew = 0.0;
+    if (i <= n - 2) {
+      const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
+      dinv = (i >= n - 3) ? 1.0 / tau_d(m, lam) : 1.0 / (tau_d(m, lam) - q2 * tau_e(m, lam));
+      cnew = tau_c(m, lam) * dinv;
+      cp[m - 1] = cnew;
+      wnew = (i >= n - 3) ? 1.0 - tau_c(i, lam) : 1.0 - q2 * w2;
+      wt[i - 1] = wnew;
     }
-    cp[n - 4] = tau_c(n - 3, lam);
-    cp[n - 3] = tau_c(n - 2, lam);
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      double r = tau_rhs(f[q], i, n);
+      if (i <= n - 4)
+        r = (r - xb[q] * tau_e(i - 2, lam)) * dinv;
+      else if (i <= n - 2)
+        r = r * dinv;
+      x[q][i - 1] = r;
+      xb[q] = xa[q];
+      xa[q] = r;
+    }
+    q2 = q1;
+    q1 = cnew;
+    w2 = w1;
+    w1 = wnew;
   }
-  // eliminate the upper off-diagonal in every right-hand side
-  for (int q = 0; q < M; ++q) {
-    const Col X = x[q];
-    X[n - 4] = X[n - 4] * wt[n - 6];
-    X[n - 3] = X[n - 3] * wt[n - 5];
-    for (int i = n - 4; i >= 3; --i) X[i - 1] = (X[i - 1] - X[i + 1] * tau_e(i - 2, lam)) * wt[i - 3];
-  }
-  // weights of the two full (boundary) rows
-  wt[n - 4] = 1.0 - cp[n - 4];
-  wt[n - 3] = 1.0 - cp[n - 3];
-  for (int i = n - 4; i >= 3; --i) wt[i - 1] = 1.0 - cp[i - 1] * wt[i + 1];
+  // c'(n-3), c'(n-2) are the unscaled c (d = 1 in the truncated rows)
+  cp[n - 4] = tau_c(n - 3, lam);
+  cp[n - 3] = tau_c(n - 2, lam);
   const double d1 = 1.0 / (1.0 - cp[0] * wt[2]);
   const double d2 = 1.0 / (1.0 - cp[1] * wt[3]);
+#pragma unroll
   for (int q = 0; q < M; ++q) {
     const Col X = x[q];
     double x1 = bc1[q] - X[n - 1];
@@ -121,19 +137,30 @@ __device__ void tau_solve(double lam, int n, const Col* f, const Col* x, const d
       x1 = x1 - X[i - 1] * wt[i - 1];
       x2 = x2 - X[i - 2] * wt[i - 2];
     }
-    X[0] = (x1 - X[2] * wt[2]) * d1;
-    X[1] = x2 * d2;
-    for (int i = 3; i <= n; ++i) X[i - 1] = X[i - 1] - cp[i - 3] * X[i - 3];
+    xa[q] = (x1 - X[2] * wt[2]) * d1;  // x(1)
+    xb[q] = x2 * d2;                   // x(2)
+    X[0] = xa[q];
+    X[1] = xb[q];
+  }
+  for (int i = 3; i <= n; ++i) {
+    const double c = cp[i - 3];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const double v = x[q][i - 1] - c * xa[q];
+      x[q][i - 1] = v;
+      xa[q] = xb[q];
+      xb[q] = v;
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Chebyshev transforms over pencils
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, int PB>
 __global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __restrict__ out, size_t out_fs,
                        Dims g, int inverse, double scale, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       int PB, int skip_oddball) {
+                       int skip_oddball) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = g.nyp;
@@ -160,7 +187,7 @@ __global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __
     if (j >= 1 && j <= N - 1) b0[(L - j) * PB + b] = w;
   }
   __syncthreads();
-  V* res = fft_columns<T>(b0, b1, PB, plan, tw, -1);
+  V* res = fft_columns<T, PB>(b0, b1, plan, tw, -1);
   for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
     const int k = t / PB;
     const int b = t - k * PB;
@@ -310,9 +337,11 @@ struct MeanArgs {
 };
 
 __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
+  extern __shared__ double msm[];  // 12 columns of n doubles
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int n = g.nyp;
   const int NP = g.NP;
+  A.scr = msm;
   Col huw1{A.scr + 0 * n, 1}, huw2{A.scr + 1 * n, 1}, fu{A.scr + 2 * n, 1}, fw{A.scr + 3 * n, 1};
   Col U{A.scr + 4 * n, 1}, W{A.scr + 5 * n, 1}, DU{A.scr + 6 * n, 1}, DW{A.scr + 7 * n, 1};
   Col cp{A.scr + 8 * n, 1}, wt{A.scr + 9 * n, 1}, t1{A.scr + 10 * n, 1}, t2{A.scr + 11 * n, 1};

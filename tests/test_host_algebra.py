@@ -1,0 +1,94 @@
+"""The step-3 pencil algebra (compiled for the host from the same source the
+CUDA kernels use) against the reference's own setmacrhs + trid (tau branch)
+and dcheb, called from the translated reference.  CPU only; the results
+must be bit-identical because both evaluate the same operations in the
+same order without fused multiply-add."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from simson_b200 import build as sbuild
+
+dp = ctypes.POINTER(ctypes.c_double)
+
+
+def P(a):
+    return a.ctypes.data_as(dp)
+
+
+def I(v):
+    return ctypes.byref(ctypes.c_int(v))
+
+
+@pytest.fixture(scope="module")
+def libs(request):
+    from conftest import reference_available
+    if not reference_available(16, 17, 16):
+        pytest.skip("reference oracle unavailable")
+    from build_ref import build
+    ref = ctypes.CDLL(build(16, 17, 16))
+    host = ctypes.CDLL(sbuild.build_hostcheck())
+    host.sbh_tau_solve.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp]
+    host.sbh_cheb_deriv.argtypes = [dp, dp, ctypes.c_int]
+    return ref, host
+
+
+def ref_tau(ref, lam, f, bc1, bc2):
+    m, n = f.shape
+    c = np.zeros(n); d = np.zeros(n); e = np.zeros(n); q = np.zeros(n + 2)
+    x = np.zeros((m, n))
+    hl = np.array([lam])
+    fc = np.ascontiguousarray(f)
+    ref.f_setmacrhs(P(x), P(fc), P(c), P(d), P(e), P(hl), I(1), I(n), I(m), I(1), I(n))
+    bc = np.zeros((m, 2))
+    bc[:, 0] = bc1
+    bc[:, 1] = bc2
+    xc = np.zeros((m, 2))
+    ref.f_trid(P(x), P(xc), P(q), P(c), P(d), P(e), P(fc), P(bc), I(1), I(n), I(m), I(1), I(n), I(0))
+    return x
+
+
+@pytest.mark.parametrize("n", [17, 33, 65, 97, 129, 193])
+@pytest.mark.parametrize("lam", [0.0, 3.7, 1.6e6, 6.3e6])
+def test_tau_solver_bitwise(libs, n, lam):
+    ref, host = libs
+    rng = np.random.default_rng(n + int(lam))
+    m = 5
+    f = rng.standard_normal((m, n)) * np.exp(-0.1 * np.arange(n))
+    bc1 = rng.standard_normal(m)
+    bc2 = rng.standard_normal(m)
+    xr = ref_tau(ref, lam, f, bc1, bc2)
+    x = np.zeros((m, n))
+    cp = np.zeros(n)
+    wt = np.zeros(n)
+    host.sbh_tau_solve(lam, n, m, P(np.ascontiguousarray(f)), P(x), P(bc1), P(bc2), P(cp), P(wt))
+    assert np.array_equal(x, xr), np.abs(x - xr).max()
+
+
+def test_tau_solver_zero_rhs_homogeneous(libs):
+    """f = 0 with boundary rows (1, 1): the homogeneous solution phi_h used by
+    the v/omega superposition (linearbl.f:505-512)."""
+    ref, host = libs
+    n, lam = 65, 2.4e6
+    f = np.zeros((1, n))
+    xr = ref_tau(ref, lam, f, np.array([1.0]), np.array([1.0]))
+    x = np.zeros((1, n))
+    cp, wt = np.zeros(n), np.zeros(n)
+    host.sbh_tau_solve(lam, n, 1, P(f), P(x), P(np.array([1.0])), P(np.array([1.0])), P(cp), P(wt))
+    assert np.array_equal(x, xr)
+    # x(+1) = sum x_k = 2, x(-1) = sum (-1)^k x_k = 0
+    assert abs(x.sum() - 2.0) < 1e-12 and abs((x * (-1.0) ** np.arange(n)).sum()) < 1e-12
+
+
+@pytest.mark.parametrize("n", [17, 65, 193])
+def test_cheb_deriv_bitwise(libs, n):
+    ref, host = libs
+    a = np.random.default_rng(n).standard_normal(n)
+    b_ref = np.zeros(n)
+    ref.f_dcheb(P(b_ref), P(a), I(n), I(1), I(1))
+    b = np.zeros(n)
+    host.sbh_cheb_deriv(P(a), P(b), n)
+    assert np.array_equal(b, b_ref)
+    # and it is the derivative: compare with numpy's Chebyshev derivative
+    np.testing.assert_allclose(b[:-1], np.polynomial.chebyshev.chebder(a), rtol=1e-12, atol=1e-10)
