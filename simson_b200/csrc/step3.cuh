@@ -37,18 +37,22 @@ __device__ __forceinline__ Col col_r(double* arr, int p, int NP) { return Col{ar
 // Chebyshev derivative: b = D a, by the backward recurrence
 // b_j = b_{j+2} + 2(j+1) a_{j+1}, b_{n-1} = 0, b_0 halved (bla/dcheb.f).
 SB_HD inline void cheb_deriv(Col b, Col a, int n) {
-  double bp2 = 2.0 * (double)(n - 1) * a[n - 1];  // b[n-2]
-  double bp1 = 2.0 * (double)(n - 2) * a[n - 2];  // b[n-3]
-  b[n - 2] = bp2;
-  b[n - 3] = bp1;
+  // a and b never alias: loads may run ahead of the stores
+  const double* __restrict__ ap = a.a;
+  double* __restrict__ bp = b.a;
+  const size_t sa = a.s, sb = b.s;
+  double bp2 = 2.0 * (double)(n - 1) * ap[(size_t)(n - 1) * sa];  // b[n-2]
+  double bp1 = 2.0 * (double)(n - 2) * ap[(size_t)(n - 2) * sa];  // b[n-3]
+  bp[(size_t)(n - 2) * sb] = bp2;
+  bp[(size_t)(n - 3) * sb] = bp1;
+#pragma unroll 8
   for (int j = n - 4; j >= 0; --j) {
-    const double v = bp2 + 2.0 * (double)(j + 1) * a[j + 1];
+    const double v = bp2 + 2.0 * (double)(j + 1) * ap[(size_t)(j + 1) * sa];
     bp2 = bp1;
     bp1 = v;
-    b[j] = v;
+    bp[(size_t)j * sb] = (j == 0) ? 0.5 * v : v;
   }
-  b[n - 1] = 0.0;
-  b[0] = 0.5 * b[0];
+  bp[(size_t)(n - 1) * sb] = 0.0;
 }
 
 // Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
@@ -91,7 +95,22 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 // means a zero right-hand side.
 template <int M>
 SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double* bc1, const double* bc2,
-                          Col cp, Col wt) {
+                     Col cp, Col wt) {
+  // every column is a distinct array: restrict-qualified raw pointers let the
+  // loads of a sweep run ahead of its stores
+  const double* __restrict__ fp[M];
+  double* __restrict__ xp[M];
+  size_t fs[M], xs[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) {
+    fp[q] = f[q].a;
+    fs[q] = f[q].s;
+    xp[q] = x[q].a;
+    xs[q] = x[q].s;
+  }
+  double* __restrict__ cpp = cp.a;
+  double* __restrict__ wtp = wt.a;
+  const size_t cs = cp.s, ws = wt.s;
   double xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
   double q1 = 0.0, q2 = 0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
   double w1 = 0.0, w2 = 0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
@@ -103,18 +122,34 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
       const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
       dinv = (i >= n - 3) ? 1.0 / tau_d(m, lam) : 1.0 / (tau_d(m, lam) - q2 * tau_e(m, lam));
       cnew = tau_c(m, lam) * dinv;
-      cp[m - 1] = cnew;
+      cpp[(size_t)(m - 1) * cs] = cnew;
       wnew = (i >= n - 3) ? 1.0 - tau_c(i, lam) : 1.0 - q2 * w2;
-      wt[i - 1] = wnew;
+      wtp[(size_t)(i - 1) * ws] = wnew;
     }
+    const double di = (double)i;
+    const double ca = (i == 3) ? 0.0 : 0.25 / ((di - 2.0) * (di - 1.0));
+    const double cb = -0.5 / ((di - 2.0) * di);
+    const double cc = 0.25 / ((di - 1.0) * di);
+    const double e2 = (i <= n - 4) ? tau_e(i - 2, lam) : 0.0;
 #pragma unroll
     for (int q = 0; q < M; ++q) {
-      double r = tau_rhs(f[q], i, n);
+      double r = 0.0;
+      if (fp[q] != nullptr) {
+        const double* __restrict__ F = fp[q];
+        const size_t st = fs[q];
+        if (i == 3) {
+          r = 0.25 * F[0] + F[4 * st] / 24.0 - F[2 * st] / 6.0;
+        } else {
+          r = ca * F[(size_t)(i - 3) * st];
+          if (i <= n - 2) r += cb * F[(size_t)(i - 1) * st];
+          if (i <= n - 4) r += cc * F[(size_t)(i + 1) * st];
+        }
+      }
       if (i <= n - 4)
-        r = (r - xb[q] * tau_e(i - 2, lam)) * dinv;
+        r = (r - xb[q] * e2) * dinv;
       else if (i <= n - 2)
         r = r * dinv;
-      x[q][i - 1] = r;
+      xp[q][(size_t)(i - 1) * xs[q]] = r;
       xb[q] = xa[q];
       xa[q] = r;
     }
@@ -124,30 +159,33 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
     w1 = wnew;
   }
   // c'(n-3), c'(n-2) are the unscaled c (d = 1 in the truncated rows)
-  cp[n - 4] = tau_c(n - 3, lam);
-  cp[n - 3] = tau_c(n - 2, lam);
-  const double d1 = 1.0 / (1.0 - cp[0] * wt[2]);
-  const double d2 = 1.0 / (1.0 - cp[1] * wt[3]);
+  cpp[(size_t)(n - 4) * cs] = tau_c(n - 3, lam);
+  cpp[(size_t)(n - 3) * cs] = tau_c(n - 2, lam);
+  const double d1 = 1.0 / (1.0 - cpp[0] * wtp[2 * ws]);
+  const double d2 = 1.0 / (1.0 - cpp[cs] * wtp[3 * ws]);
 #pragma unroll
   for (int q = 0; q < M; ++q) {
-    const Col X = x[q];
-    double x1 = bc1[q] - X[n - 1];
-    double x2 = bc2[q] - X[n - 2];
+    double* __restrict__ X = xp[q];
+    const size_t st = xs[q];
+    double x1 = bc1[q] - X[(size_t)(n - 1) * st];
+    double x2 = bc2[q] - X[(size_t)(n - 2) * st];
     for (int i = 5; i <= n - 2; i += 2) {
-      x1 = x1 - X[i - 1] * wt[i - 1];
-      x2 = x2 - X[i - 2] * wt[i - 2];
+      x1 = x1 - X[(size_t)(i - 1) * st] * wtp[(size_t)(i - 1) * ws];
+      x2 = x2 - X[(size_t)(i - 2) * st] * wtp[(size_t)(i - 2) * ws];
     }
-    xa[q] = (x1 - X[2] * wt[2]) * d1;  // x(1)
-    xb[q] = x2 * d2;                   // x(2)
+    xa[q] = (x1 - X[2 * st] * wtp[2 * ws]) * d1;  // x(1)
+    xb[q] = x2 * d2;                               // x(2)
     X[0] = xa[q];
-    X[1] = xb[q];
+    X[st] = xb[q];
   }
+#pragma unroll 4
   for (int i = 3; i <= n; ++i) {
-    const double c = cp[i - 3];
+    const double c = cpp[(size_t)(i - 3) * cs];
 #pragma unroll
     for (int q = 0; q < M; ++q) {
-      const double v = x[q][i - 1] - c * xa[q];
-      x[q][i - 1] = v;
+      const size_t o = (size_t)(i - 1) * xs[q];
+      const double v = xp[q][o] - c * xa[q];
+      xp[q][o] = v;
       xa[q] = xb[q];
       xb[q] = v;
     }
@@ -216,38 +254,48 @@ struct RKc {
   double an, bn, anp1, bnp1;
 };
 
-__global__ void k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa, const double* __restrict__ beta,
-                         double re, RKc rk) {
+__global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
+                                                const double* __restrict__ beta, double re, RKc rk) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
   const int kx = p % g.nx2;
   const int iz = p / g.nx2;
   if (iz == g.zodd || p == 0) return;
   const int n = g.nyp;
-  const int NP = g.NP;
+  const size_t NP = g.NP;
   const double a = alfa[kx], be = beta[iz];
   const double k2 = a * a + be * be;
   const double k2i = 1.0 / k2;
   const double lam = k2 + 2.0 * re / (rk.an + rk.bn);
   const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
-  auto at = [&](double2* arr, int j) -> double2& { return arr[(size_t)j * NP + p]; };
+  // this pencil's column of each array; all arrays are distinct
+#define COLP(name) double2* __restrict__ name = B.name + p
+  COLP(H1); COLP(H2); COLP(H3); COLP(PV); COLP(PW); COLP(G); COLP(DG); COLP(HV); COLP(HOM); COLP(FV); COLP(FW);
+  COLP(PHI); COLP(OM); COLP(V); COLP(DV); COLP(DOM); COLP(T1); COLP(T2); COLP(OU); COLP(OV); COLP(OW); COLP(OX);
+  COLP(OZ);
+#undef COLP
+  double* __restrict__ VH = B.VH + p;
+  double* __restrict__ DVH = B.DVH + p;
 
   // nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340)
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
-    const double2 h1 = at(B.H1, j), h3 = at(B.H3, j);
-    at(B.G, j) = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
+    const size_t o = j * NP;
+    const double2 h1 = H1[o], h3 = H3[o], pw = PW[o];
+    G[o] = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
     const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
-    at(B.HOM, j) = hom;
-    const double2 pw = at(B.PW, j);
-    at(B.FW, j) = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
+    HOM[o] = hom;
+    FW[o] = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
   }
   cheb_deriv(col_re(B.DG, p, NP), col_re(B.G, p, NP), n);
   cheb_deriv(col_im(B.DG, p, NP), col_im(B.G, p, NP), n);
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
-    const double2 dg = at(B.DG, j), h2 = at(B.H2, j), pv = at(B.PV, j);
+    const size_t o = j * NP;
+    const double2 dg = DG[o], h2 = H2[o], pv = PV[o];
     const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
-    at(B.HV, j) = hv;
-    at(B.FV, j) = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
+    HV[o] = hv;
+    FV[o] = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
   }
   // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
   {
@@ -271,19 +319,21 @@ __global__ void k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa, 
   for (int is = 0; is < 2; ++is) {
     double sr = 0.0, si = 0.0, sh = 0.0;
     for (int j = is; j < n; j += 2) {
-      const double2 dv = at(B.DV, j);
+      const double2 dv = DV[j * NP];
       sr = sr + dv.x;
       si = si + dv.y;
-      sh = sh + B.DVH[(size_t)j * NP + p];
+      sh = sh + DVH[j * NP];
     }
     const double cinv = 1.0 / sh;
     cvr[1 - is] = (0.0 - sr) * cinv;
     cvi[1 - is] = (0.0 - si) * cinv;
   }
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
-    const double vh = B.VH[(size_t)j * NP + p];
-    const double2 v = at(B.V, j);
-    at(B.V, j) = double2{v.x + cvr[j & 1] * vh, v.y + cvi[j & 1] * vh};
+    const size_t o = j * NP;
+    const double vh = VH[o];
+    const double2 v = V[o];
+    V[o] = double2{v.x + cvr[j & 1] * vh, v.y + cvi[j & 1] * vh};
   }
   // phi from the final v (tau: phi = D^2 v - k^2 v), derivatives (linearbl.f:1160-1170)
   cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
@@ -293,16 +343,17 @@ __global__ void k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa, 
   cheb_deriv(col_re(B.DOM, p, NP), col_re(B.OM, p, NP), n);
   cheb_deriv(col_im(B.DOM, p, NP), col_im(B.OM, p, NP), n);
   // u, w, omega_x, omega_z (linearbl.f:1193-1212)
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
-    const double2 v = at(B.V, j), t1 = at(B.T1, j);
+    const size_t o = j * NP;
+    const double2 v = V[o], t1 = T1[o], dv = DV[o], om = OM[o], dom = DOM[o];
     const double2 phi = double2{t1.x - k2 * v.x, t1.y - k2 * v.y};
-    at(B.PHI, j) = phi;
-    const double2 dv = at(B.DV, j), om = at(B.OM, j), dom = at(B.DOM, j);
-    at(B.OU, j) = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
-    at(B.OW, j) = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
-    at(B.OZ, j) = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
-    at(B.OX, j) = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
-    at(B.OV, j) = v;
+    PHI[o] = phi;
+    OU[o] = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
+    OW[o] = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
+    OZ[o] = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
+    OX[o] = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
+    OV[o] = v;
   }
   // partial right-hand sides of the next stage (linearbl.f:1696-1800, tau branch)
   cheb_deriv(col_re(B.T1, p, NP), col_re(B.PHI, p, NP), n);
@@ -314,11 +365,13 @@ __global__ void k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa, 
   const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
   const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
   const double k2m = k2 - c1n;
+#pragma unroll 4
   for (int j = 0; j < n; ++j) {
-    const double2 d2phi = at(B.T2, j), phi = at(B.PHI, j), hv = at(B.HV, j);
-    const double2 d2om = at(B.T1, j), om = at(B.OM, j), hom = at(B.HOM, j);
-    at(B.PV, j) = double2{-d2phi.x + k2m * phi.x - c2 * hv.x, -d2phi.y + k2m * phi.y - c2 * hv.y};
-    at(B.PW, j) = double2{-d2om.x + k2m * om.x - c2 * hom.x, -d2om.y + k2m * om.y - c2 * hom.y};
+    const size_t o = j * NP;
+    const double2 d2phi = T2[o], phi = PHI[o], hv = HV[o];
+    const double2 d2om = T1[o], om = OM[o], hom = HOM[o];
+    PV[o] = double2{-d2phi.x + k2m * phi.x - c2 * hv.x, -d2phi.y + k2m * phi.y - c2 * hv.y};
+    PW[o] = double2{-d2om.x + k2m * om.x - c2 * hom.x, -d2om.y + k2m * om.y - c2 * hom.y};
   }
 }
 
