@@ -90,6 +90,23 @@ int sgpu_event_record(sgpu_ctx* ctx, int slot);
 int sgpu_event_elapsed(sgpu_ctx* ctx, int a, int b, float* ms);
 int sgpu_sync(sgpu_ctx* ctx);
 
+/* No counterpart in the reference.  The nonlinear step of sgpu_nonlin for
+ * callers that cannot let the library allocate device memory: hosts that own
+ * every device buffer themselves (a Fortran/OpenACC code with its own memory
+ * pool, or one that has already reserved the GPU's memory for its fields).
+ * fields_in: device array of u, v, w, omega_x, omega_z, each ny x nz x nx/2
+ * complex doubles (kx fastest, the library's device layout); h_out: device
+ * array of H1, H2, H3 in the same layout; cflp_max (host, may be NULL): the
+ * CFL partial maximum max|u|/dx+|v|/dy+|w|/dz of bla/boxcfl.f; stream: a
+ * cudaStream_t or NULL.  Allocates nothing: the step's intermediates sit in
+ * one static device array of 64 MiB that every GPU loading the library holds
+ * until exit; grids needing more (9*ny*(3nz/2)*(nx/2)*16 bytes) are rejected
+ * with SGPU_E_PARAM.  Every call shares that array, so calls that overlap on
+ * the GPU race; the first call on a device looks up the array's address
+ * (make it before any stream capture). */
+int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in, void* h_out, double* cflp_max,
+                        void* stream);
+
 /* Per-kernel timing for profiling runs: enable, run substeps, read the
  * milliseconds and launch counts per kernel id (0 zinv, 1 xpass, 2 zfwd,
  * 3 Chebyshev forward, 4 pencil solve, 5 mean flow, 6 Chebyshev inverse,

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libsimson_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "simson.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "simson.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
 DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "simson_b200.h")]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
