@@ -13,20 +13,42 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
+
+#ifndef SB_HD
+#define SB_HD __host__ __device__
+#endif
+
 namespace sb {
 
 template <class T> struct C2;
 template <> struct C2<double> { typedef double2 type; };
 template <> struct C2<float> { typedef float2 type; };
 
-template <class V> __device__ __forceinline__ V cadd(V a, V b) { return V{a.x + b.x, a.y + b.y}; }
-template <class V> __device__ __forceinline__ V csub(V a, V b) { return V{a.x - b.x, a.y - b.y}; }
-template <class V> __device__ __forceinline__ V cmul(V a, V b) {
-  return V{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+template <class V> SB_HD __forceinline__ V cadd(V a, V b) { return V{a.x + b.x, a.y + b.y}; }
+template <class V> SB_HD __forceinline__ V csub(V a, V b) { return V{a.x - b.x, a.y - b.y}; }
+SB_HD __forceinline__ double fma_(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+  return __fma_rn(a, b, c);
+#else
+  return std::fma(a, b, c);
+#endif
 }
-template <class V> __device__ __forceinline__ V cconj(V a) { return V{a.x, -a.y}; }
+SB_HD __forceinline__ float fma_(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(a, b, c);
+#else
+  return std::fma(a, b, c);
+#endif
+}
+// complex product with explicit fused multiply-adds (the FFTs are not the
+// parity-sensitive part of the step; the tau solves are built without FMA)
+template <class V> SB_HD __forceinline__ V cmul(V a, V b) {
+  return V{fma_(a.x, b.x, -a.y * b.y), fma_(a.x, b.y, a.y * b.x)};
+}
+template <class V> SB_HD __forceinline__ V cconj(V a) { return V{a.x, -a.y}; }
 // multiply by i*s (s = +-1)
-template <class V> __device__ __forceinline__ V cmuli(V a, int s) {
+template <class V> SB_HD __forceinline__ V cmuli(V a, int s) {
   return s > 0 ? V{-a.y, a.x} : V{a.y, -a.x};
 }
 
@@ -45,9 +67,98 @@ struct FFTPlan {
 #define SB_C5_2 (-0.80901699437494742410229341718281905886)
 #define SB_S5_2 0.58778525229247312916870595463907276860
 #define SB_S3 0.86602540378443864676372317075293618347
+#define SB_R2 0.70710678118654752440084436210484903928
+// cos and sin of 2*pi/9, 4*pi/9, 8*pi/9 (the radix-9 inner twiddles)
+#define SB_C9_1 0.76604444311897803520239265055541667394
+#define SB_S9_1 0.64278760968653932632264340990726343291
+#define SB_C9_2 0.17364817766693034885171662676931479600
+#define SB_S9_2 0.98480775301220805936674302458952301367
+#define SB_C9_4 (-0.93969262078590838405410927732473146993)
+#define SB_S9_4 0.34202014332566873304409961468225958076
 
 template <class T, class V>
-__device__ __forceinline__ void dft_small(V* v, int R, int s) {
+SB_HD __forceinline__ void dft3(V& a, V& b, V& c, int s) {
+  V sum = cadd(b, c);
+  V dif = csub(b, c);
+  V m = V{a.x - (T)0.5 * sum.x, a.y - (T)0.5 * sum.y};
+  V r = cmuli(V{(T)SB_S3 * dif.x, (T)SB_S3 * dif.y}, s);
+  a = cadd(a, sum);
+  b = cadd(m, r);
+  c = csub(m, r);
+}
+
+template <class T, class V>
+SB_HD __forceinline__ void dft4(V& a, V& b, V& c, V& d, int s) {
+  V a0 = cadd(a, c), a1 = csub(a, c);
+  V b0 = cadd(b, d), b1 = cmuli(csub(b, d), s);
+  a = cadd(a0, b0);
+  c = csub(a0, b0);
+  b = cadd(a1, b1);
+  d = csub(a1, b1);
+}
+
+// multiply by exp(s*i*2pi*k/8) for k = 1, 3 (k = 2 is cmuli)
+template <class T, class V> SB_HD __forceinline__ V w8_1(V a, int s) {
+  // (1 + s i)/sqrt2 * a
+  return s > 0 ? V{(T)SB_R2 * (a.x - a.y), (T)SB_R2 * (a.x + a.y)} : V{(T)SB_R2 * (a.x + a.y), (T)SB_R2 * (a.y - a.x)};
+}
+template <class T, class V> SB_HD __forceinline__ V w8_3(V a, int s) {
+  // (-1 + s i)/sqrt2 * a
+  return s > 0 ? V{(T)SB_R2 * (-a.x - a.y), (T)SB_R2 * (a.x - a.y)} : V{(T)SB_R2 * (a.y - a.x), (T)SB_R2 * (-a.x - a.y)};
+}
+
+template <class T, class V>
+SB_HD __forceinline__ void dft_small(V* v, int R, int s) {
+  if (R == 8) {
+    // radix-2 over stride 4, twiddles w8^k, then two radix-4 DFTs
+    V e0 = cadd(v[0], v[4]), o0 = csub(v[0], v[4]);
+    V e1 = cadd(v[1], v[5]), o1 = w8_1<T, V>(csub(v[1], v[5]), s);
+    V e2 = cadd(v[2], v[6]), o2 = cmuli(csub(v[2], v[6]), s);
+    V e3 = cadd(v[3], v[7]), o3 = w8_3<T, V>(csub(v[3], v[7]), s);
+    dft4<T, V>(e0, e1, e2, e3, s);
+    dft4<T, V>(o0, o1, o2, o3, s);
+    v[0] = e0; v[2] = e1; v[4] = e2; v[6] = e3;
+    v[1] = o0; v[3] = o1; v[5] = o2; v[7] = o3;
+    return;
+  }
+  if (R == 6) {
+    // radix-2 over stride 3 (w6^k twiddles), then two radix-3 DFTs
+    V e0 = cadd(v[0], v[3]), o0 = csub(v[0], v[3]);
+    V e1 = cadd(v[1], v[4]), d1 = csub(v[1], v[4]);
+    V e2 = cadd(v[2], v[5]), d2 = csub(v[2], v[5]);
+    // w6 = 1/2 + s i sqrt3/2 ; w6^2 = -1/2 + s i sqrt3/2
+    V o1 = V{(T)0.5 * d1.x, (T)0.5 * d1.y};
+    o1 = cadd(o1, cmuli(V{(T)SB_S3 * d1.x, (T)SB_S3 * d1.y}, s));
+    V o2 = V{(T)-0.5 * d2.x, (T)-0.5 * d2.y};
+    o2 = cadd(o2, cmuli(V{(T)SB_S3 * d2.x, (T)SB_S3 * d2.y}, s));
+    dft3<T, V>(e0, e1, e2, s);
+    dft3<T, V>(o0, o1, o2, s);
+    v[0] = e0; v[2] = e1; v[4] = e2;
+    v[1] = o0; v[3] = o1; v[5] = o2;
+    return;
+  }
+  if (R == 9) {
+    // radix-3 over stride 3, inner twiddles w9^(k*m), radix-3 again
+    V a0 = v[0], a1 = v[3], a2 = v[6];
+    V b0 = v[1], b1 = v[4], b2 = v[7];
+    V c0 = v[2], c1 = v[5], c2 = v[8];
+    dft3<T, V>(a0, a1, a2, s);
+    dft3<T, V>(b0, b1, b2, s);
+    dft3<T, V>(c0, c1, c2, s);
+    const V w1 = V{(T)SB_C9_1, (T)(s * SB_S9_1)}, w2 = V{(T)SB_C9_2, (T)(s * SB_S9_2)};
+    const V w4 = V{(T)SB_C9_4, (T)(s * SB_S9_4)};
+    b1 = cmul(b1, w1);
+    b2 = cmul(b2, w2);
+    c1 = cmul(c1, w2);
+    c2 = cmul(c2, w4);
+    dft3<T, V>(a0, b0, c0, s);
+    dft3<T, V>(a1, b1, c1, s);
+    dft3<T, V>(a2, b2, c2, s);
+    v[0] = a0; v[3] = b0; v[6] = c0;
+    v[1] = a1; v[4] = b1; v[7] = c1;
+    v[2] = a2; v[5] = b2; v[8] = c2;
+    return;
+  }
   if (R == 2) {
     V a = v[0], b = v[1];
     v[0] = cadd(a, b);
@@ -86,19 +197,27 @@ __device__ __forceinline__ void dft_small(V* v, int R, int s) {
 // number of interleaved columns) is a compile-time constant so the column
 // index is a mask/shift; the only division left (by Ns) uses a precomputed
 // reciprocal.  The twiddle exponent r*jm*tstep is always below n.
+SB_HD __forceinline__ unsigned umulhi_(unsigned a, unsigned b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (unsigned)(((unsigned long long)a * b) >> 32);
+#endif
+}
+
 template <class T, int B, int R>
-__device__ __forceinline__ void stockham_pass(const typename C2<T>::type* __restrict__ src,
-                                              typename C2<T>::type* __restrict__ dst, int n, int Ns,
-                                              unsigned magic, int tstep,
-                                              const typename C2<T>::type* __restrict__ tw, int s) {
+SB_HD __forceinline__ void stockham_pass(const typename C2<T>::type* __restrict__ src,
+                                         typename C2<T>::type* __restrict__ dst, int n, int Ns, unsigned magic,
+                                         int tstep, const typename C2<T>::type* __restrict__ tw, int s, int t0,
+                                         int tstride) {
   typedef typename C2<T>::type V;
   const int nb = n / R;
-  for (int t = threadIdx.x; t < nb * B; t += blockDim.x) {
+  for (int t = t0; t < nb * B; t += tstride) {
     const int j = t / B;
     const int b = t - j * B;
-    const int jg = (Ns == 1) ? j : (int)__umulhi((unsigned)j, magic);
+    const int jg = (Ns == 1) ? j : (int)umulhi_((unsigned)j, magic);
     const int jm = j - jg * Ns;
-    V v[5];
+    V v[9];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * B + b];
     if (jm != 0) {
@@ -117,6 +236,30 @@ __device__ __forceinline__ void stockham_pass(const typename C2<T>::type* __rest
   }
 }
 
+// One pass of radix plan.radix[p]: work items t0, t0+tstride, ...
+template <class T, int B>
+SB_HD __forceinline__ void fft_pass(const typename C2<T>::type* src, typename C2<T>::type* dst, const FFTPlan& plan,
+                                    int p, const typename C2<T>::type* __restrict__ tw, int s, int t0, int tstride) {
+  const int R = plan.radix[p];
+  const int Ns = plan.ns[p];
+  const unsigned mg = plan.magic[p];
+  const int ts = plan.tstep[p];
+  if (R == 8)
+    stockham_pass<T, B, 8>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else if (R == 9)
+    stockham_pass<T, B, 9>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else if (R == 6)
+    stockham_pass<T, B, 6>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else if (R == 4)
+    stockham_pass<T, B, 4>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else if (R == 2)
+    stockham_pass<T, B, 2>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else if (R == 3)
+    stockham_pass<T, B, 3>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+  else
+    stockham_pass<T, B, 5>(src, dst, plan.n, Ns, mg, ts, tw, s, t0, tstride);
+}
+
 // Full transform of the B interleaved columns held in buf0; buf1 is scratch.
 // Returns the buffer holding the result.  Caller syncs before; the function
 // ends with a barrier.
@@ -127,22 +270,35 @@ __device__ typename C2<T>::type* fft_columns(typename C2<T>::type* buf0, typenam
   typename C2<T>::type* src = buf0;
   typename C2<T>::type* dst = buf1;
   for (int p = 0; p < plan.npass; ++p) {
-    const int R = plan.radix[p];
-    const int Ns = plan.ns[p];
-    if (R == 4)
-      stockham_pass<T, B, 4>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
-    else if (R == 2)
-      stockham_pass<T, B, 2>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
-    else if (R == 3)
-      stockham_pass<T, B, 3>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
-    else
-      stockham_pass<T, B, 5>(src, dst, plan.n, Ns, plan.magic[p], plan.tstep[p], tw, s);
+    fft_pass<T, B>(src, dst, plan, p, tw, s, threadIdx.x, blockDim.x);
     __syncthreads();
     typename C2<T>::type* tmp = src;
     src = dst;
     dst = tmp;
   }
   return src;
+}
+
+// Radix plan of an n-point transform: 8s first, then 9, 6, 4, 2, 3, 5.
+inline FFTPlan fft_make_plan(int n) {
+  FFTPlan p{};
+  p.n = n;
+  int m = n, k = 0;
+  const int order[7] = {8, 9, 6, 4, 2, 3, 5};
+  for (int r : order)
+    while (m % r == 0 && k < 20) {
+      p.radix[k++] = r;
+      m /= r;
+    }
+  p.npass = (m == 1) ? k : -1;
+  int ns = 1;
+  for (int i = 0; i < k; ++i) {
+    p.ns[i] = ns;
+    p.magic[i] = (ns == 1) ? 0u : (unsigned)((((unsigned long long)1 << 32) + ns - 1) / ns);
+    p.tstep[i] = n / (ns * p.radix[i]);
+    ns *= p.radix[i];
+  }
+  return p;
 }
 
 }  // namespace sb

@@ -1,6 +1,7 @@
 // Host build of the pencil algebra of step 3 (the same source the kernels
 // run), exported for the CPU unit tests that compare it with the
 // reference's setmacrhs/trid/dcheb.  Not part of the device library.
+#include "fft.cuh"
 #include "step3.cuh"
 
 using namespace sb;
@@ -25,4 +26,35 @@ extern "C" void sbh_tau_solve(double lam, int n, int m, const double* f, double*
 
 extern "C" void sbh_cheb_deriv(const double* a, double* b, int n) {
   cheb_deriv(Col{b, 1}, Col{const_cast<double*>(a), 1}, n);
+}
+
+// Host run of the shared-memory FFT passes on B interleaved columns
+// (element i of column b at [i*B + b]); in/out complex interleaved.
+extern "C" int sbh_fft(int n, const double* in, double* out, int sign) {
+  const FFTPlan plan = fft_make_plan(n);
+  if (plan.npass < 0) return -1;
+  double2* tw = new double2[n];
+  for (int m = 0; m < n; ++m) {
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+    tw[m] = double2{(double)cosl(ang), (double)sinl(ang)};
+  }
+  double2* a = new double2[n];
+  double2* b = new double2[n];
+  for (int i = 0; i < n; ++i) a[i] = double2{in[2 * i], in[2 * i + 1]};
+  double2* src = a;
+  double2* dst = b;
+  for (int p = 0; p < plan.npass; ++p) {
+    fft_pass<double, 1>(src, dst, plan, p, tw, sign, 0, 1);
+    double2* t = src;
+    src = dst;
+    dst = t;
+  }
+  for (int i = 0; i < n; ++i) {
+    out[2 * i] = src[i].x;
+    out[2 * i + 1] = src[i].y;
+  }
+  delete[] a;
+  delete[] b;
+  delete[] tw;
+  return plan.npass;
 }

@@ -68,24 +68,6 @@ int area_for_current_device(unsigned char** out) {
   return SGPU_OK;
 }
 
-FFTPlan plan_for(int n) {
-  FFTPlan p{};
-  p.n = n;
-  int m = n, k = 0;
-  while (m % 4 == 0) { p.radix[k++] = 4; m /= 4; }
-  while (m % 2 == 0) { p.radix[k++] = 2; m /= 2; }
-  while (m % 3 == 0) { p.radix[k++] = 3; m /= 3; }
-  while (m % 5 == 0) { p.radix[k++] = 5; m /= 5; }
-  p.npass = (m == 1) ? k : -1;
-  int ns = 1;
-  for (int i = 0; i < k; ++i) {
-    p.ns[i] = ns;
-    p.magic[i] = (ns == 1) ? 0u : (unsigned)((((unsigned long long)1 << 32) + ns - 1) / ns);
-    p.tstep[i] = n / (ns * p.radix[i]);
-    ns *= p.radix[i];
-  }
-  return p;
-}
 
 }  // namespace
 
@@ -110,7 +92,7 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
             P.nx, P.ny, P.nz, need, (unsigned long long)SGPU_NOALLOC_SCRATCH_BYTES);
     return SGPU_E_PARAM;
   }
-  const FFTPlan pz = plan_for(g.nzp), px = plan_for(g.nxp);
+  const FFTPlan pz = fft_make_plan(g.nzp), px = fft_make_plan(g.nxp);
   if (pz.npass < 0 || px.npass < 0) return SGPU_E_PARAM;
   unsigned char* area = nullptr;
   int rc = area_for_current_device(&area);

@@ -96,27 +96,9 @@ static int cuda_fail(cudaError_t e, const char* where) {
     if (_r) return _r;                               \
   } while (0)
 
-static FFTPlan make_plan(int n) {
-  FFTPlan p{};
-  p.n = n;
-  int m = n, k = 0;
-  while (m % 4 == 0) { p.radix[k++] = 4; m /= 4; }
-  while (m % 2 == 0) { p.radix[k++] = 2; m /= 2; }
-  while (m % 3 == 0) { p.radix[k++] = 3; m /= 3; }
-  while (m % 5 == 0) { p.radix[k++] = 5; m /= 5; }
-  p.npass = (m == 1) ? k : -1;
-  int ns = 1;
-  for (int i = 0; i < k; ++i) {
-    p.ns[i] = ns;
-    p.magic[i] = (ns == 1) ? 0u : (unsigned)((((unsigned long long)1 << 32) + ns - 1) / ns);
-    p.tstep[i] = n / (ns * p.radix[i]);
-    ns *= p.radix[i];
-  }
-  return p;
-}
 
 static int make_tw(Tw& t, int n) {
-  t.plan = make_plan(n);
+  t.plan = fft_make_plan(n);
   if (t.plan.npass < 0) return SGPU_E_PARAM;
   std::vector<double2> hd(n);
   std::vector<float2> hf(n);

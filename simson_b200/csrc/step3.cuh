@@ -277,25 +277,35 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   double* __restrict__ VH = B.VH + p;
   double* __restrict__ DVH = B.DVH + p;
 
-  // nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340)
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const size_t o = j * NP;
-    const double2 h1 = H1[o], h3 = H3[o], pw = PW[o];
-    G[o] = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
-    const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
-    HOM[o] = hom;
-    FW[o] = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
-  }
-  cheb_deriv(col_re(B.DG, p, NP), col_re(B.G, p, NP), n);
-  cheb_deriv(col_im(B.DG, p, NP), col_im(B.G, p, NP), n);
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const size_t o = j * NP;
-    const double2 dg = DG[o], h2 = H2[o], pv = PV[o];
-    const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
-    HV[o] = hv;
-    FV[o] = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
+  // Nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340) in
+  // one backward sweep: g = i alpha H1 + i beta H3 and its y-derivative by the
+  // dcheb recurrence dg_j = dg_{j+2} + 2(j+1) g_{j+1} (same operations as
+  // cheb_deriv), hv = -(dg + k^2 H2), homy = i beta H1 - i alpha H3,
+  // f_v = p_v - c1 hv, f_omega = p_omega - c1 homy.
+  {
+    double2 g1 = double2{0.0, 0.0};                   // g_{j+1}
+    double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
+    for (int j = n - 1; j >= 0; --j) {
+      const size_t o = j * NP;
+      const double2 h1 = H1[o], h2 = H2[o], h3 = H3[o], pv = PV[o], pw = PW[o];
+      double2 dg;
+      if (j == n - 1) {
+        dg = double2{0.0, 0.0};
+      } else {
+        const double f = 2.0 * (double)(j + 1);
+        dg = (j == n - 2) ? double2{f * g1.x, f * g1.y} : double2{d2.x + f * g1.x, d2.y + f * g1.y};
+      }
+      d2 = d1;
+      d1 = dg;
+      if (j == 0) dg = double2{0.5 * dg.x, 0.5 * dg.y};
+      g1 = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
+      const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
+      HOM[o] = hom;
+      FW[o] = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
+      const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
+      HV[o] = hv;
+      FV[o] = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
+    }
   }
   // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
   {
@@ -311,7 +321,9 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     const double bc1[3] = {0, 0, 0}, bc2[3] = {0, 0, 0};
     tau_solve<3>(k2, n, f, x, bc1, bc2, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
   }
-  // dv/dy = 0 at the walls: add the homogeneous solution per parity (linearbl.f:1020-1085)
+  // dv/dy = 0 at the walls: add the homogeneous solution per parity
+  // (linearbl.f:1020-1085).  The parity sums of dv run in ascending order as
+  // in the reference, so dv and dvh are stored by a backward derivative sweep.
   cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
   cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
   cheb_deriv(col_r(B.DVH, p, NP), col_r(B.VH, p, NP), n);
@@ -328,50 +340,58 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     cvr[1 - is] = (0.0 - sr) * cinv;
     cvi[1 - is] = (0.0 - si) * cinv;
   }
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const size_t o = j * NP;
-    const double vh = VH[o];
-    const double2 v = V[o];
-    V[o] = double2{v.x + cvr[j & 1] * vh, v.y + cvi[j & 1] * vh};
-  }
-  // phi from the final v (tau: phi = D^2 v - k^2 v), derivatives (linearbl.f:1160-1170)
-  cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
-  cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
-  cheb_deriv(col_re(B.T1, p, NP), col_re(B.DV, p, NP), n);
-  cheb_deriv(col_im(B.T1, p, NP), col_im(B.DV, p, NP), n);
-  cheb_deriv(col_re(B.DOM, p, NP), col_re(B.OM, p, NP), n);
-  cheb_deriv(col_im(B.DOM, p, NP), col_im(B.OM, p, NP), n);
-  // u, w, omega_x, omega_z (linearbl.f:1193-1212)
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const size_t o = j * NP;
-    const double2 v = V[o], t1 = T1[o], dv = DV[o], om = OM[o], dom = DOM[o];
-    const double2 phi = double2{t1.x - k2 * v.x, t1.y - k2 * v.y};
-    PHI[o] = phi;
-    OU[o] = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
-    OW[o] = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
-    OZ[o] = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
-    OX[o] = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
-    OV[o] = v;
-  }
-  // partial right-hand sides of the next stage (linearbl.f:1696-1800, tau branch)
-  cheb_deriv(col_re(B.T1, p, NP), col_re(B.PHI, p, NP), n);
-  cheb_deriv(col_im(B.T1, p, NP), col_im(B.PHI, p, NP), n);
-  cheb_deriv(col_re(B.T2, p, NP), col_re(B.T1, p, NP), n);
-  cheb_deriv(col_im(B.T2, p, NP), col_im(B.T1, p, NP), n);
-  cheb_deriv(col_re(B.T1, p, NP), col_re(B.DOM, p, NP), n);
-  cheb_deriv(col_im(B.T1, p, NP), col_im(B.DOM, p, NP), n);
-  const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
-  const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
-  const double k2m = k2 - c1n;
-#pragma unroll 4
-  for (int j = 0; j < n; ++j) {
-    const size_t o = j * NP;
-    const double2 d2phi = T2[o], phi = PHI[o], hv = HV[o];
-    const double2 d2om = T1[o], om = OM[o], hom = HOM[o];
-    PV[o] = double2{-d2phi.x + k2m * phi.x - c2 * hv.x, -d2phi.y + k2m * phi.y - c2 * hv.y};
-    PW[o] = double2{-d2om.x + k2m * om.x - c2 * hom.x, -d2om.y + k2m * om.y - c2 * hom.y};
+  // One backward sweep for everything after the superposition: the final v,
+  // its first and second derivative, phi = D^2 v - k^2 v (tau, linearbl.f:
+  // 1160-1170), D phi, D^2 phi, D omega_y, D^2 omega_y (chained dcheb
+  // recurrences; each level's halving of coefficient 0 only touches its last
+  // value), then u, w, omega_x, omega_z (loop 2800, :1193-1212) and the next
+  // partial right-hand sides (:1696-1800).
+  {
+    const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
+    const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
+    const double k2m = k2 - c1n;
+    // value at j+1 and derivative values at j+1, j+2 of each chain
+    double2 v1 = {0, 0}, dv1 = {0, 0}, dv2 = {0, 0}, ddv1 = {0, 0}, ddv2 = {0, 0};
+    double2 ph1 = {0, 0}, dph1 = {0, 0}, dph2 = {0, 0}, ddph1 = {0, 0}, ddph2 = {0, 0};
+    double2 om1 = {0, 0}, dom1 = {0, 0}, dom2 = {0, 0}, ddom1 = {0, 0}, ddom2 = {0, 0};
+    auto step = [&](double2 x1, double2& b1, double2& b2, int j) -> double2 {
+      // b_j from b_{j+2} = b2 and x_{j+1} = x1; updates (b1, b2) <- (b_j, b_{j+1})
+      double2 b;
+      if (j == n - 1) {
+        b = double2{0.0, 0.0};
+      } else {
+        const double f = 2.0 * (double)(j + 1);
+        b = (j == n - 2) ? double2{f * x1.x, f * x1.y} : double2{b2.x + f * x1.x, b2.y + f * x1.y};
+      }
+      b2 = b1;
+      b1 = b;
+      return (j == 0) ? double2{0.5 * b.x, 0.5 * b.y} : b;
+    };
+    for (int j = n - 1; j >= 0; --j) {
+      const size_t o = j * NP;
+      const double vh = VH[o];
+      const double2 vp = V[o];
+      const double2 v = double2{vp.x + cvr[j & 1] * vh, vp.y + cvi[j & 1] * vh};
+      const double2 om = OM[o], hv = HV[o], hom = HOM[o];
+      const double2 dv = step(v1, dv1, dv2, j);
+      // second derivative from the first derivative at j+1 (before halving)
+      const double2 ddv = step(dv2, ddv1, ddv2, j);
+      const double2 phi = double2{ddv.x - k2 * v.x, ddv.y - k2 * v.y};
+      const double2 dph = step(ph1, dph1, dph2, j);
+      const double2 ddph = step(dph2, ddph1, ddph2, j);
+      const double2 dom = step(om1, dom1, dom2, j);
+      const double2 ddom = step(dom2, ddom1, ddom2, j);
+      OU[o] = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
+      OW[o] = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
+      OZ[o] = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
+      OX[o] = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
+      OV[o] = v;
+      PV[o] = double2{-ddph.x + k2m * phi.x - c2 * hv.x, -ddph.y + k2m * phi.y - c2 * hv.y};
+      PW[o] = double2{-ddom.x + k2m * om.x - c2 * hom.x, -ddom.y + k2m * om.y - c2 * hom.y};
+      v1 = v;
+      ph1 = phi;
+      om1 = om;
+    }
   }
 }
 

@@ -92,3 +92,19 @@ def test_cheb_deriv_bitwise(libs, n):
     assert np.array_equal(b, b_ref)
     # and it is the derivative: compare with numpy's Chebyshev derivative
     np.testing.assert_allclose(b[:-1], np.polynomial.chebyshev.chebder(a), rtol=1e-12, atol=1e-10)
+
+
+@pytest.mark.parametrize("n", [8, 9, 12, 18, 32, 72, 96, 128, 192, 240, 256, 288, 384, 576])
+def test_fft_passes_match_numpy(n):
+    """The radix-8/9/6/4/2/3/5 Stockham passes of every transform of the step
+    (host build of the device source) against numpy's FFT, both signs."""
+    host = ctypes.CDLL(sbuild.build_hostcheck())
+    host.sbh_fft.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int]
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    inp = np.ascontiguousarray(np.stack([x.real, x.imag], -1).ravel())
+    out = np.zeros(2 * n)
+    for sign, ref in ((-1, np.fft.fft(x)), (1, np.fft.ifft(x) * n)):
+        assert host.sbh_fft(n, P(inp), P(out), sign) > 0
+        y = out[0::2] + 1j * out[1::2]
+        assert np.abs(y - ref).max() <= 1e-15 * n * np.abs(ref).max()
