@@ -100,35 +100,40 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def substep_bytes(nc, s_bytes):
-    # algorithmic main-storage traffic of one substep: step 2 reads 5 fields and
-    # writes 3, step 3 reads 5 and writes 7 (20 field passes)
-    return 20 * nc * s_bytes
+def substep_bytes(nc, precision):
+    """Algorithmic main-storage traffic of one substep: step 2 reads 5 fields
+    and writes 3, step 3 reads 5 and writes 7 (20 field passes), at the
+    storage precision of each field: FP64 everywhere, or under the mixed
+    path FP32 for u, v, w, omega_x, omega_z and H (16 passes) and FP64 for
+    p_v, p_omega (4 passes)."""
+    if precision == "fp64":
+        return 20 * nc * 16
+    return 16 * nc * 8 + 4 * nc * 16
 
 
-def kernel_bytes(name, w):
-    """Algorithmic (compulsory) HBM bytes of one launch of each kernel, FP64."""
+def kernel_bytes(name, w, precision="fp64"):
+    """Algorithmic (compulsory) HBM bytes of one launch of each kernel."""
     nx2, ny, nz = w["nx"] // 2, w["ny"], w["nz"]
     nzp = nz + nz // 2
-    c = 16
+    c = 16 if precision == "fp64" else 8
     fld = nx2 * ny * nz * c          # one spectral field
     fine = nx2 * ny * nzp * c        # one z-transformed field on the 3/2 z grid
+    f64 = nx2 * ny * nz * 16         # a field kept in FP64 (Chebyshev-space scratch of step 3)
     return {
         "zinv": 5 * fld + 6 * fine,
         "xpass": 6 * fine + 3 * fine,
         "zfwd": 3 * fine + 3 * fld,
-        "cheb_fwd": 3 * fld + 3 * fld,
-        "cheb_inv": 5 * fld + 5 * fld,
+        "cheb_fwd": 3 * fld + 3 * f64,
+        "cheb_inv": 5 * f64 + 5 * fld,
     }.get(name)
 
 
-def own_arm(args, rank, world):
+def own_arm(args, rank, world, precision):
     from simson_b200.bla import Channel, PinnedArray, FP64, MIXED
     from simson_b200.fields import channel_field
-    import ctypes
 
     w = WORKLOAD
-    prec = MIXED if args.precision == "mixed" else FP64
+    prec = MIXED if precision == "mixed" else FP64
     dev = int(os.environ.get("LOCAL_RANK", 0))
     ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], precision=prec, device=dev)
     u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"] + rank)
@@ -149,6 +154,7 @@ def own_arm(args, rank, world):
     clocks = clk.stop()
     ms = dist_max(ms, world)
     sc = ch.scalars()
+    uvw = ch.state(3)  # after warm-up + timed steps, for the mixed-vs-FP64 comparison
     # per-kernel times (a separate, profiled run of 2 steps)
     ch.profile(True)
     ch.step(2)
@@ -175,7 +181,7 @@ def own_arm(args, rank, world):
     finite = bool(np.isfinite(sc["px"]))
     ch.close()
     return dict(ms=ms, launches=launches, clocks=clocks, prof=prof, e2e_s=e2e_s, e2e_steps=e2e_steps,
-                e2e_bytes=nbytes, scalars=sc, finite=finite)
+                e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw)
 
 
 def dist_barrier(world):
@@ -222,7 +228,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="both: time FP64 and mixed; value is the mixed-precision step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -240,6 +247,7 @@ def main():
               "precision": args.precision, "l2": "state 1.6 GB > L2, no flush needed",
               "parallelism": f"replicas x{args.gpus}"}
     if args.impl == "reference":
+        config["precision"] = "fp64 (the reference computes in double precision)"
         if rank != 0:
             return
         try:
@@ -254,12 +262,16 @@ def main():
                                           "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
-    res = own_arm(args, rank, world)
+    runs = {}
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+        runs[prec] = own_arm(args, rank, world, prec)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank != 0:
         return
+    head = "mixed" if "mixed" in runs else "fp64"
+    res = runs[head]
     steps_per_s = args.steps / (res["ms"] / 1000.0) * args.gpus
     ms_step = res["ms"] / args.steps
     hbm, peak_kind = peaks()
@@ -268,7 +280,7 @@ def main():
     # dominant kernel by measured time
     dom = max((k for k in prof if k not in ("other",) and prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms = prof[dom][0] / prof[dom][1]
-    dom_bytes = kernel_bytes(dom, w)
+    dom_bytes = kernel_bytes(dom, w, head)
     roof = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
             "traffic": None, "launch_ms": dom_ms}
     if dom_bytes:
@@ -276,12 +288,15 @@ def main():
         roof.update(achieved=ach, frac=ach / hbm, algorithmic_bytes=dom_bytes)
     else:
         roof.update(achieved=None, frac=None, algorithmic_bytes=None)
-    stage_bytes = substep_bytes(nc, 16)
+    stage_bytes = substep_bytes(nc, head)
     step_ach = 3 * stage_bytes / (ms_step / 1000.0) / 1e9
+    config["precision"] = {"mixed": "mixed: FP32 x/z FFTs, products, Chebyshev transforms and u,v,w,omega storage; "
+                                    "FP64 tau solves, mean flow, partial RHS",
+                           "fp64": "fp64: every transform and solve in FP64"}[head]
     line = {
         "metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
         "config": config,
         "grid_point_stages_per_s": w["nx"] * w["ny"] * w["nz"] * 3 * steps_per_s,
         "roofline": roof,
@@ -294,6 +309,18 @@ def main():
         "clocks": res["clocks"],
         "finite": res["finite"],
     }
+    if "fp64" in runs and "mixed" in runs:
+        r64 = runs["fp64"]
+        sps64 = args.steps / (r64["ms"] / 1000.0) * args.gpus
+        errs = [float(np.linalg.norm(runs["mixed"]["uvw"][k] - r64["uvw"][k]) / np.linalg.norm(r64["uvw"][k]))
+                for k in range(3)]
+        line["fp64"] = {"value": sps64, "ms_per_step": r64["ms"] / args.steps,
+                        "kernel_ms_per_substep": {k: (v[0] / max(v[1], 1)) for k, v in r64["prof"].items() if v[1]},
+                        "e2e": r64["e2e_steps"] / r64["e2e_s"] * args.gpus}
+        line["mixed_over_fp64"] = steps_per_s / sps64
+        line["mixed_vs_fp64_rel_l2_uvw"] = {"after_steps": args.warmup + args.steps, "u": errs[0], "v": errs[1],
+                                            "w": errs[2]}
+        line["gpu_launches"] += r64["launches"]
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference(1, threads, "bounded sample")

@@ -159,18 +159,18 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   const size_t s_z = 2 * (size_t)g.nzp * KB * sizeof(double2);
   const size_t s_x = 2 * (size_t)g.nxp * 3 * RB * sizeof(double2);
   if (s_z > 227 * 1024 || s_x > 227 * 1024) return SGPU_E_PARAM;
-  cudaFuncSetAttribute(k_zinv<double, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<double, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zinv<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zfwd<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
   cudaFuncSetAttribute(k_xpass<double, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
   const double2* in = static_cast<const double2*>(fields_in);
   double2* out = static_cast<double2*>(h_out);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
-  k_zinv<double, KB><<<gz, TH, s_z, st>>>(in, zb, g, pz, twz, alfa, beta);
+  k_zinv<double, KB, double><<<gz, TH, s_z, st>>>(in, zb, g, pz, twz, alfa, beta);
   dim3 gx((g.nzp + RB - 1) / RB, g.nyp);
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
   k_xpass<double, RB><<<gx, TH, s_x, st>>>(zb, xb, g, px, twx, dyi, dxi, dzi, P.rot, cfl_bits);
-  k_zfwd<double, KB><<<gz, TH, s_z, st>>>(xb, out, g, pz, twz);
+  k_zfwd<double, KB, double><<<gz, TH, s_z, st>>>(xb, out, g, pz, twz);
   if (cudaGetLastError() != cudaSuccess) return SGPU_E_CUDA;
   if (cflp_max) {
     unsigned long long bits = 0;

@@ -40,7 +40,9 @@ struct sgpu_ctx {
   cudaEvent_t fork = nullptr, join = nullptr;
   cudaEvent_t ev[16] = {};
   // resident state
-  double2* st = nullptr;     // [7][nyp][NP]
+  double2* st = nullptr;     // [7][nyp][NP]; SGPU_MIXED keeps only slots 5-6 (p_v, p_omega) here
+  float2* stf = nullptr;     // SGPU_MIXED: slots 0-4 (u, v, w, omega_x, omega_z / H) in FP32
+  bool mixed = false;
   double* puw = nullptr;     // [2][ny]
   double* scal = nullptr;    // [0] px, [1] mflux
   unsigned long long* cfl_bits = nullptr;
@@ -66,6 +68,7 @@ struct sgpu_ctx {
   bool have_state = false;
   long long launches = 0;
   static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 128;
+  static constexpr int kbf = 8, rbf = 2, pbf = 8;  // FP32 tiles (same shared memory as FP64)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
   std::vector<cudaEvent_t> pev;
@@ -146,6 +149,46 @@ __global__ void k_to_ref(const double2* __restrict__ st, double* __restrict__ re
   }
 }
 
+// SGPU_MIXED: slots 0-4 live in FP32 (stf), slots 5-6 in FP64 (st)
+__global__ void k_from_ref_mixed(const double* __restrict__ re, const double* __restrict__ im,
+                                 double2* __restrict__ st, float2* __restrict__ stf, Dims g, int nslots) {
+  const size_t tot = (size_t)nslots * g.nyp * g.NP;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    size_t r = i;
+    const int x = r % g.nx2; r /= g.nx2;
+    const int y = r % g.nyp; r /= g.nyp;
+    const int z = r % g.nz; r /= g.nz;
+    const int s = (int)r;
+    const size_t o = ((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x;
+    if (s < 5)
+      stf[o] = float2{(float)re[i], (float)im[i]};
+    else
+      st[o] = double2{re[i], im[i]};
+  }
+}
+
+__global__ void k_to_ref_mixed(const double2* __restrict__ st, const float2* __restrict__ stf,
+                               double* __restrict__ re, double* __restrict__ im, Dims g, int nslots) {
+  const size_t tot = (size_t)nslots * g.nyp * g.NP;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    size_t r = i;
+    const int x = r % g.nx2; r /= g.nx2;
+    const int y = r % g.nyp; r /= g.nyp;
+    const int z = r % g.nz; r /= g.nz;
+    const int s = (int)r;
+    const size_t o = ((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x;
+    if (s < 5) {
+      const float2 v = stf[o];
+      re[i] = (double)v.x;
+      im[i] = (double)v.y;
+    } else {
+      const double2 v = st[o];
+      re[i] = v.x;
+      im[i] = v.y;
+    }
+  }
+}
+
 __global__ void k_cfl_reset(unsigned long long* c) { *c = 0ull; }
 
 // ---------------------------------------------------------------------------
@@ -169,10 +212,11 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   *out = nullptr;
   const sgpu_params& P = *prm;
   if (P.nx < 4 || P.nz < 4 || P.nx % 4 || P.nz % 2 || P.ny < 9 || (P.ny % 2) == 0 || P.nst != 3 || !(P.dt > 0) ||
-      !(P.re > 0) || !(P.xl > 0) || !(P.zl > 0) || P.precision != SGPU_FP64)
+      !(P.re > 0) || !(P.xl > 0) || !(P.zl > 0) || (P.precision != SGPU_FP64 && P.precision != SGPU_MIXED))
     return SGPU_E_PARAM;
   sgpu_ctx* c = new sgpu_ctx();
   c->prm = P;
+  c->mixed = (P.precision == SGPU_MIXED);
   Dims& g = c->g;
   g.nx = P.nx; g.ny = P.ny; g.nz = P.nz;
   g.nx2 = P.nx / 2; g.nyp = P.ny;
@@ -207,6 +251,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
+  if (c->mixed && cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess) return fail(SGPU_E_CUDA);
   cudaMemset(c->st, 0, 7 * fld * sizeof(double2));
   cudaMemset(c->puw, 0, 2 * g.ny * sizeof(double));
   // wavenumbers (bla/preprbl.f:36-43) and CFL grid spacing (bla/boxcfl.f:25-56)
@@ -236,10 +281,19 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
   const size_t s_y = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
   if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024) return fail(SGPU_E_PARAM);
-  cudaFuncSetAttribute(k_zinv<double, sgpu_ctx::kb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<double, sgpu_ctx::kb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zinv<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zfwd<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
   cudaFuncSetAttribute(k_xpass<double, sgpu_ctx::rb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
-  cudaFuncSetAttribute(k_cheb<double, sgpu_ctx::pb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_y);
+  cudaFuncSetAttribute(k_cheb<double, sgpu_ctx::pb, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)s_y);
+  // FP32 variants: twice the columns in the same shared memory
+  cudaFuncSetAttribute(k_zinv<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_zfwd<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
+  cudaFuncSetAttribute(k_xpass<float, sgpu_ctx::rbf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
+  cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)s_y);
+  cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)s_y);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -249,7 +303,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->st, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+  void* ptrs[] = {c->st, c->stf, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -269,7 +323,10 @@ extern "C" int sgpu_upload_state(sgpu_ctx* c, const double* ur, const double* ui
   const size_t n = (size_t)nslots * c->g.nyp * c->g.NP;
   CK(cudaMemcpyAsync(c->stage, ur, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->stage + n, ui, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  k_from_ref<<<592, 256, 0, c->stream>>>(c->stage, c->stage + n, c->st, c->g, nslots);
+  if (c->mixed)
+    k_from_ref_mixed<<<592, 256, 0, c->stream>>>(c->stage, c->stage + n, c->st, c->stf, c->g, nslots);
+  else
+    k_from_ref<<<592, 256, 0, c->stream>>>(c->stage, c->stage + n, c->st, c->g, nslots);
   c->launches++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
@@ -280,7 +337,10 @@ extern "C" int sgpu_upload_state(sgpu_ctx* c, const double* ur, const double* ui
 extern "C" int sgpu_download_state(sgpu_ctx* c, double* ur, double* ui, int nslots) {
   if (!c || !ur || !ui || nslots < 1 || nslots > 7) return SGPU_E_PARAM;
   const size_t n = (size_t)nslots * c->g.nyp * c->g.NP;
-  k_to_ref<<<592, 256, 0, c->stream>>>(c->st, c->stage, c->stage + n, c->g, nslots);
+  if (c->mixed)
+    k_to_ref_mixed<<<592, 256, 0, c->stream>>>(c->st, c->stf, c->stage, c->stage + n, c->g, nslots);
+  else
+    k_to_ref<<<592, 256, 0, c->stream>>>(c->st, c->stage, c->stage + n, c->g, nslots);
   c->launches++;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ur, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -307,14 +367,38 @@ static double2* czf(sgpu_ctx* c, int k) { return c->cz + (size_t)k * c->g.nyp * 
 static double* rzf(sgpu_ctx* c, int k) { return c->rz + (size_t)k * c->g.nyp * c->g.NP; }
 static double2* slot(sgpu_ctx* c, int s) { return c->st + (size_t)s * c->g.nyp * c->g.NP; }
 
-static void launch_cheb(sgpu_ctx* c, const double2* in, size_t in_fs, double2* out, size_t out_fs, int nfields,
-                        int inverse, double scale, int skip_oddball) {
+template <class T, int PB, class SI, class SO>
+static void launch_cheb_t(sgpu_ctx* c, const typename C2<SI>::type* in, size_t in_fs, typename C2<SO>::type* out,
+                          size_t out_fs, int nfields, int inverse, double scale, int skip_oddball,
+                          const typename C2<T>::type* tw) {
   const Dims& g = c->g;
-  dim3 grid((g.NP + c->pb - 1) / c->pb, nfields);
-  const size_t sm = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
-  k_cheb<double, sgpu_ctx::pb><<<grid, sgpu_ctx::fft_threads, sm, c->stream>>>(
-      in, in_fs, out, out_fs, g, inverse, scale, c->twy.plan, c->twy.d, skip_oddball);
+  dim3 grid((g.NP + PB - 1) / PB, nfields);
+  const size_t sm = smem_fft(2 * (g.nyp - 1), PB, sizeof(typename C2<T>::type));
+  k_cheb<T, PB, SI, SO><<<grid, sgpu_ctx::fft_threads, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse, scale,
+                                                                        c->twy.plan, tw, skip_oddball);
   c->launches++;
+}
+
+// Chebyshev transform of nfields y-pencil fields.  Physical-y fields live in
+// the state (FP64, or FP32 under SGPU_MIXED); Chebyshev-y fields are FP64.
+static void cheb_to_spec(sgpu_ctx* c, int slot0, double2* out, int nfields, double scale) {
+  const size_t fld = (size_t)c->g.nyp * c->g.NP;
+  if (c->mixed)
+    launch_cheb_t<float, sgpu_ctx::pbf, float, double>(c, c->stf + slot0 * fld, fld, out, fld, nfields, 0, scale, 0,
+                                                       c->twy.f);
+  else
+    launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->st + slot0 * fld, fld, out, fld, nfields, 0, scale, 0,
+                                                        c->twy.d);
+}
+
+static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields, int skip_oddball) {
+  const size_t fld = (size_t)c->g.nyp * c->g.NP;
+  if (c->mixed)
+    launch_cheb_t<float, sgpu_ctx::pbf, double, float>(c, in, fld, c->stf + slot0 * fld, fld, nfields, 1, 1.0,
+                                                       skip_oddball, c->twy.f);
+  else
+    launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, in, fld, c->st + slot0 * fld, fld, nfields, 1, 1.0,
+                                                        skip_oddball, c->twy.d);
 }
 
 extern "C" int sgpu_prhs(sgpu_ctx* c) {
@@ -333,7 +417,7 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   c->t = 0.0;
   c->tc = 0.0;
   // Chebyshev coefficients of u, v, w
-  launch_cheb(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0, 0);
+  cheb_to_spec(c, 0, czf(c, 0), 3, 1.0);
   PrhsBufs B;
   B.U1 = czf(c, 0); B.U2 = czf(c, 1); B.U3 = czf(c, 2);
   B.OMY = czf(c, 3); B.OX = czf(c, 4); B.OZ = czf(c, 5); B.PHI = czf(c, 6); B.T1 = czf(c, 7); B.T2 = czf(c, 8);
@@ -341,7 +425,8 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   k_prhs<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, c->prm.re, c->anp1);
   c->launches++;
   // omega_x, omega_z back to physical y into slots 3, 4
-  launch_cheb(c, czf(c, 4), fld, slot(c, 3), fld, 2, 1, 1.0, 0);
+  cheb_to_phys(c, czf(c, 4), 3, 2, 0);
+  (void)fld;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
@@ -361,19 +446,37 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   }
   dim3 gz((g.nx2 + c->kb - 1) / c->kb, g.nyp);
   const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
-  prof_mark(c, K_ZINV);
-  k_zinv<double, sgpu_ctx::kb><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->st, c->zb, g, c->twz.plan, c->twz.d,
-                                                                              c->alfa, c->beta);
-  dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
-  const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
-  prof_mark(c, K_XPASS);
-  k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::fft_threads, s_x, c->stream>>>(
-      c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, do_cfl ? c->cfl_bits : nullptr);
-  prof_mark(c, K_ZFWD);
-  k_zfwd<double, sgpu_ctx::kb><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->xb, c->st, g, c->twz.plan,
-                                                                              c->twz.d);
+  const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
+  unsigned long long* cflp = do_cfl ? c->cfl_bits : nullptr;
+  if (c->mixed) {
+    // FP32 transforms and products on the FP32 velocity/vorticity fields
+    float2* zbf = reinterpret_cast<float2*>(c->zb);
+    float2* xbf = reinterpret_cast<float2*>(c->xb);
+    dim3 gzf((g.nx2 + sgpu_ctx::kbf - 1) / sgpu_ctx::kbf, g.nyp);
+    dim3 gxf((g.nzp + sgpu_ctx::rbf - 1) / sgpu_ctx::rbf, g.nyp);
+    prof_mark(c, K_ZINV);
+    k_zinv<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+        c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta);
+    prof_mark(c, K_XPASS);
+    k_xpass<float, sgpu_ctx::rbf><<<gxf, sgpu_ctx::fft_threads, s_x, c->stream>>>(
+        zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp);
+    prof_mark(c, K_ZFWD);
+    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(xbf, c->stf, g, c->twz.plan,
+                                                                                        c->twz.f);
+  } else {
+    prof_mark(c, K_ZINV);
+    k_zinv<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+        c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta);
+    dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
+    prof_mark(c, K_XPASS);
+    k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::fft_threads, s_x, c->stream>>>(
+        c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, cflp);
+    prof_mark(c, K_ZFWD);
+    k_zfwd<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->xb, c->st, g,
+                                                                                        c->twz.plan, c->twz.d);
+  }
   c->launches += 3;
   if (do_cfl) c->cfl_pending = true;
   return cuda_fail(cudaGetLastError(), "nonlin launch");
@@ -393,7 +496,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   RKc rk{c->an, c->bn, c->anp1, c->bnp1};
   // Chebyshev transform of H, normalised by 1/(nxp nzp) (linearbl.f:262-273)
   prof_mark(c, K_CHEB_FWD);
-  launch_cheb(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0 / ((double)g.nxp * (double)g.nzp), 0);
+  cheb_to_spec(c, 0, czf(c, 0), 3, 1.0 / ((double)g.nxp * (double)g.nzp));
   PencilBufs B;
   B.H1 = czf(c, 0); B.H2 = czf(c, 1); B.H3 = czf(c, 2);
   B.PV = slot(c, 5); B.PW = slot(c, 6);
@@ -421,7 +524,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
-  launch_cheb(c, B.OU, fld, slot(c, 0), fld, 5, 1, 1.0, 1);
+  cheb_to_phys(c, B.OU, 0, 5, 1);
   prof_mark(c, K_OTHER);
   c->launches += 2;
   // bla/bla.f:2598-2607

@@ -23,8 +23,8 @@
 
 namespace sb {
 
-template <class T, int KB>
-__global__ void k_zinv(const double2* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
+template <class T, int KB, class S>
+__global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
                        FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
                        const double* __restrict__ alfa, const double* __restrict__ beta) {
   typedef typename C2<T>::type V;
@@ -51,12 +51,12 @@ __global__ void k_zinv(const double2* __restrict__ st, typename C2<T>::type* __r
       if (iz >= 0 && kx < g.nx2) {
         const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
         if (f == 4) {
-          const double2 u = st[off];
-          const double2 w = st[2 * slot + off];
+          const auto u = st[off];
+          const auto w = st[2 * slot + off];
           const double a = alfa[kx], be = beta[iz];
-          val = V{(T)(-be * u.y + a * w.y), (T)(be * u.x - a * w.x)};
+          val = V{(T)(-be * (double)u.y + a * (double)w.y), (T)(be * (double)u.x - a * (double)w.x)};
         } else {
-          const double2 q = st[src_slot[f] * slot + off];
+          const auto q = st[src_slot[f] * slot + off];
           val = V{(T)q.x, (T)q.y};
         }
       }
@@ -170,8 +170,8 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
   }
 }
 
-template <class T, int KB>
-__global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, double2* __restrict__ st, Dims g,
+template <class T, int KB, class S>
+__global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<S>::type* __restrict__ st, Dims g,
                        FFTPlan plan, const typename C2<T>::type* __restrict__ tw) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -198,7 +198,7 @@ __global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, double2* __r
       if (kx >= g.nx2) continue;
       const int m = (iz < nzh) ? iz : iz + (g.nzp - g.nz);
       const V h = res[m * KB + b];
-      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = double2{(double)h.x, (double)h.y};
+      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = typename C2<S>::type{(S)h.x, (S)h.y};
     }
     __syncthreads();
   }

@@ -195,10 +195,10 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
 // ---------------------------------------------------------------------------
 // Chebyshev transforms over pencils
 // ---------------------------------------------------------------------------
-template <class T, int PB>
-__global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __restrict__ out, size_t out_fs,
-                       Dims g, int inverse, double scale, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       int skip_oddball) {
+template <class T, int PB, class SI, class SO>
+__global__ void k_cheb(const typename C2<SI>::type* __restrict__ in, size_t in_fs,
+                       typename C2<SO>::type* __restrict__ out, size_t out_fs, Dims g, int inverse, double scale,
+                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw, int skip_oddball) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = g.nyp;
@@ -208,13 +208,17 @@ __global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __
   V* b1 = b0 + (size_t)L * PB;
   const int f = blockIdx.y;
   const int p0 = blockIdx.x * PB;
-  const double2* src = in + f * in_fs;
-  double2* dst = out + f * out_fs;
+  const typename C2<SI>::type* src = in + f * in_fs;
+  typename C2<SO>::type* dst = out + f * out_fs;
   for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
     const int j = t / PB;
     const int b = t - j * PB;
     const int p = p0 + b;
-    double2 v = (p < g.NP) ? src[(size_t)j * g.NP + p] : double2{0.0, 0.0};
+    double2 v = double2{0.0, 0.0};
+    if (p < g.NP) {
+      const auto q = src[(size_t)j * g.NP + p];
+      v = double2{(double)q.x, (double)q.y};
+    }
     if (inverse) {
       const double cb = (j == 0 || j == N) ? 1.0 : 0.5;
       v.x *= cb;
@@ -235,7 +239,7 @@ __global__ void k_cheb(const double2* __restrict__ in, size_t in_fs, double2* __
     const V e = res[k * PB + b];
     double fac = scale;
     if (!inverse) fac = scale / ((double)N * ((k == 0 || k == N) ? 2.0 : 1.0));
-    dst[(size_t)k * g.NP + p] = double2{(double)e.x * fac, (double)e.y * fac};
+    dst[(size_t)k * g.NP + p] = typename C2<SO>::type{(SO)((double)e.x * fac), (SO)((double)e.y * fac)};
   }
 }
 
