@@ -165,12 +165,12 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   const double2* in = static_cast<const double2*>(fields_in);
   double2* out = static_cast<double2*>(h_out);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
-  k_zinv<double, KB, double><<<gz, TH, s_z, st>>>(in, zb, g, pz, twz, alfa, beta);
+  k_zinv<double, KB, double><<<gz, TH, s_z, st>>>(in, zb, g, pz, twz, alfa, beta, 0);
   dim3 gx((g.nzp + RB - 1) / RB, g.nyp);
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
-  k_xpass<double, RB><<<gx, TH, s_x, st>>>(zb, xb, g, px, twx, dyi, dxi, dzi, P.rot, cfl_bits);
-  k_zfwd<double, KB, double><<<gz, TH, s_z, st>>>(xb, out, g, pz, twz);
+  k_xpass<double, RB><<<gx, TH, s_x, st>>>(zb, xb, g, px, twx, dyi, dxi, dzi, P.rot, cfl_bits, nullptr);
+  k_zfwd<double, KB, double><<<gz, TH, s_z, st>>>(xb, out, g, pz, twz, nullptr, 0.0);
   if (cudaGetLastError() != cudaSuccess) return SGPU_E_CUDA;
   if (cflp_max) {
     unsigned long long bits = 0;

@@ -58,6 +58,7 @@ struct sgpu_ctx {
   double* rz = nullptr;      // real scratch columns, [nrz][nyp][NP]
   int nrz = 0;
   double* mscr = nullptr;    // mean-flow scratch
+  double* meanp = nullptr;   // [4][nyp] U, W, Omega_x, Omega_z for the mixed step 2
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   // RK bookkeeping (host mirror of the reference driver scalars)
@@ -251,7 +252,9 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
-  if (c->mixed && cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if (c->mixed && (cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess ||
+                   cudaMalloc(&c->meanp, 4 * (size_t)g.nyp * sizeof(double)) != cudaSuccess))
+    return fail(SGPU_E_CUDA);
   cudaMemset(c->st, 0, 7 * fld * sizeof(double2));
   cudaMemset(c->puw, 0, 2 * g.ny * sizeof(double));
   // wavenumbers (bla/preprbl.f:36-43) and CFL grid spacing (bla/boxcfl.f:25-56)
@@ -303,7 +306,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->st, c->stf, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+  void* ptrs[] = {c->st, c->stf, c->meanp, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -456,26 +459,30 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     float2* xbf = reinterpret_cast<float2*>(c->xb);
     dim3 gzf((g.nx2 + sgpu_ctx::kbf - 1) / sgpu_ctx::kbf, g.nyp);
     dim3 gxf((g.nzp + sgpu_ctx::rbf - 1) / sgpu_ctx::rbf, g.nyp);
+    // the FFTs carry only the perturbations; the mean profiles enter the
+    // products analytically and their mean-mean product in FP64
     prof_mark(c, K_ZINV);
+    k_mean_profiles<float><<<(g.nyp + 127) / 128, 128, 0, c->stream>>>(c->stf, c->meanp, g);
     k_zinv<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(
-        c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta);
+        c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta, 1);
     prof_mark(c, K_XPASS);
     k_xpass<float, sgpu_ctx::rbf><<<gxf, sgpu_ctx::fft_threads, s_x, c->stream>>>(
-        zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp);
+        zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
     prof_mark(c, K_ZFWD);
-    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(xbf, c->stf, g, c->twz.plan,
-                                                                                        c->twz.f);
+    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+        xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp, P.rot);
+    c->launches++;
   } else {
     prof_mark(c, K_ZINV);
     k_zinv<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
-        c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta);
+        c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta, 0);
     dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
     prof_mark(c, K_XPASS);
     k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::fft_threads, s_x, c->stream>>>(
-        c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, cflp);
+        c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
     prof_mark(c, K_ZFWD);
-    k_zfwd<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(c->xb, c->st, g,
-                                                                                        c->twz.plan, c->twz.d);
+    k_zfwd<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+        c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr, 0.0);
   }
   c->launches += 3;
   if (do_cfl) c->cfl_pending = true;

@@ -23,10 +23,12 @@
 
 namespace sb {
 
+// drop_mean: leave out the kx = kz = 0 mode (the mean profiles U, W,
+// Omega_x, Omega_z), which the mixed-precision path adds back analytically.
 template <class T, int KB, class S>
 __global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
                        FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       const double* __restrict__ alfa, const double* __restrict__ beta) {
+                       const double* __restrict__ alfa, const double* __restrict__ beta, int drop_mean) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* b0 = reinterpret_cast<V*>(smem_raw);
@@ -48,7 +50,7 @@ __global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<
       else if (m > g.nzp - nzh)
         iz = m - (g.nzp - g.nz);
       V val = V{(T)0, (T)0};
-      if (iz >= 0 && kx < g.nx2) {
+      if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
         const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
         if (f == 4) {
           const auto u = st[off];
@@ -83,7 +85,7 @@ template <class T, int RB>
 __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb,
                         Dims g, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
                         const double* __restrict__ dyi, double dxi, double dzi, double rot,
-                        unsigned long long* __restrict__ cfl_bits) {
+                        unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int B = 3 * RB;
@@ -130,13 +132,29 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
     const V z1 = res[j * B + 3 * r + 1];
     const V z2 = res[j * B + 3 * r + 2];
     const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
-    const T h1 = v * (oz + r2) - w * oy;
-    const T h2 = w * ox - u * (oz + r2);
-    const T h3 = u * oy - v * ox;
+    T h1, h2, h3;
+    double ut = (double)u, wt = (double)w;
+    if (mean == nullptr) {
+      h1 = v * (oz + r2) - w * oy;
+      h2 = w * ox - u * (oz + r2);
+      h3 = u * oy - v * ox;
+    } else {
+      // u, w, omega_x, omega_z are perturbations; the plane means U, W,
+      // Omega_x, Omega_z + 2 rot enter term by term so no product of two
+      // O(1) means is rounded here (their W Omega_x - U Omega_z goes to the
+      // kx = kz = 0 mode in FP64, in k_zfwd).  V = Omega_y = 0.
+      const T U = (T)mean[0 * g.nyp + y], W = (T)mean[1 * g.nyp + y];
+      const T Ox = (T)mean[2 * g.nyp + y], Oz = (T)(mean[3 * g.nyp + y] + 2.0 * rot);
+      h1 = v * Oz + (v * oz - (W + w) * oy);
+      h2 = (W * ox + w * Ox - U * oz - u * Oz) + (w * ox - u * oz);
+      h3 = U * oy - v * Ox + (u * oy - v * ox);
+      ut += mean[0 * g.nyp + y];
+      wt += mean[1 * g.nyp + y];
+    }
     oth[j * B2 + 2 * r + 0] = V{h1, h2};
     oth[j * B2 + 2 * r + 1] = V{h3, (T)0};
     if (m0 + r < g.nzp) {
-      const double cl = fabs((double)u) * dxi + fabs((double)v) * dy + fabs((double)w) * dzi;
+      const double cl = fabs(ut) * dxi + fabs((double)v) * dy + fabs(wt) * dzi;
       cmax = fmax(cmax, cl);
     }
   }
@@ -170,9 +188,12 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
   }
 }
 
+// mean != nullptr: add nxp*nzp*(W Omega_x - U (Omega_z + 2 rot)) to the
+// kx = kz = 0 mode of H2 in FP64 (the mean-mean product left out by k_xpass).
 template <class T, int KB, class S>
 __global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<S>::type* __restrict__ st, Dims g,
-                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw) {
+                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
+                       const double* __restrict__ mean, double rot) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* b0 = reinterpret_cast<V*>(smem_raw);
@@ -198,10 +219,29 @@ __global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<
       if (kx >= g.nx2) continue;
       const int m = (iz < nzh) ? iz : iz + (g.nzp - g.nz);
       const V h = res[m * KB + b];
-      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = typename C2<S>::type{(S)h.x, (S)h.y};
+      double hx = (double)h.x, hy = (double)h.y;
+      if (mean != nullptr && f == 1 && iz == 0 && kx == 0) {
+        const double U = mean[0 * g.nyp + y], W = mean[1 * g.nyp + y];
+        const double Ox = mean[2 * g.nyp + y], Oz = mean[3 * g.nyp + y] + 2.0 * rot;
+        hx += (double)g.nxp * (double)g.nzp * (W * Ox - U * Oz);
+      }
+      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = typename C2<S>::type{(S)hx, (S)hy};
     }
     __syncthreads();
   }
 }
 
+}  // namespace sb
+
+namespace sb {
+// Mean profiles U, W, Omega_x, Omega_z (the kx = kz = 0 coefficients of state
+// slots 0, 2, 3, 4) into mean[4][nyp], read by the mixed-precision step 2.
+template <class S>
+__global__ void k_mean_profiles(const typename C2<S>::type* __restrict__ st, double* __restrict__ mean, Dims g) {
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= g.nyp) return;
+  const size_t slot = (size_t)g.nyp * g.NP;
+  const int src[4] = {0, 2, 3, 4};
+  for (int k = 0; k < 4; ++k) mean[k * g.nyp + y] = (double)st[src[k] * slot + (size_t)y * g.NP].x;
+}
 }  // namespace sb
