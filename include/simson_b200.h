@@ -31,7 +31,8 @@ extern "C" {
 #define SGPU_E_NAN (-5)        /* non-finite value detected in the state   */
 
 #define SGPU_FP64 0            /* every transform and solve in FP64 */
-#define SGPU_MIXED 1           /* FP32 FFTs/products/Chebyshev transforms, FP64 solves */
+#define SGPU_MIXED 1           /* FP32 x/z FFTs, products, Chebyshev transforms and u,v,w,omega
+                                  storage; FP64 tau solves, mean flow, p_v/p_omega and prhs */
 
 typedef struct sgpu_ctx sgpu_ctx;
 

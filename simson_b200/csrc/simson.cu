@@ -161,10 +161,10 @@ __global__ void k_from_ref_mixed(const double* __restrict__ re, const double* __
     const int z = r % g.nz; r /= g.nz;
     const int s = (int)r;
     const size_t o = ((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x;
-    if (s < 5)
-      stf[o] = float2{(float)re[i], (float)im[i]};
-    else
-      st[o] = double2{re[i], im[i]};
+    // every slot also lands in FP64: sgpu_prhs differentiates u, v, w up to
+    // four times in y, which FP32 rounding would not survive
+    if (s < 5) stf[o] = float2{(float)re[i], (float)im[i]};
+    st[o] = double2{re[i], im[i]};
   }
 }
 
@@ -419,8 +419,9 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   c->it = 1;
   c->t = 0.0;
   c->tc = 0.0;
-  // Chebyshev coefficients of u, v, w
-  cheb_to_spec(c, 0, czf(c, 0), 3, 1.0);
+  // Chebyshev coefficients of u, v, w, from the FP64 copy uploaded with the
+  // state (also under SGPU_MIXED: p_v needs four y-derivatives of v)
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0, 0, c->twy.d);
   PrhsBufs B;
   B.U1 = czf(c, 0); B.U2 = czf(c, 1); B.U3 = czf(c, 2);
   B.OMY = czf(c, 3); B.OX = czf(c, 4); B.OZ = czf(c, 5); B.PHI = czf(c, 6); B.T1 = czf(c, 7); B.T2 = czf(c, 8);
