@@ -312,8 +312,10 @@ def main():
     if "fp64" in runs and "mixed" in runs:
         r64 = runs["fp64"]
         sps64 = args.steps / (r64["ms"] / 1000.0) * args.gpus
-        errs = [float(np.linalg.norm(runs["mixed"]["uvw"][k] - r64["uvw"][k]) / np.linalg.norm(r64["uvw"][k]))
-                for k in range(3)]
+        keep = np.ones(w["nz"], bool)
+        keep[w["nz"] // 2] = False  # the oddball kz plane carries the last H in both paths; never read
+        errs = [float(np.linalg.norm(runs["mixed"]["uvw"][k][keep] - r64["uvw"][k][keep]) /
+                      np.linalg.norm(r64["uvw"][k][keep])) for k in range(3)]
         line["fp64"] = {"value": sps64, "ms_per_step": r64["ms"] / args.steps,
                         "kernel_ms_per_substep": {k: (v[0] / max(v[1], 1)) for k, v in r64["prof"].items() if v[1]},
                         "e2e": r64["e2e_steps"] / r64["e2e_s"] * args.gpus}
