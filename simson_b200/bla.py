@@ -48,7 +48,7 @@ def load_library(build: bool = True):
     global _LIB
     if _LIB is not None:
         return _LIB
-    path = _build.build() if build else _build.LIB
+    path = os.environ.get("SIMSON_LIB") or (_build.build() if build else _build.LIB)
     if not os.path.exists(path):
         raise SimsonError(f"CUDA library missing: {path}")
     lib = ctypes.CDLL(path)

@@ -68,7 +68,9 @@ struct sgpu_ctx {
   bool cfl_pending = false;
   bool have_state = false;
   long long launches = 0;
-  static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 128;
+  // threads per CTA of the FFT kernels (measured on B200: 256 everywhere but
+  // the FP64 x-pass, whose register use prefers 128)
+  static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 256, xpass64_threads = 128;
   static constexpr int kbf = 8, rbf = 2, pbf = 8;  // FP32 tiles (same shared memory as FP64)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
@@ -297,6 +299,8 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
                        (int)s_y);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_y);
+  cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)s_y);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -386,17 +390,24 @@ static void launch_cheb_t(sgpu_ctx* c, const typename C2<SI>::type* in, size_t i
 // the state (FP64, or FP32 under SGPU_MIXED); Chebyshev-y fields are FP64.
 static void cheb_to_spec(sgpu_ctx* c, int slot0, double2* out, int nfields, double scale) {
   const size_t fld = (size_t)c->g.nyp * c->g.NP;
-  if (c->mixed)
-    launch_cheb_t<float, sgpu_ctx::pbf, float, double>(c, c->stf + slot0 * fld, fld, out, fld, nfields, 0, scale, 0,
-                                                       c->twy.f);
+  if (c->mixed)  // FP32 Chebyshev coefficients of H (the pencil kernel reads them as float2)
+    // the output fields sit where the FP64 scratch fields would (stride fld
+    // double2 = 2*fld float2), so the pencil kernel addresses them as usual
+    launch_cheb_t<float, sgpu_ctx::pbf, float, float>(c, c->stf + slot0 * fld, fld, reinterpret_cast<float2*>(out),
+                                                      2 * fld, nfields, 0, scale, 0, c->twy.f);
   else
     launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->st + slot0 * fld, fld, out, fld, nfields, 0, scale, 0,
                                                         c->twy.d);
 }
 
-static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields, int skip_oddball) {
+static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields, int skip_oddball,
+                         bool fp32_input = false) {
   const size_t fld = (size_t)c->g.nyp * c->g.NP;
-  if (c->mixed)
+  if (c->mixed && fp32_input)
+    launch_cheb_t<float, sgpu_ctx::pbf, float, float>(c, reinterpret_cast<const float2*>(in), 2 * fld,
+                                                      c->stf + slot0 * fld, fld, nfields, 1, 1.0, skip_oddball,
+                                                      c->twy.f);
+  else if (c->mixed)
     launch_cheb_t<float, sgpu_ctx::pbf, double, float>(c, in, fld, c->stf + slot0 * fld, fld, nfields, 1, 1.0,
                                                        skip_oddball, c->twy.f);
   else
@@ -479,7 +490,7 @@ static int enqueue_nonlin(sgpu_ctx* c) {
         c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta, 0);
     dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
     prof_mark(c, K_XPASS);
-    k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::fft_threads, s_x, c->stream>>>(
+    k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::xpass64_threads, s_x, c->stream>>>(
         c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
     prof_mark(c, K_ZFWD);
     k_zfwd<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
@@ -520,19 +531,28 @@ static int enqueue_linear(sgpu_ctx* c) {
   M.cflux = P.cflux;
   if (c->prof) {
     prof_mark(c, K_MEAN);
-    k_mean<<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
+    if (c->mixed)
+      k_mean<float2><<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
+    else
+      k_mean<double2><<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
   } else {
     cudaEventRecord(c->fork, c->stream);
     cudaStreamWaitEvent(c->side, c->fork, 0);
-    k_mean<<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
+    if (c->mixed)
+      k_mean<float2><<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
+    else
+      k_mean<double2><<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
     cudaEventRecord(c->join, c->side);
   }
   prof_mark(c, K_PENCIL);
-  k_pencil<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+  if (c->mixed)
+    k_pencil<float2><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+  else
+    k_pencil<double2><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
-  cheb_to_phys(c, B.OU, 0, 5, 1);
+  cheb_to_phys(c, B.OU, 0, 5, 1, /*fp32_input=*/c->mixed);
   prof_mark(c, K_OTHER);
   c->launches += 2;
   // bla/bla.f:2598-2607

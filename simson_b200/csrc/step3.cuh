@@ -258,6 +258,10 @@ struct RKc {
   double an, bn, anp1, bnp1;
 };
 
+// IO: storage of the Chebyshev H inputs and of the u, v, w, omega_x, omega_z
+// outputs (double2, or float2 under the mixed-precision path); all algebra
+// and the other columns are FP64.
+template <class IO>
 __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                 const double* __restrict__ beta, double re, RKc rk) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,10 +278,11 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
   // this pencil's column of each array; all arrays are distinct
 #define COLP(name) double2* __restrict__ name = B.name + p
-  COLP(H1); COLP(H2); COLP(H3); COLP(PV); COLP(PW); COLP(G); COLP(DG); COLP(HV); COLP(HOM); COLP(FV); COLP(FW);
-  COLP(PHI); COLP(OM); COLP(V); COLP(DV); COLP(DOM); COLP(T1); COLP(T2); COLP(OU); COLP(OV); COLP(OW); COLP(OX);
-  COLP(OZ);
+  COLP(PV); COLP(PW); COLP(HV); COLP(HOM); COLP(FV); COLP(FW); COLP(OM); COLP(V); COLP(DV);
 #undef COLP
+#define COLIO(name) IO* __restrict__ name = reinterpret_cast<IO*>(B.name) + p
+  COLIO(H1); COLIO(H2); COLIO(H3); COLIO(OU); COLIO(OV); COLIO(OW); COLIO(OX); COLIO(OZ);
+#undef COLIO
   double* __restrict__ VH = B.VH + p;
   double* __restrict__ DVH = B.DVH + p;
 
@@ -291,7 +296,10 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
     for (int j = n - 1; j >= 0; --j) {
       const size_t o = j * NP;
-      const double2 h1 = H1[o], h2 = H2[o], h3 = H3[o], pv = PV[o], pw = PW[o];
+      const IO h1i = H1[o], h2i = H2[o], h3i = H3[o];
+      const double2 h1 = {(double)h1i.x, (double)h1i.y}, h2 = {(double)h2i.x, (double)h2i.y};
+      const double2 h3 = {(double)h3i.x, (double)h3i.y};
+      const double2 pv = PV[o], pw = PW[o];
       double2 dg;
       if (j == n - 1) {
         dg = double2{0.0, 0.0};
@@ -385,11 +393,12 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
       const double2 ddph = step(dph2, ddph1, ddph2, j);
       const double2 dom = step(om1, dom1, dom2, j);
       const double2 ddom = step(dom2, ddom1, ddom2, j);
-      OU[o] = double2{(-a * dv.y + be * om.y) * k2i, (a * dv.x - be * om.x) * k2i};
-      OW[o] = double2{(-a * om.y - be * dv.y) * k2i, (a * om.x + be * dv.x) * k2i};
-      OZ[o] = double2{(-be * dom.y + a * phi.y) * k2i, (be * dom.x - a * phi.x) * k2i};
-      OX[o] = double2{(-a * dom.y - be * phi.y) * k2i, (a * dom.x + be * phi.x) * k2i};
-      OV[o] = v;
+      typedef decltype(IO::x) R;
+      OU[o] = IO{(R)((-a * dv.y + be * om.y) * k2i), (R)((a * dv.x - be * om.x) * k2i)};
+      OW[o] = IO{(R)((-a * om.y - be * dv.y) * k2i), (R)((a * om.x + be * dv.x) * k2i)};
+      OZ[o] = IO{(R)((-be * dom.y + a * phi.y) * k2i), (R)((be * dom.x - a * phi.x) * k2i)};
+      OX[o] = IO{(R)((-a * dom.y - be * phi.y) * k2i), (R)((a * dom.x + be * phi.x) * k2i)};
+      OV[o] = IO{(R)v.x, (R)v.y};
       PV[o] = double2{-ddph.x + k2m * phi.x - c2 * hv.x, -ddph.y + k2m * phi.y - c2 * hv.y};
       PW[o] = double2{-ddom.x + k2m * om.x - c2 * hom.x, -ddom.y + k2m * om.y - c2 * hom.y};
       v1 = v;
@@ -413,6 +422,7 @@ struct MeanArgs {
   int cflux;
 };
 
+template <class IO>
 __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
   extern __shared__ double msm[];  // 12 columns of n doubles
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -426,8 +436,8 @@ __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
   double px = A.scal[0];
   const double mflux = A.scal[1];
   for (int j = 0; j < n; ++j) {
-    huw1[j] = A.H1[(size_t)j * NP].x;
-    huw2[j] = A.H3[(size_t)j * NP].x;
+    huw1[j] = (double)reinterpret_cast<const IO*>(A.H1)[(size_t)j * NP].x;
+    huw2[j] = (double)reinterpret_cast<const IO*>(A.H3)[(size_t)j * NP].x;
     fu[j] = A.puw[j] - c1 * huw1[j];
     fw[j] = A.puw[n + j] - c1 * huw2[j];
   }
@@ -455,12 +465,13 @@ __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
   }
   cheb_deriv(DU, U, n);
   cheb_deriv(DW, W, n);
+  typedef decltype(IO::x) R;
   for (int j = 0; j < n; ++j) {
-    A.OU[(size_t)j * NP] = double2{U[j], 0.0};
-    A.OW[(size_t)j * NP] = double2{W[j], 0.0};
-    A.OV[(size_t)j * NP] = double2{0.0, 0.0};
-    A.OX[(size_t)j * NP] = double2{DW[j], 0.0};
-    A.OZ[(size_t)j * NP] = double2{-DU[j], 0.0};
+    reinterpret_cast<IO*>(A.OU)[(size_t)j * NP] = IO{(R)U[j], (R)0};
+    reinterpret_cast<IO*>(A.OW)[(size_t)j * NP] = IO{(R)W[j], (R)0};
+    reinterpret_cast<IO*>(A.OV)[(size_t)j * NP] = IO{(R)0, (R)0};
+    reinterpret_cast<IO*>(A.OX)[(size_t)j * NP] = IO{(R)DW[j], (R)0};
+    reinterpret_cast<IO*>(A.OZ)[(size_t)j * NP] = IO{(R)(-DU[j]), (R)0};
     A.PV[(size_t)j * NP] = double2{0.0, 0.0};
     A.PW[(size_t)j * NP] = double2{0.0, 0.0};
   }
