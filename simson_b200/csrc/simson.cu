@@ -239,7 +239,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
     return fail(rc);
   const size_t fld = (size_t)g.nyp * g.NP;
   c->ncz = 23;
-  c->nrz = 5;
+  c->nrz = 7;
   if (cudaMalloc(&c->st, 7 * fld * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&c->puw, 2 * g.ny * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->scal, 4 * sizeof(double)) != cudaSuccess ||
@@ -524,6 +524,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   B.T1 = czf(c, 14); B.T2 = czf(c, 15);
   B.OU = czf(c, 16); B.OV = czf(c, 17); B.OW = czf(c, 18); B.OX = czf(c, 19); B.OZ = czf(c, 20);
   B.PHIH = rzf(c, 0); B.VH = rzf(c, 1); B.DVH = rzf(c, 2); B.CP = rzf(c, 3); B.WT = rzf(c, 4);
+  B.CPL = rzf(c, 5); B.WTL = rzf(c, 6);
   // kx = kz = 0 (mean flow, cflux) on the side stream, concurrent with the pencils
   MeanArgs M;
   M.H1 = B.H1; M.H3 = B.H3; M.puw = c->puw; M.scal = c->scal; M.scr = c->mscr;
@@ -546,9 +547,9 @@ static int enqueue_linear(sgpu_ctx* c) {
   }
   prof_mark(c, K_PENCIL);
   if (c->mixed)
-    k_pencil<float2><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<float2, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
   else
-    k_pencil<double2><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<double2, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);

@@ -24,11 +24,13 @@ namespace sb {
 #define SB_HD __host__ __device__
 #endif
 
-struct Col {
-  double* a;
+template <class S>
+struct ColT {
+  S* a;
   size_t s;
-  SB_HD __forceinline__ double& operator[](int j) const { return a[(size_t)j * s]; }
+  SB_HD __forceinline__ S& operator[](int j) const { return a[(size_t)j * s]; }
 };
+typedef ColT<double> Col;
 
 __device__ __forceinline__ Col col_re(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p, 2 * (size_t)NP}; }
 __device__ __forceinline__ Col col_im(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p + 1, 2 * (size_t)NP}; }
@@ -57,14 +59,17 @@ SB_HD inline void cheb_deriv(Col b, Col a, int n) {
 
 // Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
 // (1-based row index i as in bla/setmacrhs.f).
-SB_HD __forceinline__ double tau_c(int i, double lam) {
-  return (i == 1) ? -0.25 * lam : (-0.25 / ((double)i * ((double)i + 1.0))) * lam;
+template <class S>
+SB_HD __forceinline__ S tau_c(int i, S lam) {
+  return (i == 1) ? (S)-0.25 * lam : ((S)-0.25 / ((S)i * ((S)i + (S)1.0))) * lam;
 }
-SB_HD __forceinline__ double tau_d(int i, double lam) {
-  return 1.0 + (0.5 / ((double)i * ((double)i + 2.0))) * lam;
+template <class S>
+SB_HD __forceinline__ S tau_d(int i, S lam) {
+  return (S)1.0 + ((S)0.5 / ((S)i * ((S)i + (S)2.0))) * lam;
 }
-SB_HD __forceinline__ double tau_e(int i, double lam) {
-  return (-0.25 / (((double)i + 1.0) * ((double)i + 2.0))) * lam;
+template <class S>
+SB_HD __forceinline__ S tau_e(int i, S lam) {
+  return ((S)-0.25 / (((S)i + (S)1.0) * ((S)i + (S)2.0))) * lam;
 }
 
 // Tau right-hand side of row i (3 <= i <= n, 1-based) from f: the
@@ -93,13 +98,13 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 //   3. forward (rows 3..n): x(i) -= c'(i-2) x(i-2).
 // cp, wt: per-pencil scratch columns (n entries each).  f[q].a == nullptr
 // means a zero right-hand side.
-template <int M>
-SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double* bc1, const double* bc2,
-                     Col cp, Col wt) {
+template <int M, class S = double, class FS = S>
+SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S* bc1, const S* bc2, ColT<S> cp,
+                     ColT<S> wt) {
   // every column is a distinct array: restrict-qualified raw pointers let the
   // loads of a sweep run ahead of its stores
-  const double* __restrict__ fp[M];
-  double* __restrict__ xp[M];
+  const FS* __restrict__ fp[M];
+  S* __restrict__ xp[M];
   size_t fs[M], xs[M];
 #pragma unroll
   for (int q = 0; q < M; ++q) {
@@ -108,41 +113,41 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
     xp[q] = x[q].a;
     xs[q] = x[q].s;
   }
-  double* __restrict__ cpp = cp.a;
-  double* __restrict__ wtp = wt.a;
+  S* __restrict__ cpp = cp.a;
+  S* __restrict__ wtp = wt.a;
   const size_t cs = cp.s, ws = wt.s;
-  double xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
-  double q1 = 0.0, q2 = 0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
-  double w1 = 0.0, w2 = 0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
+  S xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
+  S q1 = (S)0.0, q2 = (S)0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
+  S w1 = (S)0.0, w2 = (S)0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
 #pragma unroll
-  for (int q = 0; q < M; ++q) xa[q] = xb[q] = 0.0;
+  for (int q = 0; q < M; ++q) xa[q] = xb[q] = (S)0.0;
   for (int i = n; i >= 3; --i) {
-    double dinv = 1.0, cnew = 0.0, wnew = 0.0;
+    S dinv = (S)1.0, cnew = (S)0.0, wnew = (S)0.0;
     if (i <= n - 2) {
       const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
-      dinv = (i >= n - 3) ? 1.0 / tau_d(m, lam) : 1.0 / (tau_d(m, lam) - q2 * tau_e(m, lam));
+      dinv = (i >= n - 3) ? (S)1.0 / tau_d(m, lam) : (S)1.0 / (tau_d(m, lam) - q2 * tau_e(m, lam));
       cnew = tau_c(m, lam) * dinv;
       cpp[(size_t)(m - 1) * cs] = cnew;
-      wnew = (i >= n - 3) ? 1.0 - tau_c(i, lam) : 1.0 - q2 * w2;
+      wnew = (i >= n - 3) ? (S)1.0 - tau_c(i, lam) : (S)1.0 - q2 * w2;
       wtp[(size_t)(i - 1) * ws] = wnew;
     }
-    const double di = (double)i;
-    const double ca = (i == 3) ? 0.0 : 0.25 / ((di - 2.0) * (di - 1.0));
-    const double cb = -0.5 / ((di - 2.0) * di);
-    const double cc = 0.25 / ((di - 1.0) * di);
-    const double e2 = (i <= n - 4) ? tau_e(i - 2, lam) : 0.0;
+    const S di = (S)i;
+    const S ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
+    const S cb = (S)-0.5 / ((di - (S)2.0) * di);
+    const S cc = (S)0.25 / ((di - (S)1.0) * di);
+    const S e2 = (i <= n - 4) ? tau_e(i - 2, lam) : (S)0.0;
 #pragma unroll
     for (int q = 0; q < M; ++q) {
-      double r = 0.0;
+      S r = (S)0.0;
       if (fp[q] != nullptr) {
-        const double* __restrict__ F = fp[q];
+        const FS* __restrict__ F = fp[q];
         const size_t st = fs[q];
         if (i == 3) {
-          r = 0.25 * F[0] + F[4 * st] / 24.0 - F[2 * st] / 6.0;
+          r = (S)0.25 * (S)F[0] + (S)F[4 * st] / (S)24.0 - (S)F[2 * st] / (S)6.0;
         } else {
-          r = ca * F[(size_t)(i - 3) * st];
-          if (i <= n - 2) r += cb * F[(size_t)(i - 1) * st];
-          if (i <= n - 4) r += cc * F[(size_t)(i + 1) * st];
+          r = ca * (S)F[(size_t)(i - 3) * st];
+          if (i <= n - 2) r += cb * (S)F[(size_t)(i - 1) * st];
+          if (i <= n - 4) r += cc * (S)F[(size_t)(i + 1) * st];
         }
       }
       if (i <= n - 4)
@@ -161,14 +166,14 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
   // c'(n-3), c'(n-2) are the unscaled c (d = 1 in the truncated rows)
   cpp[(size_t)(n - 4) * cs] = tau_c(n - 3, lam);
   cpp[(size_t)(n - 3) * cs] = tau_c(n - 2, lam);
-  const double d1 = 1.0 / (1.0 - cpp[0] * wtp[2 * ws]);
-  const double d2 = 1.0 / (1.0 - cpp[cs] * wtp[3 * ws]);
+  const S d1 = (S)1.0 / ((S)1.0 - cpp[0] * wtp[2 * ws]);
+  const S d2 = (S)1.0 / ((S)1.0 - cpp[cs] * wtp[3 * ws]);
 #pragma unroll
   for (int q = 0; q < M; ++q) {
-    double* __restrict__ X = xp[q];
+    S* __restrict__ X = xp[q];
     const size_t st = xs[q];
-    double x1 = bc1[q] - X[(size_t)(n - 1) * st];
-    double x2 = bc2[q] - X[(size_t)(n - 2) * st];
+    S x1 = bc1[q] - X[(size_t)(n - 1) * st];
+    S x2 = bc2[q] - X[(size_t)(n - 2) * st];
     for (int i = 5; i <= n - 2; i += 2) {
       x1 = x1 - X[(size_t)(i - 1) * st] * wtp[(size_t)(i - 1) * ws];
       x2 = x2 - X[(size_t)(i - 2) * st] * wtp[(size_t)(i - 2) * ws];
@@ -180,11 +185,11 @@ SB_HD void tau_solve(double lam, int n, const Col* f, const Col* x, const double
   }
 #pragma unroll 4
   for (int i = 3; i <= n; ++i) {
-    const double c = cpp[(size_t)(i - 3) * cs];
+    const S c = cpp[(size_t)(i - 3) * cs];
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       const size_t o = (size_t)(i - 1) * xs[q];
-      const double v = xp[q][o] - c * xa[q];
+      const S v = xp[q][o] - c * xa[q];
       xp[q][o] = v;
       xa[q] = xb[q];
       xb[q] = v;
@@ -252,6 +257,7 @@ struct PencilBufs {
   double2 *G, *DG, *HV, *HOM, *FV, *FW, *PHI, *OM, *V, *DV, *DOM, *T1, *T2;
   double2 *OU, *OV, *OW, *OX, *OZ;  // outputs (Chebyshev)
   double *PHIH, *VH, *DVH, *CP, *WT;
+  double *CPL, *WTL;  // coefficients of the lambda solve (its own arrays: their type may differ)
 };
 
 struct RKc {
@@ -261,9 +267,13 @@ struct RKc {
 // IO: storage of the Chebyshev H inputs and of the u, v, w, omega_x, omega_z
 // outputs (double2, or float2 under the mixed-precision path); all algebra
 // and the other columns are FP64.
-template <class IO>
+// SC: scalar of the omega_y / particular-phi Helmholtz solve and of its
+// forcing columns (double, or float under the mixed-precision path); the
+// fourth-order v solve, the superposition and every derivative stay FP64.
+template <class IO, class SC>
 __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                 const double* __restrict__ beta, double re, RKc rk) {
+  typedef typename C2<SC>::type SC2;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
   const int kx = p % g.nx2;
@@ -278,8 +288,11 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
   // this pencil's column of each array; all arrays are distinct
 #define COLP(name) double2* __restrict__ name = B.name + p
-  COLP(PV); COLP(PW); COLP(HV); COLP(HOM); COLP(FV); COLP(FW); COLP(OM); COLP(V); COLP(DV);
+  COLP(PV); COLP(PW); COLP(V); COLP(DV);
 #undef COLP
+#define COLS(name) SC2* __restrict__ name = reinterpret_cast<SC2*>(B.name) + p
+  COLS(HV); COLS(HOM); COLS(FV); COLS(FW); COLS(OM);
+#undef COLS
 #define COLIO(name) IO* __restrict__ name = reinterpret_cast<IO*>(B.name) + p
   COLIO(H1); COLIO(H2); COLIO(H3); COLIO(OU); COLIO(OV); COLIO(OW); COLIO(OX); COLIO(OZ);
 #undef COLIO
@@ -312,26 +325,27 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
       if (j == 0) dg = double2{0.5 * dg.x, 0.5 * dg.y};
       g1 = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
       const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
-      HOM[o] = hom;
-      FW[o] = double2{pw.x - c1 * hom.x, pw.y - c1 * hom.y};
+      HOM[o] = SC2{(SC)hom.x, (SC)hom.y};
+      FW[o] = SC2{(SC)(pw.x - c1 * hom.x), (SC)(pw.y - c1 * hom.y)};
       const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
-      HV[o] = hv;
-      FV[o] = double2{pv.x - c1 * hv.x, pv.y - c1 * hv.y};
+      HV[o] = SC2{(SC)hv.x, (SC)hv.y};
+      FV[o] = SC2{(SC)(pv.x - c1 * hv.x), (SC)(pv.y - c1 * hv.y)};
     }
   }
   // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
   {
-    const Col f[5] = {col_re(B.FV, p, NP), col_im(B.FV, p, NP), col_re(B.FW, p, NP), col_im(B.FW, p, NP), Col{nullptr, 0}};
-    const Col x[5] = {col_re(B.PHI, p, NP), col_im(B.PHI, p, NP), col_re(B.OM, p, NP), col_im(B.OM, p, NP), col_r(B.PHIH, p, NP)};
-    const double bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
-    tau_solve<5>(lam, n, f, x, bc1, bc2, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
-  }
-  // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001)
-  {
-    const Col f[3] = {col_re(B.PHI, p, NP), col_im(B.PHI, p, NP), col_r(B.PHIH, p, NP)};
-    const Col x[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
-    const double bc1[3] = {0, 0, 0}, bc2[3] = {0, 0, 0};
-    tau_solve<3>(k2, n, f, x, bc1, bc2, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
+    auto cre = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p, 2 * NP}; };
+    auto cim = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
+    auto crl = [&](double* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + p, NP}; };
+    const ColT<SC> f[5] = {cre(B.FV), cim(B.FV), cre(B.FW), cim(B.FW), ColT<SC>{nullptr, 0}};
+    const ColT<SC> x[5] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM), crl(B.PHIH)};
+    const SC bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
+    tau_solve<5, SC>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
+    // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
+    const ColT<SC> fv[3] = {cre(B.PHI), cim(B.PHI), crl(B.PHIH)};
+    const Col xv[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
+    const double b0[3] = {0, 0, 0};
+    tau_solve<3, double, SC>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
   }
   // dv/dy = 0 at the walls: add the homogeneous solution per parity
   // (linearbl.f:1020-1085).  The parity sums of dv run in ascending order as
@@ -384,7 +398,9 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
       const double vh = VH[o];
       const double2 vp = V[o];
       const double2 v = double2{vp.x + cvr[j & 1] * vh, vp.y + cvi[j & 1] * vh};
-      const double2 om = OM[o], hv = HV[o], hom = HOM[o];
+      const SC2 omi = OM[o], hvi = HV[o], homi = HOM[o];
+      const double2 om = {(double)omi.x, (double)omi.y}, hv = {(double)hvi.x, (double)hvi.y};
+      const double2 hom = {(double)homi.x, (double)homi.y};
       const double2 dv = step(v1, dv1, dv2, j);
       // second derivative from the first derivative at j+1 (before halving)
       const double2 ddv = step(dv2, ddv1, ddv2, j);
