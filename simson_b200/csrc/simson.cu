@@ -547,9 +547,9 @@ static int enqueue_linear(sgpu_ctx* c) {
   }
   prof_mark(c, K_PENCIL);
   if (c->mixed)
-    k_pencil<float2, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<float2, double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
   else
-    k_pencil<double2, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);

@@ -267,13 +267,16 @@ struct RKc {
 // IO: storage of the Chebyshev H inputs and of the u, v, w, omega_x, omega_z
 // outputs (double2, or float2 under the mixed-precision path); all algebra
 // and the other columns are FP64.
-// SC: scalar of the omega_y / particular-phi Helmholtz solve and of its
-// forcing columns (double, or float under the mixed-precision path); the
-// fourth-order v solve, the superposition and every derivative stay FP64.
-template <class IO, class SC>
+// SC: scalar of the omega_y / particular-phi Helmholtz solve; FC: storage of
+// its forcing columns h_v, h_omega, f_v, f_omega (read by the solve and the
+// next partial RHS, never differentiated).  FP64 path: double/double; the
+// mixed-precision path stores the forcing in float.  The fourth-order v solve,
+// the superposition and every derivative are FP64 in both.
+template <class IO, class SC, class FC>
 __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                 const double* __restrict__ beta, double re, RKc rk) {
   typedef typename C2<SC>::type SC2;
+  typedef typename C2<FC>::type FC2;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
   const int kx = p % g.nx2;
@@ -290,9 +293,10 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
 #define COLP(name) double2* __restrict__ name = B.name + p
   COLP(PV); COLP(PW); COLP(V); COLP(DV);
 #undef COLP
-#define COLS(name) SC2* __restrict__ name = reinterpret_cast<SC2*>(B.name) + p
-  COLS(HV); COLS(HOM); COLS(FV); COLS(FW); COLS(OM);
-#undef COLS
+#define COLF(name) FC2* __restrict__ name = reinterpret_cast<FC2*>(B.name) + p
+  COLF(HV); COLF(HOM); COLF(FV); COLF(FW);
+#undef COLF
+  SC2* __restrict__ OM = reinterpret_cast<SC2*>(B.OM) + p;
 #define COLIO(name) IO* __restrict__ name = reinterpret_cast<IO*>(B.name) + p
   COLIO(H1); COLIO(H2); COLIO(H3); COLIO(OU); COLIO(OV); COLIO(OW); COLIO(OX); COLIO(OZ);
 #undef COLIO
@@ -325,11 +329,11 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
       if (j == 0) dg = double2{0.5 * dg.x, 0.5 * dg.y};
       g1 = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
       const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
-      HOM[o] = SC2{(SC)hom.x, (SC)hom.y};
-      FW[o] = SC2{(SC)(pw.x - c1 * hom.x), (SC)(pw.y - c1 * hom.y)};
+      HOM[o] = FC2{(FC)hom.x, (FC)hom.y};
+      FW[o] = FC2{(FC)(pw.x - c1 * hom.x), (FC)(pw.y - c1 * hom.y)};
       const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
-      HV[o] = SC2{(SC)hv.x, (SC)hv.y};
-      FV[o] = SC2{(SC)(pv.x - c1 * hv.x), (SC)(pv.y - c1 * hv.y)};
+      HV[o] = FC2{(FC)hv.x, (FC)hv.y};
+      FV[o] = FC2{(FC)(pv.x - c1 * hv.x), (FC)(pv.y - c1 * hv.y)};
     }
   }
   // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
@@ -337,10 +341,12 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     auto cre = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p, 2 * NP}; };
     auto cim = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
     auto crl = [&](double* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + p, NP}; };
-    const ColT<SC> f[5] = {cre(B.FV), cim(B.FV), cre(B.FW), cim(B.FW), ColT<SC>{nullptr, 0}};
+    auto fre = [&](double2* arr) { return ColT<FC>{reinterpret_cast<FC*>(arr) + 2 * (size_t)p, 2 * NP}; };
+    auto fim = [&](double2* arr) { return ColT<FC>{reinterpret_cast<FC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
+    const ColT<FC> f[5] = {fre(B.FV), fim(B.FV), fre(B.FW), fim(B.FW), ColT<FC>{nullptr, 0}};
     const ColT<SC> x[5] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM), crl(B.PHIH)};
     const SC bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
-    tau_solve<5, SC>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
+    tau_solve<5, SC, FC>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
     // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
     const ColT<SC> fv[3] = {cre(B.PHI), cim(B.PHI), crl(B.PHIH)};
     const Col xv[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
@@ -398,7 +404,8 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
       const double vh = VH[o];
       const double2 vp = V[o];
       const double2 v = double2{vp.x + cvr[j & 1] * vh, vp.y + cvi[j & 1] * vh};
-      const SC2 omi = OM[o], hvi = HV[o], homi = HOM[o];
+      const SC2 omi = OM[o];
+      const FC2 hvi = HV[o], homi = HOM[o];
       const double2 om = {(double)omi.x, (double)omi.y}, hv = {(double)hvi.x, (double)hvi.y};
       const double2 hom = {(double)homi.x, (double)homi.y};
       const double2 dv = step(v1, dv1, dv2, j);
