@@ -85,6 +85,17 @@ int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
  * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises. */
 int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
+/* Statistics of the current state, as bla/boxamp.f and bla/wampbl.f:124-278
+ * compute them at the start of a full step when iamp > 0: amp[20*ny] in the
+ * layout of amp(nyp,20) (plane averages of squared velocity and vorticity
+ * fluctuations, <|omega_y|^2/k^2>, Reynolds stresses, mean U, W, Omega_x,
+ * Omega_z per y; column 13 unused), and, if row is not NULL, the 19 values of
+ * one amp.stat line (bla/wampbl.f:276-278): t, u/v/w rms, omega_x/y/z rms,
+ * <|omega_y|^2/k^2>, <u'v'>, e0, h+ (Re_tau), px, Re_bulk, wall shears tau1
+ * (y=+1) and tau2 (y=-1), 99 %, displacement and momentum thickness, W bulk.
+ * Synchronises the library's stream. */
+int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
+
 /* Stream-ordered timing on the library's stream: record event slot (0..15),
  * elapsed milliseconds between two recorded slots (synchronises on b). */
 int sgpu_event_record(sgpu_ctx* ctx, int slot);

@@ -44,7 +44,7 @@ OUT_ROOT = os.path.join(HERE, "_ref")
 UNIT_FILES = [
     "nonlinbl.f", "advection.f", "boxcfl.f", "fft2db.f", "fft2df.f", "getxz.f", "putxz.f",
     "linearbl.f", "getxy.f", "putxy.f", "setmacrhs.f", "trid.f", "dcheb.f", "evald.f",
-    "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f",
+    "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
 ]
 
 MAIN_RANGES = [

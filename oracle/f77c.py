@@ -731,6 +731,8 @@ class Ctx:
 
     def expr(self, e, st) -> str:
         k = e[0]
+        if k == "cexpr":  # a C expression made by the translator itself
+            return e[1]
         if k == "num":
             s = e[1].replace("d", "e")
             return s
@@ -1220,7 +1222,20 @@ class Translator:
             if v is None or v.dims is None:
                 raise F77Error(f"{where}: assignment to non-array {lhs[1]}(...)")
             if any(a[0] == "slice" for a in lhs[2]):
-                raise F77Error(f"{where}: array-section assignment unsupported")
+                # scalar assigned to a section with explicit bounds: a loop nest
+                if any(a[0] == "slice" and (a[1] is None or a[2] is None) for a in lhs[2]) or \
+                        ctx.etype(rhs) not in ("i", "r", "l", "c"):
+                    raise F77Error(f"{where}: array-section assignment unsupported")
+                idx, loops = [], []
+                for a in lhs[2]:
+                    if a[0] == "slice":
+                        ctx.tmp += 1
+                        iv = f"_s{ctx.tmp}"
+                        loops.append(f"for (long {iv} = {ctx.expr(a[1], st)}; {iv} <= {ctx.expr(a[2], st)}; {iv}++)")
+                        idx.append(("cexpr", iv))
+                    else:
+                        idx.append(a)
+                return " ".join(loops) + f" {ctx.index(lhs[1], idx, st)} = {ctx.expr(rhs, st)};"
             return f"{ctx.index(lhs[1], lhs[2], st)} = {ctx.expr(rhs, st)};"
         raise F77Error(f"{where}: bad assignment target")
 

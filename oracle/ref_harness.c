@@ -134,3 +134,8 @@ void sref_grid(double *eta, double *wint) {
   memcpy(eta, v_eta, (size_t)v_nyp * sizeof(double));
   memcpy(wint, v_wint, (size_t)v_nyp * sizeof(double));
 }
+
+/* Plane statistics: nonlinbl calls boxamp at the first substep of a step
+ * when iamp > 0 (bla/nonlinbl.f:425-432); amp(nyp,20) is copied out. */
+void sref_set_iamp(int iamp) { v_iamp = iamp > 0 ? iamp : -1000000; }
+void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(double)); }

@@ -35,6 +35,8 @@ def _lib(nx, ny, nz, build=True, fma=False):
     lib.sref_get_puw.argtypes = [dp]
     lib.sref_grid.argtypes = [dp, dp]
     lib.sref_dims.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    lib.sref_set_iamp.argtypes = [ctypes.c_int]
+    lib.sref_get_amp.argtypes = [dp]
     return lib
 
 
@@ -103,6 +105,16 @@ class RefSim:
         wint = np.empty(self.nyp)
         self.lib.sref_grid(_dp(eta), _dp(wint))
         return eta, wint
+
+    def set_iamp(self, iamp):
+        """Plane statistics (boxamp) every iamp substeps from the next step on."""
+        self.lib.sref_set_iamp(int(iamp))
+
+    def amp(self):
+        """amp(nyp,20) as an array (20, nyp): amp[k-1, y-1] = amp(y, k)."""
+        a = np.empty((20, self.nyp))
+        self.lib.sref_get_amp(_dp(a))
+        return a
 
     def state(self):
         return [self.get_slot(k) for k in range(1, 8)]

@@ -71,6 +71,7 @@ def load_library(build: bool = True):
     lib.sgpu_error_string.restype = ctypes.c_char_p
     lib.sgpu_host_alloc.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
     lib.sgpu_host_free.argtypes = [vp]
+    lib.sgpu_amplitudes.argtypes = [vp, dp, dp]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -94,6 +95,8 @@ class Channel:
         self.shape = (nz, ny, nx // 2)
         if px is None:
             px = -2.0 / re  # bla/bla.f:1630 first guess under cflux
+        if isinstance(precision, str):
+            precision = {"fp64": FP64, "mixed": MIXED}[precision.lower()]
         prm = SgpuParams(nx, ny, nz, re, xl, zl, dt, 3, int(cflux), mflux, px, rot, icfl, precision, device)
         self._ctx = ctypes.c_void_p()
         self._check(self.lib.sgpu_init(ctypes.byref(prm), ctypes.byref(self._ctx)), "sgpu_init")
@@ -190,6 +193,18 @@ class Channel:
         dp = ctypes.POINTER(ctypes.c_double)
         self._check(self.lib.sgpu_download_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
                     "download")
+
+    AMP_ROW = ("t", "urms", "vrms", "wrms", "omxrms", "omyrms", "omzrms", "omy2_k2", "uv", "e0", "hplus", "px",
+               "re_bulk", "tau1", "tau2", "delta99", "delta_star", "theta", "w_bulk")
+
+    def amplitudes(self):
+        """Plane statistics and the amp.stat row of the current state
+        (bla/boxamp.f, bla/wampbl.f): (amp array (20, ny) with amp[k-1, y-1] =
+        amp(y, k), row as a dict keyed by AMP_ROW)."""
+        amp = np.zeros((20, self.ny))
+        row = np.zeros(19)
+        self._check(self.lib.sgpu_amplitudes(self._ctx, _dp(amp), _dp(row)), "amplitudes")
+        return amp, dict(zip(self.AMP_ROW, row))
 
     KERNELS = ("zinv", "xpass", "zfwd", "cheb_fwd", "pencil", "mean", "cheb_inv", "other")
 

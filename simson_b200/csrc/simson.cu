@@ -15,6 +15,7 @@
 #include "layout.cuh"
 #include "step2.cuh"
 #include "step3.cuh"
+#include "stats.cuh"
 
 using namespace sb;
 
@@ -59,6 +60,7 @@ struct sgpu_ctx {
   int nrz = 0;
   double* mscr = nullptr;    // mean-flow scratch
   double* meanp = nullptr;   // [4][nyp] U, W, Omega_x, Omega_z for the mixed step 2
+  double* ampd = nullptr;    // [20][nyp] plane statistics
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   // RK bookkeeping (host mirror of the reference driver scalars)
@@ -252,7 +254,8 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->cz, (size_t)c->ncz * fld * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&c->rz, (size_t)c->nrz * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess)
+      cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->ampd, 20 * (size_t)g.nyp * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
   if (c->mixed && (cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess ||
                    cudaMalloc(&c->meanp, 4 * (size_t)g.nyp * sizeof(double)) != cudaSuccess))
@@ -310,7 +313,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->st, c->stf, c->meanp, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+  void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -504,7 +507,6 @@ static int enqueue_nonlin(sgpu_ctx* c) {
 static int enqueue_linear(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
-  const size_t fld = (size_t)g.nyp * g.NP;
   // RK weights (bla/bla.f:2384-2397)
   c->an = c->anp1;
   c->bn = c->bnp1;
@@ -672,5 +674,69 @@ extern "C" int sgpu_profile_read(sgpu_ctx* c, double* ms, int* count, int n) {
     if (id < n) { ms[id] += t; count[id] += 1; }
   }
   c->pnext = 0;
+  return SGPU_OK;
+}
+
+// Plane statistics and the amp.stat row (bla/boxamp.f; bla/wampbl.f:124-278
+// for the channel, dstar = 1, one process).  The per-plane sums run on the
+// device; the y-integrals of the row run here with the Clenshaw-Curtis weights
+// of bla/preprbl.f:78-87 and gridy = 1 + eta (:56-58).
+extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
+  if (!c || !amp) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  const Dims& g = c->g;
+  if (c->mixed)
+    k_amp<float><<<g.nyp, 256, 0, c->stream>>>(c->stf, g, c->alfa, c->beta, c->ampd);
+  else
+    k_amp<double><<<g.nyp, 256, 0, c->stream>>>(c->st, g, c->alfa, c->beta, c->ampd);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(amp, c->ampd, 20 * (size_t)g.nyp * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  double sc[4];
+  CK(cudaMemcpyAsync(sc, c->scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (!row) return SGPU_OK;
+  const int n = g.nyp;
+  const double pi = 3.1415926535897932385;
+  std::vector<double> wint(n), gridy(n), a(20 * (size_t)n);
+  for (int y = 0; y < n; ++y) {
+    double wv = -.5;
+    for (int i = 1; i <= (n + 1) / 2 - 2; ++i)
+      wv = wv + cos(pi * (double)(2 * i * y) / (double)(n - 1)) / (double)((2 * i) * (2 * i) - 1);
+    wv = wv + .5 * cos(pi * (double)y) / (double)((n - 1) * (n - 1) - 1);
+    wv = -4. / (double)(n - 1) * wv;
+    if (y == 0 || y == n - 1) wv = wv * .5;
+    wint[y] = wv;
+    gridy[y] = 1. + cos(pi * (double)y / (double)(n - 1));
+  }
+  memcpy(a.data(), amp, a.size() * sizeof(double));
+  auto A = [&](int y, int k) -> double& { return a[(size_t)(k - 1) * n + y]; };  // amp(y+1, k)
+  double sum[21] = {0};
+  for (int y = 0; y < n; ++y) {
+    A(y, 8) = -A(y, 8);
+    A(y, 13) = A(y, 9);
+  }
+  for (int i = 1; i <= 10; ++i)
+    for (int y = 0; y < n; ++y) sum[i] += A(y, i) * wint[y];
+  for (int y = 0; y < n; ++y) sum[13] += A(y, 13) * wint[y];
+  double delta[4] = {0, 0, 0, 0};
+  for (int y = 0; y < n; ++y) {
+    if (delta[1] == 0. && A(y, 13) <= 0.99) {
+      if (A(y, 13) == 0.99 || y == 0)
+        delta[1] = gridy[y];
+      else
+        delta[1] = gridy[y] + (0.99 - A(y, 13)) * (gridy[y - 1] - gridy[y]) / (A(y - 1, 13) - A(y, 13));
+    }
+    delta[2] += (1. - A(y, 13)) * wint[y];
+    delta[3] += A(y, 13) * (1. - A(y, 13)) * wint[y];
+  }
+  for (int j = 1; j <= 7; ++j) sum[j] = sqrt(sum[j] * .5);
+  const double wb = sum[10] * .5;
+  const double e0 = sqrt((sum[9] + sum[10]) * .5);
+  const double tau1 = A(0, 12), tau2 = A(n - 1, 12);
+  const double hplus = sqrt((fabs(tau1) + fabs(tau2)) * c->prm.re / 2.);
+  const double r[19] = {c->t, sum[1], sum[2], sum[3], sum[4], sum[5], sum[6], sum[7], sum[8], e0, hplus, sc[0],
+                        sum[13] * c->prm.re / 2., tau1, tau2, delta[1], delta[2], delta[3], wb};
+  memcpy(row, r, sizeof(r));
   return SGPU_OK;
 }

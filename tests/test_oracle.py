@@ -84,3 +84,24 @@ def test_seeded_field_is_divergence_free_and_scaled():
     # Hermitian kx = 0 column
     for kz in range(1, 7):
         assert np.allclose(v[kz, :, 0], np.conj(v[nz - kz, :, 0]))
+
+
+def test_amp_row_laminar_channel():
+    """amp.stat row of the laminar Poiseuille profile U = 1 - y^2, no
+    fluctuations: bulk Reynolds number (4/3) Re/2, wall shears Omega_z = 2y,
+    h+ = sqrt(2 Re), 99 % thickness at the wall point, W bulk 0."""
+    from amp_row import amp_row
+    from simson_b200.fields import gl_points
+    nyp, re = 33, 4200.0
+    eta = gl_points(nyp)
+    amp = np.zeros((20, nyp))
+    amp[8] = 1 - eta ** 2
+    amp[11] = 2 * eta
+    row = amp_row(amp, 1.5, re, -2.0 / re)
+    assert row[0] == 1.5 and np.all(row[1:9] == 0.0)
+    assert abs(row[12] - 4.0 / 3.0 * re / 2) < 1e-10 * re
+    assert row[13] == 2.0 and row[14] == -2.0
+    assert abs(row[10] - np.sqrt(2 * re)) < 1e-12 * re
+    assert row[15] == 2.0 and row[18] == 0.0
+    # displacement thickness of 1 - y^2 over [-1, 1]: 2 - 4/3
+    assert abs(row[16] - 2.0 / 3.0) < 1e-13
