@@ -85,6 +85,31 @@ int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
  * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises. */
 int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
+/* Large-eddy model, the reference's sgs.i (bla/rparamles.f:31-60):
+ *   iles        0 none, 1 ADM-RT (approximate deconvolution, relaxation term)
+ *   cutoff_inv  1 / cut-off wavenumber fraction of the primary filter (1.5)
+ *   iord        order N of the deconvolution, 0..5 (5)
+ *   chi         relaxation coefficient (0.2)
+ *   ihighorder  0 two-dimensional, 1 iterative, 2 tensorial filtering (2) */
+typedef struct {
+  int iles;
+  double cutoff_inv;
+  int iord;
+  double chi;
+  int ihighorder;
+} sgpu_les_params;
+
+/* Enables the LES model: builds the filters of bla/init_filter.f and
+ * bla/bla.f:1489-1518 and allocates the filtered-velocity fields.  Call after
+ * sgpu_init and before sgpu_prhs (which filters the start-up velocities, as
+ * bla/prhs.f:95-193 does); step 2 then adds -chi gu (bla/nonlinbl.f:920-965)
+ * and step 3 refilters the new velocities (bla/linearbl.f:1871-1960).
+ * iles = 2, 3 (eddy-viscosity models) are rejected with SGPU_E_PARAM. */
+int sgpu_set_les(sgpu_ctx* ctx, const sgpu_les_params* p);
+
+/* The filtered velocities gur, gui(memnx, memny, memnz, 1..3). */
+int sgpu_download_les(sgpu_ctx* ctx, double* gr, double* gi);
+
 /* Statistics of the current state, as bla/boxamp.f and bla/wampbl.f:124-278
  * compute them at the start of a full step when iamp > 0: amp[20*ny] in the
  * layout of amp(nyp,20) (plane averages of squared velocity and vorticity

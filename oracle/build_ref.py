@@ -21,7 +21,9 @@ Translated units (reference file: what it contributes):
   bla/linearbl.f getxy.f putxy.f setmacrhs.f trid.f dcheb.f evald.f evalbc.f
                  solvbc.f                                                  (step 3)
   bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
-Everything else those units call (LES filters, forcing, MPI, timers, ...) is
+  bla/boxamp.f                                                             (plane statistics)
+  bla/init_filter.f lpf_y.f hpf_y.f bandsolver.f + bla.f 1489-1545         (ADM-RT LES filters)
+Everything else those units call (dynamic SGS models, forcing, MPI, timers, ...) is
 emitted as a stub that aborts if reached; the timers ``ctim``/``wall_time``
 are no-ops.  The channel configuration never reaches a stub.
 """
@@ -45,12 +47,14 @@ UNIT_FILES = [
     "nonlinbl.f", "advection.f", "boxcfl.f", "fft2db.f", "fft2df.f", "getxz.f", "putxz.f",
     "linearbl.f", "getxy.f", "putxy.f", "setmacrhs.f", "trid.f", "dcheb.f", "evald.f",
     "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
+    "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
 ]
 
 MAIN_RANGES = [
     ("bla_rkcoeff", 849, 849),
     ("bla_preprbl", 1080, 1082),
     ("bla_firststep", 1466, 1478),
+    ("bla_lesinit", 1489, 1545),
     ("bla_prhs", 1562, 1569),
     ("bla_pxinit", 1622, 1662),
     ("bla_substep_time", 1796, 1797),

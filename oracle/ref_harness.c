@@ -139,3 +139,32 @@ void sref_grid(double *eta, double *wint) {
  * when iamp > 0 (bla/nonlinbl.f:425-432); amp(nyp,20) is copied out. */
 void sref_set_iamp(int iamp) { v_iamp = iamp > 0 ? iamp : -1000000; }
 void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(double)); }
+
+/* ADM-RT LES (iles = 1) as rparamles.f would leave it for an sgs.i with
+ * cutoff_inv, iord, chi (bla/rparamles.f:31-60), ihighorder as given (the
+ * reference default is 2), then the filter set-up of bla/bla.f:1489-1545 and
+ * chi_scaled = chi/dstar (:2220).  Call after sref_setup, before sref_start. */
+void sref_set_les(int iles, double cutoff_inv, int iord, double chi, int ihighorder) {
+  v_iles = iles; v_cutoff = 1.0 / cutoff_inv; v_iord = iord; v_chi = chi;
+  v_ihighorder = ihighorder; v_cs = 0.0; v_ineg = 1; v_prt = 0.6;
+  v_chi_scaled = v_chi / v_dstar;
+  bla_lesinit();
+}
+
+/* Filter tables: gewy1, gewy2, diags (nyp,5 each), gewspecx (nx/2+2),
+ * gewspecz (nz/2+2), lpfxz (nx/2,nz). */
+void sref_get_filter(double *g1, double *g2, double *dg, double *sx, double *sz, double *lpf) {
+  memcpy(g1, v_gewy1, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(g2, v_gewy2, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(dg, v_diags, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(sx, v_gewspecx, (size_t)(v_nx / 2 + 2) * sizeof(double));
+  memcpy(sz, v_gewspecz, (size_t)(v_nz / 2 + 2) * sizeof(double));
+  memcpy(lpf, v_lpfxz, (size_t)(v_nx / 2) * v_nz * sizeof(double));
+}
+
+/* High-pass filtered velocity gur,gui(memnx,memny,memnz,5), component 1..3. */
+void sref_get_gu(int comp, double *re_part, double *im_part) {
+  long n = slot_size();
+  memcpy(re_part, v_gur + (long)(comp - 1) * n, n * sizeof(double));
+  memcpy(im_part, v_gui + (long)(comp - 1) * n, n * sizeof(double));
+}

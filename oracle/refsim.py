@@ -36,6 +36,9 @@ def _lib(nx, ny, nz, build=True, fma=False):
     lib.sref_grid.argtypes = [dp, dp]
     lib.sref_dims.argtypes = [ctypes.POINTER(ctypes.c_int)]
     lib.sref_set_iamp.argtypes = [ctypes.c_int]
+    lib.sref_set_les.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    lib.sref_get_filter.argtypes = [dp] * 6
+    lib.sref_get_gu.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_amp.argtypes = [dp]
     return lib
 
@@ -105,6 +108,25 @@ class RefSim:
         wint = np.empty(self.nyp)
         self.lib.sref_grid(_dp(eta), _dp(wint))
         return eta, wint
+
+    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1):
+        """ADM-RT LES (bla/rparamles.f defaults), filters set up as bla/bla.f:1489-1545."""
+        self.lib.sref_set_les(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder))
+
+    def filter_tables(self):
+        """gewy1, gewy2, diags (5, nyp); gewspecx (nx/2+2); gewspecz (nz/2+2); lpfxz (nz, nx/2)."""
+        nx, nz = self.dims[0], self.dims[2]
+        g1 = np.empty((5, self.nyp)); g2 = np.empty((5, self.nyp)); dg = np.empty((5, self.nyp))
+        sx = np.empty(nx // 2 + 2); sz = np.empty(nz // 2 + 2); lpf = np.empty((nz, nx // 2))
+        self.lib.sref_get_filter(_dp(g1), _dp(g2), _dp(dg), _dp(sx), _dp(sz), _dp(lpf))
+        return g1, g2, dg, sx, sz, lpf
+
+    def gu(self, comp):
+        """High-pass filtered velocity component comp (1..3), shape (nz, nyp, nx//2)."""
+        re_ = np.empty(self.shape)
+        im_ = np.empty(self.shape)
+        self.lib.sref_get_gu(int(comp), _dp(re_), _dp(im_))
+        return re_ + 1j * im_
 
     def set_iamp(self, iamp):
         """Plane statistics (boxamp) every iamp substeps from the next step on."""

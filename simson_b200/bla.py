@@ -36,6 +36,14 @@ class SgpuParams(ctypes.Structure):
     ]
 
 
+class SgpuLesParams(ctypes.Structure):
+    """sgs.i of the reference (bla/rparamles.f): iles 1 = ADM-RT."""
+    _fields_ = [
+        ("iles", ctypes.c_int), ("cutoff_inv", ctypes.c_double), ("iord", ctypes.c_int),
+        ("chi", ctypes.c_double), ("ihighorder", ctypes.c_int),
+    ]
+
+
 class SimsonError(RuntimeError):
     pass
 
@@ -72,6 +80,8 @@ def load_library(build: bool = True):
     lib.sgpu_host_alloc.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
     lib.sgpu_host_free.argtypes = [vp]
     lib.sgpu_amplitudes.argtypes = [vp, dp, dp]
+    lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
+    lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -193,6 +203,19 @@ class Channel:
         dp = ctypes.POINTER(ctypes.c_double)
         self._check(self.lib.sgpu_download_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
                     "download")
+
+    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1):
+        """ADM-RT large-eddy model (defaults of bla/rparamles.f); call before prhs()."""
+        p = SgpuLesParams(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder))
+        self._check(self.lib.sgpu_set_les(self._ctx, ctypes.byref(p)), "set_les")
+
+    def les_gu(self):
+        """High-pass filtered velocities (gur, gui of the reference), shape (3, nz, ny, nx//2)."""
+        shape = (3,) + self.shape
+        re_ = np.empty(shape)
+        im_ = np.empty(shape)
+        self._check(self.lib.sgpu_download_les(self._ctx, _dp(re_), _dp(im_)), "download_les")
+        return re_ + 1j * im_
 
     AMP_ROW = ("t", "urms", "vrms", "wrms", "omxrms", "omyrms", "omzrms", "omy2_k2", "uv", "e0", "hplus", "px",
                "re_bulk", "tau1", "tau2", "delta99", "delta_star", "theta", "w_bulk")

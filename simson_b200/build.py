@@ -61,7 +61,7 @@ def build_hostcheck(force: bool = False) -> str:
         return HOSTCHECK
     os.makedirs(LIB_DIR, exist_ok=True)
     cmd = [nvcc(), ARCH, "-O2", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
-           "-o", HOSTCHECK + ".tmp", src]
+           "--expt-relaxed-constexpr", "-o", HOSTCHECK + ".tmp", src]
     subprocess.run(cmd, check=True)
     os.replace(HOSTCHECK + ".tmp", HOSTCHECK)
     return HOSTCHECK

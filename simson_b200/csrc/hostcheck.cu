@@ -1,7 +1,12 @@
 // Host build of the pencil algebra of step 3 (the same source the kernels
 // run), exported for the CPU unit tests that compare it with the
 // reference's setmacrhs/trid/dcheb.  Not part of the device library.
+#include <cstring>
+#include <vector>
+
 #include "fft.cuh"
+#include "les.cuh"
+#include "les_filter.h"
 #include "step3.cuh"
 
 using namespace sb;
@@ -57,4 +62,53 @@ extern "C" int sbh_fft(int n, const double* in, double* out, int sign) {
   delete[] b;
   delete[] tw;
   return plan.npass;
+}
+
+// ADM-RT filter tables (les_filter.h) for the CPU comparison with the
+// reference's init_filter: g1, g2 [nyp][5], specx [nx/2+1], specz [nz/2+1],
+// lpfxz [nz][nx/2].  Returns 0, or -1 if the tables cannot be built.
+extern "C" int sbh_les_filter(int nyp, int nx, int nz, double cutoff, int iord, double* g1, double* g2, double* specx,
+                              double* specz, double* lpfxz) {
+  LesFilter F;
+  if (!les_filter_build(nyp, nx, nz, cutoff, iord, F)) return -1;
+  memcpy(g1, F.g1.data(), F.g1.size() * sizeof(double));
+  memcpy(g2, F.g2.data(), F.g2.size() * sizeof(double));
+  memcpy(specx, F.specx.data(), F.specx.size() * sizeof(double));
+  memcpy(specz, F.specz.data(), F.specz.size() * sizeof(double));
+  memcpy(lpfxz, F.lpfxz.data(), F.lpfxz.size() * sizeof(double));
+  return 0;
+}
+
+// One high-pass filtered column (the device routine run on the host):
+// in/out complex interleaved, nyp values; mode = ihighorder.
+extern "C" int sbh_les_hpf_column(int nyp, int nx, int nz, double cutoff, int iord, int mode, int kx, int iz,
+                                  const double* in, double* out) {
+  LesFilter F;
+  if (!les_filter_build(nyp, nx, nz, cutoff, iord, F)) return -1;
+  std::vector<double> coef;
+  les_filter_rows(F, coef);
+  YFilter Y{coef.data(), F.fact2, F.factm2, nyp};
+  std::vector<double2> src(nyp), gu(nyp), Z(nyp);
+  for (int j = 0; j < nyp; ++j) src[j] = double2{in[2 * j], in[2 * j + 1]};
+  const size_t t = (size_t)iz * F.nx2 + kx;
+  les_hpf_column(Y, mode, iord, F.lpfxz[t], F.filtxz[t], src.data(), gu.data(), Z.data(), 1);
+  for (int j = 0; j < nyp; ++j) {
+    out[2 * j] = gu[j].x;
+    out[2 * j + 1] = gu[j].y;
+  }
+  return 0;
+}
+
+// One application of the wall-normal filter (hpf = 1 high pass, 0 low pass)
+// to a real column, as the reference's hpf_y / lpf_y on one row.
+extern "C" int sbh_les_yfilter(int nyp, double cutoff, int hpf, const double* in, double* out) {
+  LesFilter F;
+  if (!les_filter_build(nyp, 8, 8, cutoff, 0, F)) return -1;
+  std::vector<double> coef;
+  les_filter_rows(F, coef);
+  YFilter Y{coef.data(), F.fact2, F.factm2, nyp};
+  std::vector<double2> Z(nyp);
+  yfilter_column(
+      Y, hpf != 0, [&](int j) { return double2{in[j], 0.0}; }, Z.data(), 1, [&](int j, double2 x) { out[j] = x.x; });
+  return 0;
 }

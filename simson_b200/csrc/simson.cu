@@ -16,6 +16,8 @@
 #include "step2.cuh"
 #include "step3.cuh"
 #include "stats.cuh"
+#include "les.cuh"
+#include "les_filter.h"
 
 using namespace sb;
 
@@ -61,6 +63,14 @@ struct sgpu_ctx {
   double* mscr = nullptr;    // mean-flow scratch
   double* meanp = nullptr;   // [4][nyp] U, W, Omega_x, Omega_z for the mixed step 2
   double* ampd = nullptr;    // [20][nyp] plane statistics
+  // ADM-RT LES (sgpu_set_les): gu = high-pass filtered u, v, w [3][nyp][NP]
+  int iles = 0, les_mode = 2, les_iord = 5;
+  double les_chi = 0.0;
+  double2* les_gu = nullptr;
+  double* les_coef = nullptr;  // [nyp][LES_ROW]
+  double* les_lpf = nullptr;   // [NP] L_xz
+  double* les_filt = nullptr;  // [NP] F_xz
+  double les_fact2 = 0.0, les_factm2 = 0.0;
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   // RK bookkeeping (host mirror of the reference driver scalars)
@@ -313,7 +323,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+  void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -418,6 +428,8 @@ static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields,
                                                         skip_oddball, c->twy.d);
 }
 
+static void les_filter_velocity(sgpu_ctx* c, int skip_oddball);
+
 extern "C" int sgpu_prhs(sgpu_ctx* c) {
   if (!c) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
@@ -444,10 +456,29 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   c->launches++;
   // omega_x, omega_z back to physical y into slots 3, 4
   cheb_to_phys(c, czf(c, 4), 3, 2, 0);
+  // ADM-RT: high-pass filtered start-up velocities (bla/prhs.f:95-193)
+  if (c->iles == 1) les_filter_velocity(c, 0);
   (void)fld;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
+}
+
+// gu = high-pass filtered u, v, w of the current state (les.cuh); the
+// scratch columns are free whenever this runs (after the inverse Chebyshev
+// transforms of prhs or of step 3).
+static void les_filter_velocity(sgpu_ctx* c, int skip_oddball) {
+  const Dims& g = c->g;
+  YFilter F{c->les_coef, c->les_fact2, c->les_factm2, g.nyp};
+  dim3 grid((g.NP + 127) / 128, 3);
+  prof_mark(c, K_OTHER);
+  if (c->mixed)
+    k_les_hpf<float2><<<grid, 128, 0, c->stream>>>(c->stf, c->les_gu, czf(c, 0), F, c->les_lpf, c->les_filt, g,
+                                                   c->les_mode, c->les_iord, skip_oddball);
+  else
+    k_les_hpf<double2><<<grid, 128, 0, c->stream>>>(c->st, c->les_gu, czf(c, 0), F, c->les_lpf, c->les_filt, g,
+                                                    c->les_mode, c->les_iord, skip_oddball);
+  c->launches++;
 }
 
 static int enqueue_nonlin(sgpu_ctx* c) {
@@ -500,6 +531,17 @@ static int enqueue_nonlin(sgpu_ctx* c) {
         c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr, 0.0);
   }
   c->launches += 3;
+  if (c->iles == 1) {
+    // ADM-RT relaxation term -chi gu on H (bla/nonlinbl.f:920-965)
+    const size_t n3 = 3 * (size_t)g.nyp * g.NP;
+    const unsigned nb = (unsigned)((n3 + 255) / 256);
+    prof_mark(c, K_OTHER);
+    if (c->mixed)
+      k_les_relax<float2><<<nb, 256, 0, c->stream>>>(c->stf, c->les_gu, g, c->les_chi);
+    else
+      k_les_relax<double2><<<nb, 256, 0, c->stream>>>(c->st, c->les_gu, g, c->les_chi);
+    c->launches++;
+  }
   if (do_cfl) c->cfl_pending = true;
   return cuda_fail(cudaGetLastError(), "nonlin launch");
 }
@@ -556,6 +598,8 @@ static int enqueue_linear(sgpu_ctx* c) {
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
   cheb_to_phys(c, B.OU, 0, 5, 1, /*fp32_input=*/c->mixed);
+  // ADM-RT: high-pass filtered new velocities (bla/linearbl.f:1871-1960)
+  if (c->iles == 1) les_filter_velocity(c, 1);
   prof_mark(c, K_OTHER);
   c->launches += 2;
   // bla/bla.f:2598-2607
@@ -738,5 +782,64 @@ extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
   const double r[19] = {c->t, sum[1], sum[2], sum[3], sum[4], sum[5], sum[6], sum[7], sum[8], e0, hplus, sc[0],
                         sum[13] * c->prm.re / 2., tau1, tau2, delta[1], delta[2], delta[3], wb};
   memcpy(row, r, sizeof(r));
+  return SGPU_OK;
+}
+
+// ADM-RT large-eddy model (bla/rparamles.f, bla/bla.f:1489-1518, 2212-2231):
+// filter tables on the host (les_filter.h), gu and the tables on the device.
+extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
+  if (!c || !p) return SGPU_E_PARAM;
+  if (p->iles == 0) {
+    c->iles = 0;
+    return SGPU_OK;
+  }
+  if (p->iles != 1) {
+    fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0 or 1)\n", p->iles);
+    return SGPU_E_PARAM;
+  }
+  if (!(p->cutoff_inv >= 1.0) || p->iord < 0 || p->iord > 5 || p->ihighorder < 0 || p->ihighorder > 2 ||
+      !(p->chi >= 0.0))
+    return SGPU_E_PARAM;
+  const Dims& g = c->g;
+  if (g.nyp < 7) return SGPU_E_PARAM;
+  LesFilter F;
+  if (!les_filter_build(g.nyp, g.nx, g.nz, 1.0 / p->cutoff_inv, p->iord, F)) return SGPU_E_PARAM;
+  std::vector<double> rows;
+  les_filter_rows(F, rows);
+  const size_t fld = (size_t)g.nyp * g.NP;
+  if (!c->les_gu) {
+    if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&c->les_coef, rows.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->les_lpf, (size_t)g.NP * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->les_filt, (size_t)g.NP * sizeof(double)) != cudaSuccess)
+      return SGPU_E_CUDA;
+    CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
+  }
+  CK(cudaMemcpyAsync(c->les_coef, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->les_lpf, F.lpfxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->les_filt, F.filtxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->les_fact2 = F.fact2;
+  c->les_factm2 = F.factm2;
+  c->les_mode = p->ihighorder;
+  c->les_iord = p->iord;
+  c->les_chi = p->chi;  // chi_scaled = chi / dstar, dstar = 1
+  c->iles = 1;
+  return SGPU_OK;
+}
+
+// gur, gui(memnx, memny, memnz, 1..3) of the reference: the high-pass
+// filtered velocities the next step 2 relaxes towards zero.
+extern "C" int sgpu_download_les(sgpu_ctx* c, double* gr, double* gi) {
+  if (!c || !gr || !gi) return SGPU_E_PARAM;
+  if (c->iles != 1) return SGPU_E_STATE;
+  const size_t n = 3 * (size_t)c->g.nyp * c->g.NP;
+  k_to_ref<<<592, 256, 0, c->stream>>>(c->les_gu, c->stage, c->stage + n, c->g, 3);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(gr, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(gi, c->stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
 }

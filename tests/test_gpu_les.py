@@ -1,0 +1,125 @@
+"""ADM-RT large-eddy model on the device against the translated reference
+(iles = 1, sgs.i of the reference's LES example: cut-off 1/1.5, N = 5,
+chi = 0.2, tensorial filtering unless stated).
+
+The seeded fields carry modes up to |k| = nx/2 - 2 so that the high pass is
+not empty.  gu is a linear filter of u, and a smooth part of u passes it to
+roundoff only, so its error is measured relative to the velocity it was
+filtered from: within 1e-12 after the start-up prhs, 1e-10 after substeps.
+The state keeps the channel step's gate: u, v, w within 1e-11 and every other
+field within 1e-10 (relative L2).  gu of the oddball plane (kz = -nz/2) is
+left out: linearbl never visits that plane and step 2 never reads it."""
+import numpy as np
+import pytest
+
+from simson_b200.fields import channel_field
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _pair(nx, ny, nz, xl, zl, re, dt, rms, seed, need_ref, **les):
+    need_ref(nx, ny, nz)
+    from refsim import RefSim
+    from simson_b200.bla import Channel
+    u, v, w = channel_field(nx, ny, nz, xl, zl, rms, seed, kmax=min(nx, nz) // 2 - 2)
+    ref = RefSim(nx, ny, nz, re, xl, zl, dt)
+    ref.set_les(**les)
+    ref.set_velocity(u, v, w)
+    ref.start()
+    gpu = Channel(nx, ny, nz, re, xl, zl, dt)
+    gpu.set_les(**les)
+    gpu.set_velocity(u, v, w)
+    gpu.start()
+    return ref, gpu
+
+
+def _gu_errors(ref, gpu, nz):
+    keep = np.ones(nz, bool)
+    keep[nz // 2] = False
+    g = gpu.les_gu()
+    rs = ref.state()
+    return [float(np.linalg.norm(g[c][keep] - ref.gu(c + 1)[keep]) / np.linalg.norm(rs[c][keep])) for c in range(3)]
+
+
+def _state_errors(ref, gpu):
+    rs, gs = ref.state(), gpu.state()
+    return [rel_l2(gs[k], rs[k]) for k in range(7)]
+
+
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_les_start_matches_reference(grid, need_ref):
+    nx, ny, nz = grid
+    ref, gpu = _pair(nx, ny, nz, 4 * np.pi, 2 * np.pi, 4200.0, 0.01, 0.05, 3, need_ref)
+    errs = _gu_errors(ref, gpu, nz)
+    assert max(errs) < 1e-12, errs
+
+
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_les_substeps_match_reference(mode, need_ref):
+    nx, ny, nz = 16, 17, 16
+    ref, gpu = _pair(nx, ny, nz, 4 * np.pi, 2 * np.pi, 4200.0, 0.01, 0.05, 5, need_ref, ihighorder=mode)
+    for _ in range(6):
+        ref.substep()
+        gpu.substep()
+        e = _state_errors(ref, gpu)
+        assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+        g = _gu_errors(ref, gpu, nz)
+        assert max(g) < 1e-10, g
+
+
+def test_les_config_d_ten_steps(need_ref):
+    """The LES configuration: 64x97x64 on 2pi x 2 x pi, Re 4200, rms 0.1,
+    dt 0.005, ten RK3 steps with ADM-RT."""
+    nx, ny, nz = 64, 97, 64
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 4, need_ref)
+    for _ in range(30):
+        ref.substep()
+        gpu.substep()
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+    assert max(_gu_errors(ref, gpu, nz)) < 1e-10
+
+
+def test_les_relaxation_acts():
+    """chi > 0 removes energy at the smallest scales: after 20 steps the
+    high-pass energy with the model is below the one without it."""
+    from simson_b200.bla import Channel
+    nx, ny, nz = 48, 65, 48
+    xl, zl = 2 * np.pi, np.pi
+    u, v, w = channel_field(nx, ny, nz, xl, zl, 0.1, 8, kmax=20)
+    e = {}
+    for chi in (0.0, 5.0):
+        ch = Channel(nx, ny, nz, 4200.0, xl, zl, 0.005)
+        ch.set_les(chi=chi)
+        ch.set_velocity(u, v, w)
+        ch.start()
+        ch.substeps(60)
+        g = ch.les_gu()
+        g[:, :, :, 0] = 0.0  # kx = 0 column carries the mean profile's high pass
+        e[chi] = float(np.sum(np.abs(g) ** 2))
+        ch.close()
+    assert e[5.0] < 0.9 * e[0.0], e
+
+
+def test_les_mixed_close_to_fp64():
+    from simson_b200.bla import FP64, MIXED, Channel
+    nx, ny, nz = 64, 97, 64
+    xl, zl = 2 * np.pi, np.pi
+    u, v, w = channel_field(nx, ny, nz, xl, zl, 0.1, 4, kmax=30)
+    out = {}
+    for prec in (FP64, MIXED):
+        ch = Channel(nx, ny, nz, 4200.0, xl, zl, 0.005, precision=prec)
+        ch.set_les()
+        ch.set_velocity(u, v, w)
+        ch.start()
+        ch.substeps(60)
+        out[prec] = ch.state(3)
+        ch.close()
+    keep = np.ones(nz, bool)
+    keep[nz // 2] = False
+    err = rel_l2(np.stack(out[MIXED])[:, keep], np.stack(out[FP64])[:, keep])
+    assert err < 1e-5, err
