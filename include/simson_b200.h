@@ -86,29 +86,42 @@ int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
 int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
 /* Large-eddy model, the reference's sgs.i (bla/rparamles.f:31-60):
- *   iles        0 none, 1 ADM-RT (approximate deconvolution, relaxation term)
+ *   iles        0 none, 1 ADM-RT (approximate deconvolution, relaxation term),
+ *               2 eddy viscosity (Smagorinsky; dynamic when cs = 0)
  *   cutoff_inv  1 / cut-off wavenumber fraction of the primary filter (1.5)
  *   iord        order N of the deconvolution, 0..5 (5)
  *   chi         relaxation coefficient (0.2)
- *   ihighorder  0 two-dimensional, 1 iterative, 2 tensorial filtering (2) */
+ *   ihighorder  0 two-dimensional, 1 iterative, 2 tensorial filtering (2)
+ *   cs          Smagorinsky constant; 0 = dynamic procedure (0)
+ *   ineg        dynamic coefficient: 0 no clipping, 1 C >= 0, 2 nu_t + nu >= 0 (1) */
 typedef struct {
   int iles;
   double cutoff_inv;
   int iord;
   double chi;
   int ihighorder;
+  double cs;
+  int ineg;
 } sgpu_les_params;
 
-/* Enables the LES model: builds the filters of bla/init_filter.f and
- * bla/bla.f:1489-1518 and allocates the filtered-velocity fields.  Call after
- * sgpu_init and before sgpu_prhs (which filters the start-up velocities, as
- * bla/prhs.f:95-193 does); step 2 then adds -chi gu (bla/nonlinbl.f:920-965)
- * and step 3 refilters the new velocities (bla/linearbl.f:1871-1960).
- * iles = 2, 3 (eddy-viscosity models) are rejected with SGPU_E_PARAM. */
+/* Enables the LES model (rparamles + bla/bla.f:1489-1518).  Call after
+ * sgpu_init and before sgpu_prhs.
+ * iles = 1: builds the filters of bla/init_filter.f; sgpu_prhs filters the
+ *   start-up velocities (bla/prhs.f:95-193), step 2 adds -chi gu
+ *   (bla/nonlinbl.f:920-965), step 3 refilters (bla/linearbl.f:1871-1960).
+ * iles = 2: every substep starts with the SGS stress of bla/les.f and its
+ *   divergence (bla/sgs_stress.f, the loops of bla/bla.f:1945-2020); step 2
+ *   adds -sigma (bla/nonlinbl.f:1011-1048).  Needs nx, nz divisible by 4.
+ * iles = 3 (HPF eddy viscosity) is rejected with SGPU_E_PARAM. */
 int sgpu_set_les(sgpu_ctx* ctx, const sgpu_les_params* p);
 
-/* The filtered velocities gur, gui(memnx, memny, memnz, 1..3). */
+/* gur, gui(memnx, memny, memnz, 1..3): the filtered velocities (iles = 1) or
+ * the SGS force sigma (iles = 2). */
 int sgpu_download_les(sgpu_ctx* ctx, double* gr, double* gi);
+
+/* taur, taui(memnx, memny, memnz, 1..6) (iles = 2): the SGS stress of the
+ * last substep, components 11 12 13 22 23 33 (bla/les.f:1620-1640). */
+int sgpu_download_sgs_stress(sgpu_ctx* ctx, double* tr, double* ti);
 
 /* Statistics of the current state, as bla/boxamp.f and bla/wampbl.f:124-278
  * compute them at the start of a full step when iamp > 0: amp[20*ny] in the

@@ -23,6 +23,10 @@ Translated units (reference file: what it contributes):
   bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
   bla/boxamp.f                                                             (plane statistics)
   bla/init_filter.f lpf_y.f hpf_y.f bandsolver.f + bla.f 1489-1545         (ADM-RT LES filters)
+  bla/les.f sgs_stress.f filter_cutoff.f + bla.f 1945-2020                 (eddy-viscosity LES)
+For grids up to SMAG_MAX_POINTS the driver's compile-time switch iiles_smag
+(bla/bla.f:28) is set to 1, as the reference instructs for dynamic
+Smagorinsky runs, so that its SGS-stress arrays exist.
 Everything else those units call (dynamic SGS models, forcing, MPI, timers, ...) is
 emitted as a stub that aborts if reached; the timers ``ctim``/``wall_time``
 are no-ops.  The channel configuration never reaches a stub.
@@ -48,6 +52,7 @@ UNIT_FILES = [
     "linearbl.f", "getxy.f", "putxy.f", "setmacrhs.f", "trid.f", "dcheb.f", "evald.f",
     "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
     "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
+    "les.f", "sgs_stress.f", "filter_cutoff.f",
 ]
 
 MAIN_RANGES = [
@@ -58,6 +63,7 @@ MAIN_RANGES = [
     ("bla_prhs", 1562, 1569),
     ("bla_pxinit", 1622, 1662),
     ("bla_substep_time", 1796, 1797),
+    ("bla_les", 1945, 2020),
     ("bla_boxshift", 1819, 1826),
     ("bla_nonlin", 2251, 2288),
     ("bla_cfl", 2349, 2351),
@@ -67,6 +73,7 @@ MAIN_RANGES = [
 ]
 
 NOOP_STUBS = ("ctim", "wall_time", "fft_identify")
+SMAG_MAX_POINTS = 2_000_000  # nx*ny*nz; larger oracle grids keep iiles_smag = 0
 NTHREAD = 64  # compile-time thread slots (par.f nthread); the harness never runs more
 
 
@@ -88,7 +95,12 @@ def generate_c(nx: int, ny: int, nz: int) -> str:
         with open(os.path.join(REF_BLA, fn)) as f:
             sources.append((fn, f.read()))
     with open(os.path.join(REF_BLA, "bla.f")) as f:
-        sources.append(("bla.f", f.read()))
+        bla = f.read()
+    if nx * ny * nz <= SMAG_MAX_POINTS:
+        bla, n = re.subn(r"iiles_smag = iiles\*0", "iiles_smag = iiles*1", bla)
+        if n != 1:
+            raise RuntimeError("bla.f iiles_smag switch not recognised")
+    sources.append(("bla.f", bla))
     return translate(sources, par_text(nx, ny, nz), defines={"OPENMP"},
                      main_ranges=MAIN_RANGES, stubs_noop=NOOP_STUBS,
                      skip_units=("fft_identify",), provided=("stopnow",))

@@ -97,6 +97,7 @@ void sref_substep(void) {
 #endif
   bla_substep_time();
   bla_boxshift();
+  bla_les();
   bla_nonlin();
   bla_cfl();
   bla_rkweights();
@@ -109,6 +110,7 @@ void sref_substep(void) {
 void sref_nonlin_only(void) {
   bla_substep_time();
   bla_boxshift();
+  bla_les();
   bla_nonlin();
 }
 void sref_linear_only(void) {
@@ -140,13 +142,15 @@ void sref_grid(double *eta, double *wint) {
 void sref_set_iamp(int iamp) { v_iamp = iamp > 0 ? iamp : -1000000; }
 void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(double)); }
 
-/* ADM-RT LES (iles = 1) as rparamles.f would leave it for an sgs.i with
- * cutoff_inv, iord, chi (bla/rparamles.f:31-60), ihighorder as given (the
- * reference default is 2), then the filter set-up of bla/bla.f:1489-1545 and
- * chi_scaled = chi/dstar (:2220).  Call after sref_setup, before sref_start. */
-void sref_set_les(int iles, double cutoff_inv, int iord, double chi, int ihighorder) {
+/* LES as rparamles.f would leave it for an sgs.i with iles, cutoff_inv, iord,
+ * chi, cs, ineg (bla/rparamles.f:31-60), ihighorder as given (the reference
+ * default is 2), then the filter set-up of bla/bla.f:1489-1545 and
+ * chi_scaled = chi/dstar (:2220).  Call after sref_setup, before sref_start.
+ * iles = 2 (eddy viscosity, cs = 0 dynamic) needs an oracle built with
+ * iiles_smag = 1. */
+void sref_set_les(int iles, double cutoff_inv, int iord, double chi, int ihighorder, double cs, int ineg) {
   v_iles = iles; v_cutoff = 1.0 / cutoff_inv; v_iord = iord; v_chi = chi;
-  v_ihighorder = ihighorder; v_cs = 0.0; v_ineg = 1; v_prt = 0.6;
+  v_ihighorder = ihighorder; v_cs = cs; v_ineg = ineg; v_prt = 0.6;
   v_chi_scaled = v_chi / v_dstar;
   bla_lesinit();
 }
@@ -167,4 +171,12 @@ void sref_get_gu(int comp, double *re_part, double *im_part) {
   long n = slot_size();
   memcpy(re_part, v_gur + (long)(comp - 1) * n, n * sizeof(double));
   memcpy(im_part, v_gui + (long)(comp - 1) * n, n * sizeof(double));
+}
+
+/* SGS stress tau_ij (taur, taui slot 1..6: 11 12 13 22 23 33) of the last
+ * les() call; its divergence sigma_i is in gur, gui slots 1..3. */
+void sref_get_tau(int comp, double *re_part, double *im_part) {
+  long n = slot_size();
+  memcpy(re_part, v_taur + (long)(comp - 1) * n, n * sizeof(double));
+  memcpy(im_part, v_taui + (long)(comp - 1) * n, n * sizeof(double));
 }

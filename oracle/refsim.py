@@ -36,7 +36,9 @@ def _lib(nx, ny, nz, build=True, fma=False):
     lib.sref_grid.argtypes = [dp, dp]
     lib.sref_dims.argtypes = [ctypes.POINTER(ctypes.c_int)]
     lib.sref_set_iamp.argtypes = [ctypes.c_int]
-    lib.sref_set_les.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    lib.sref_set_les.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_int]
+    lib.sref_get_tau.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_filter.argtypes = [dp] * 6
     lib.sref_get_gu.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_amp.argtypes = [dp]
@@ -109,9 +111,18 @@ class RefSim:
         self.lib.sref_grid(_dp(eta), _dp(wint))
         return eta, wint
 
-    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1):
-        """ADM-RT LES (bla/rparamles.f defaults), filters set up as bla/bla.f:1489-1545."""
-        self.lib.sref_set_les(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder))
+    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1, cs=0.0, ineg=1):
+        """LES of sgs.i (bla/rparamles.f defaults): iles 1 ADM-RT, 2 eddy viscosity
+        (cs = 0: dynamic Smagorinsky); filters set up as bla/bla.f:1489-1545."""
+        self.lib.sref_set_les(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder),
+                              float(cs), int(ineg))
+
+    def tau(self, comp):
+        """SGS stress component comp (1..6 = 11 12 13 22 23 33), shape (nz, nyp, nx//2)."""
+        re_ = np.empty(self.shape)
+        im_ = np.empty(self.shape)
+        self.lib.sref_get_tau(int(comp), _dp(re_), _dp(im_))
+        return re_ + 1j * im_
 
     def filter_tables(self):
         """gewy1, gewy2, diags (5, nyp); gewspecx (nx/2+2); gewspecz (nz/2+2); lpfxz (nz, nx/2)."""

@@ -37,10 +37,11 @@ class SgpuParams(ctypes.Structure):
 
 
 class SgpuLesParams(ctypes.Structure):
-    """sgs.i of the reference (bla/rparamles.f): iles 1 = ADM-RT."""
+    """sgs.i of the reference (bla/rparamles.f): iles 1 = ADM-RT, 2 = eddy viscosity."""
     _fields_ = [
         ("iles", ctypes.c_int), ("cutoff_inv", ctypes.c_double), ("iord", ctypes.c_int),
         ("chi", ctypes.c_double), ("ihighorder", ctypes.c_int),
+        ("cs", ctypes.c_double), ("ineg", ctypes.c_int),
     ]
 
 
@@ -82,6 +83,7 @@ def load_library(build: bool = True):
     lib.sgpu_amplitudes.argtypes = [vp, dp, dp]
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
+    lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -204,9 +206,11 @@ class Channel:
         self._check(self.lib.sgpu_download_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
                     "download")
 
-    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1):
-        """ADM-RT large-eddy model (defaults of bla/rparamles.f); call before prhs()."""
-        p = SgpuLesParams(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder))
+    def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1, cs=0.0, ineg=1):
+        """Large-eddy model (defaults of bla/rparamles.f): iles 1 ADM-RT, 2 eddy
+        viscosity (cs = 0: dynamic Smagorinsky).  Call before prhs()."""
+        p = SgpuLesParams(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder), float(cs),
+                          int(ineg))
         self._check(self.lib.sgpu_set_les(self._ctx, ctypes.byref(p)), "set_les")
 
     def les_gu(self):
@@ -215,6 +219,14 @@ class Channel:
         re_ = np.empty(shape)
         im_ = np.empty(shape)
         self._check(self.lib.sgpu_download_les(self._ctx, _dp(re_), _dp(im_)), "download_les")
+        return re_ + 1j * im_
+
+    def sgs_stress(self):
+        """tau_ij of the last substep (iles = 2), shape (6, nz, ny, nx//2): 11 12 13 22 23 33."""
+        shape = (6,) + self.shape
+        re_ = np.empty(shape)
+        im_ = np.empty(shape)
+        self._check(self.lib.sgpu_download_sgs_stress(self._ctx, _dp(re_), _dp(im_)), "download_sgs_stress")
         return re_ + 1j * im_
 
     AMP_ROW = ("t", "urms", "vrms", "wrms", "omxrms", "omyrms", "omzrms", "omy2_k2", "uv", "e0", "hplus", "px",

@@ -1,0 +1,428 @@
+// Eddy-viscosity large-eddy model on the device (iles = 2): the Smagorinsky
+// stress tau_ij = -2 C Delta^2 |S| S_ij with the dynamic (Germano/Lilly)
+// coefficient C, its divergence sigma_i = d tau_ij / dx_j, and -sigma added
+// to H in step 2.  The reference computes tau plane by plane in bla/les.f
+// (before nonlinbl, every substep), sigma pencil by pencil in
+// bla/sgs_stress.f, and adds it in bla/nonlinbl.f:1011-1048.
+//
+// Grid: the stored modes on the nx x nz grid (no 3/2 padding), as les.f's
+// getxz(...,0,...) and its length-nx / length-nz transforms.
+//
+//   k_sgs_zinv   per plane and kx block: u, v, w and the six strain-rate
+//                components S_ij (from u, v, w, omega_x, omega_z: x and z
+//                derivatives spectrally, y derivatives from the vorticity and
+//                continuity, les.f:288-327), oddball zeroed, inverse z FFT
+//   k_sgs_xpass1 per plane and z row: inverse x FFT (two real fields per
+//                complex FFT), |S|; the 21 fields the test filter acts on
+//                (M_ij parts, L_ij parts, S_ij, u_i; les.f:709-771), forward
+//                x FFT, keep kx < nx/4 (filter_cutoff.f)
+//   k_sgs_zfilt  forward z FFT, keep |kz| <= nz/4, inverse z FFT
+//   k_sgs_xpass2 inverse x FFT of the filtered fields, L_ij and M_ij
+//                (les.f:783-881), per-point M:L and M:M
+//   k_sgs_coef   C(x, y) = max(<M:L>_z / (2 <M:M>_z), 0), the average over z
+//                (les.f:1385-1480, ineg = 1 clipping, zero at the walls)
+//   k_sgs_tau_x  tau_ij / (nx nz) (les.f:1489-1560), forward x FFT
+//   k_sgs_zfwd   forward z FFT, oddball zeroed: tau in the state layout
+//   k_sgs_sigma  per pencil, on Chebyshev coefficients of tau:
+//                sigma_i = i alpha tau_i1 + i beta tau_i3 + D tau_i2
+//                (bla/sgs_stress.f)
+//
+// All arithmetic is FP64 whatever the state storage.
+#pragma once
+#include "fft.cuh"
+#include "layout.cuh"
+#include "step3.cuh"
+
+namespace sb {
+
+struct SgsBufs {
+  double2* spec9;   // [9][nyp][nz][nx/2]   z physical, x spectral
+  double* phys10;   // [10][nyp][nz][nx]    u v w S11 S12 S13 S22 S23 S33 |S|
+  double2* filt21;  // [21][nyp][nz][nx/4]  test-filtered fields, x spectral
+  double* numden;   // [2][nyp][nz][nx]     M:L and M:M per point
+  double* cxy;      // [nyp][nx]            C(x, y)
+  double2* tauz6;   // [6][nyp][nz][nx/2]   tau, z physical, x spectral
+  double2* tau;     // [6][nyp][NP]         tau, state layout
+};
+
+struct SgsGrid {
+  int nx, nz, nx2, nx4, nyp, NP, zodd;
+};
+
+// u, v, w, S11, S12, S13, S22, S23, S33 spectral at (y, iz, kx)
+template <class V>
+__device__ __forceinline__ double2 sgs_spec_field(const V* st, size_t slot, size_t off, int f, double a, double b) {
+  auto ld = [&](int s) { const V q = st[(size_t)s * slot + off]; return double2{(double)q.x, (double)q.y}; };
+  // i k q = (-k q.y, k q.x)
+  switch (f) {
+    case 0: return ld(0);
+    case 1: return ld(1);
+    case 2: return ld(2);
+    case 3: { const double2 u = ld(0); return double2{-a * u.y, a * u.x}; }
+    case 4: {
+      // S12 = (dv/dx + du/dy)/2, du/dy = dv/dx - omega_z
+      const double2 v = ld(1), oz = ld(4);
+      const double2 dvdx{-a * v.y, a * v.x};
+      return double2{.5 * (dvdx.x + (dvdx.x - oz.x)), .5 * (dvdx.y + (dvdx.y - oz.y))};
+    }
+    case 5: {
+      const double2 u = ld(0), w = ld(2);
+      return double2{.5 * (-a * w.y + -b * u.y), .5 * (a * w.x + b * u.x)};
+    }
+    case 6: {
+      // dv/dy = -du/dx - dw/dz
+      const double2 u = ld(0), w = ld(2);
+      return double2{a * u.y + b * w.y, -a * u.x - b * w.x};
+    }
+    case 7: {
+      // S23 = (dv/dz + dw/dy)/2, dw/dy = omega_x + dv/dz
+      const double2 v = ld(1), ox = ld(3);
+      const double2 dvdz{-b * v.y, b * v.x};
+      return double2{.5 * (dvdz.x + (ox.x + dvdz.x)), .5 * (dvdz.y + (ox.y + dvdz.y))};
+    }
+    default: { const double2 w = ld(2); return double2{-b * w.y, b * w.x}; }
+  }
+}
+
+template <class V, int KB>
+__global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPlan plan,
+                           const double2* __restrict__ tw, const double* __restrict__ alfa,
+                           const double* __restrict__ beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* b0 = reinterpret_cast<double2*>(smem_raw);
+  double2* b1 = b0 + (size_t)G.nz * KB;
+  const int y = blockIdx.y;
+  const int kx0 = blockIdx.x * KB;
+  const size_t slot = (size_t)G.nyp * G.NP;
+  for (int f = 0; f < 9; ++f) {
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int iz = t / KB;
+      const int kx = kx0 + t - iz * KB;
+      double2 val{0.0, 0.0};
+      if (kx < G.nx2 && iz != G.zodd)
+        val = sgs_spec_field(st, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz]);
+      b0[t] = val;
+    }
+    __syncthreads();
+    double2* res = fft_columns<double, KB>(b0, b1, plan, tw, +1);
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int kx = kx0 + t - m * KB;
+      if (kx < G.nx2) B.spec9[(((size_t)f * G.nyp + y) * G.nz + m) * G.nx2 + kx] = res[t];
+    }
+    __syncthreads();
+  }
+}
+
+// Hermitian completion of the half spectra a, b (kx < nk, the rest zero) of
+// two real rows into the spectrum of a + i b at index k of a length-n FFT.
+__device__ __forceinline__ double2 sgs_pair(const double2* a, const double2* b, int k, int n, int nk) {
+  if (k == 0) return double2{a ? a[0].x : 0.0, b ? b[0].x : 0.0};
+  if (k < nk) {
+    const double2 p = a ? a[k] : double2{0.0, 0.0}, q = b ? b[k] : double2{0.0, 0.0};
+    return double2{p.x - q.y, p.y + q.x};
+  }
+  if (k > n - nk) {
+    const int kk = n - k;
+    const double2 p = a ? a[kk] : double2{0.0, 0.0}, q = b ? b[kk] : double2{0.0, 0.0};
+    return double2{p.x + q.y, q.x - p.y};
+  }
+  return double2{0.0, 0.0};
+}
+
+// sqrt(2 (S11^2 + S22^2 + S33^2) + 4 (S12^2 + S13^2 + S23^2)), les.f:660-665
+__device__ __forceinline__ double sgs_sabs(const double* s) {
+  return sqrt(2. * (s[0] * s[0] + s[3] * s[3] + s[5] * s[5]) + 4. * (s[1] * s[1] + s[2] * s[2] + s[4] * s[4]));
+}
+
+// One z row per CTA.  Shared memory: two buffers of 11 columns x nx.
+__global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
+                             const double* __restrict__ delta2) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NC = 11;
+  double2* bA = reinterpret_cast<double2*>(smem_raw);
+  double2* bB = bA + (size_t)G.nx * NC;
+  const int m = blockIdx.x, y = blockIdx.y;
+  const int n = G.nx;
+  const size_t fs9 = (size_t)G.nyp * G.nz * G.nx2;
+  const size_t row = ((size_t)y * G.nz + m) * G.nx2;
+  // five complex FFTs carry the nine real rows (u+iv, w+iS11, S12+iS13, S22+iS23, S33)
+  for (int t = threadIdx.x; t < n * 5; t += blockDim.x) {
+    const int k = t / 5, c = t - 5 * (t / 5);
+    const double2* a = B.spec9 + (size_t)(2 * c) * fs9 + row;
+    const double2* b = (2 * c + 1 < 9) ? B.spec9 + (size_t)(2 * c + 1) * fs9 + row : nullptr;
+    bA[k * 5 + c] = sgs_pair(a, b, k, n, G.nx2);
+  }
+  __syncthreads();
+  double2* res = fft_columns<double, 5>(bA, bB, plan, tw, +1);
+  double2* oth = (res == bA) ? bB : bA;
+  const double d2 = delta2[y];
+  const size_t fs10 = (size_t)G.nyp * G.nz * G.nx;
+  const size_t prow = ((size_t)y * G.nz + m) * G.nx;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double q[9];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const double2 z = res[j * 5 + c];
+      q[2 * c] = z.x;
+      if (2 * c + 1 < 9) q[2 * c + 1] = z.y;
+    }
+    const double u = q[0], v = q[1], w = q[2];
+    const double* s = q + 3;  // S11 S12 S13 S22 S23 S33
+    const double sabs = sgs_sabs(s);
+#pragma unroll
+    for (int f = 0; f < 9; ++f) B.phys10[(size_t)f * fs10 + prow + j] = q[f];
+    B.phys10[(size_t)9 * fs10 + prow + j] = sabs;
+    const double dr = sabs * d2;
+    double r[22];
+    for (int l = 0; l < 6; ++l) r[l] = -s[l] * dr;  // M parts
+    r[6] = -u * u;                                   // L parts
+    r[7] = -v * u;
+    r[8] = -w * u;
+    r[9] = -v * v;
+    r[10] = -w * v;
+    r[11] = -w * w;
+    for (int l = 0; l < 6; ++l) r[12 + l] = s[l];  // B = S
+    r[18] = u;
+    r[19] = v;
+    r[20] = w;
+    r[21] = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) oth[j * NC + c] = double2{r[2 * c], r[2 * c + 1]};
+  }
+  __syncthreads();
+  double2* fres = fft_columns<double, NC>(oth, res, plan, tw, -1);
+  const size_t fs21 = (size_t)G.nyp * G.nz * G.nx4;
+  const size_t frow = ((size_t)y * G.nz + m) * G.nx4;
+  for (int t = threadIdx.x; t < G.nx4 * NC; t += blockDim.x) {
+    const int k = t / NC, c = t - NC * (t / NC);
+    const double2 a = fres[k * NC + c];
+    const double2 b = fres[((n - k) % n) * NC + c];
+    // spectra of the real and imaginary rows
+    B.filt21[(size_t)(2 * c) * fs21 + frow + k] = double2{(a.x + b.x) * .5, (a.y - b.y) * .5};
+    if (2 * c + 1 < 21) B.filt21[(size_t)(2 * c + 1) * fs21 + frow + k] = double2{(a.y + b.y) * .5, (b.x - a.x) * .5};
+  }
+}
+
+// Test filter in z on the kept kx < nx/4 columns: forward FFT, zero
+// nz/4 < |kz| (filter_cutoff.f: z = nz/4+2 .. nz-nz/4 zeroed), inverse FFT.
+template <int KB>
+__global__ void k_sgs_zfilt(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* b0 = reinterpret_cast<double2*>(smem_raw);
+  double2* b1 = b0 + (size_t)G.nz * KB;
+  const int y = blockIdx.y;
+  const int kx0 = blockIdx.x * KB;
+  const size_t fs21 = (size_t)G.nyp * G.nz * G.nx4;
+  const int zlo = G.nz / 4 + 1, zhi = G.nz - G.nz / 4 - 1;
+  for (int f = 0; f < 21; ++f) {
+    double2* fld = B.filt21 + (size_t)f * fs21 + (size_t)y * G.nz * G.nx4;
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int kx = kx0 + t - m * KB;
+      b0[t] = (kx < G.nx4) ? fld[(size_t)m * G.nx4 + kx] : double2{0.0, 0.0};
+    }
+    __syncthreads();
+    double2* res = fft_columns<double, KB>(b0, b1, plan, tw, -1);
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int m = t / KB;
+      if (m >= zlo && m <= zhi) res[t] = double2{0.0, 0.0};
+    }
+    __syncthreads();
+    double2* oth = (res == b0) ? b1 : b0;
+    double2* back = fft_columns<double, KB>(res, oth, plan, tw, +1);
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int kx = kx0 + t - m * KB;
+      if (kx < G.nx4) fld[(size_t)m * G.nx4 + kx] = back[t];
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse x FFT of the 21 test-filtered fields (divided by nx nz as
+// filter_cutoff.f does), then L_ij, M_ij and the per-point contractions.
+__global__ void k_sgs_xpass2(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
+                             const double* __restrict__ delta2) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NC = 11;
+  double2* bA = reinterpret_cast<double2*>(smem_raw);
+  double2* bB = bA + (size_t)G.nx * NC;
+  const int m = blockIdx.x, y = blockIdx.y;
+  const int n = G.nx;
+  const size_t fs21 = (size_t)G.nyp * G.nz * G.nx4;
+  const size_t frow = ((size_t)y * G.nz + m) * G.nx4;
+  for (int t = threadIdx.x; t < n * NC; t += blockDim.x) {
+    const int k = t / NC, c = t - NC * (t / NC);
+    const double2* a = B.filt21 + (size_t)(2 * c) * fs21 + frow;
+    const double2* b = (2 * c + 1 < 21) ? B.filt21 + (size_t)(2 * c + 1) * fs21 + frow : nullptr;
+    bA[k * NC + c] = sgs_pair(a, b, k, n, G.nx4);
+  }
+  __syncthreads();
+  double2* res = fft_columns<double, NC>(bA, bB, plan, tw, +1);
+  const double inv = 1.0 / (double)(G.nx * G.nz);
+  const double gd2 = pow(4., 2. / 3.) * delta2[y];
+  const size_t fs10 = (size_t)G.nyp * G.nz * G.nx;
+  const size_t prow = ((size_t)y * G.nz + m) * G.nx;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double r[22];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const double2 z = res[j * NC + c];
+      r[2 * c] = z.x * inv;
+      r[2 * c + 1] = z.y * inv;
+    }
+    const double* mt = r;       // filtered M parts
+    const double* lt = r + 6;   // filtered -u_i u_j
+    const double* bt = r + 12;  // filtered S
+    const double u = r[18], v = r[19], w = r[20];
+    double L[6], M[6];
+    L[0] = lt[0] + u * u;
+    L[1] = lt[1] + v * u;
+    L[2] = lt[2] + w * u;
+    L[3] = lt[3] + v * v;
+    L[4] = lt[4] + w * v;
+    L[5] = lt[5] + w * w;
+    const double dr = gd2 * sgs_sabs(bt);
+    for (int l = 0; l < 6; ++l) M[l] = mt[l] + bt[l] * dr;
+    const double num = M[0] * L[0] + M[3] * L[3] + M[5] * L[5] + 2. * (M[1] * L[1] + M[2] * L[2] + M[4] * L[4]);
+    const double den = M[0] * M[0] + M[3] * M[3] + M[5] * M[5] + 2. * (M[1] * M[1] + M[2] * M[2] + M[4] * M[4]);
+    B.numden[prow + j] = num;
+    B.numden[fs10 + prow + j] = den;
+  }
+}
+
+// C(x, y) from the z averages (les.f:1385-1480).  cs > 0: fixed C = cs^2.
+// ineg: 0 no clipping, 1 C >= 0 and zero at the walls, 2 zero at the walls
+// (the nu_t + nu >= 0 clip follows in k_sgs_tau_x).
+__global__ void k_sgs_coef(SgsBufs B, SgsGrid G, double cs, int ineg) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= G.nx) return;
+  double c;
+  if (cs != 0.0) {
+    c = cs * cs;
+  } else {
+    const size_t plane = (size_t)G.nyp * G.nz * G.nx;
+    double num = 0.0, den = 0.0;
+    for (int m = 0; m < G.nz; ++m) {
+      const size_t o = ((size_t)y * G.nz + m) * G.nx + x;
+      num += B.numden[o];
+      den += B.numden[plane + o];
+    }
+    const bool wall = (y == 0 || y == G.nyp - 1);
+    if (ineg == 1)
+      c = wall ? 0.0 : fmax(.5 * num / den, 0.);
+    else if (ineg == 2)
+      c = wall ? 0.0 : .5 * num / den;
+    else
+      c = .5 * num / den;
+  }
+  B.cxy[(size_t)y * G.nx + x] = c;
+}
+
+// tau_ij / (nx nz) = -2 C Delta^2 |S| S_ij / (nx nz) in physical space, then
+// the forward x FFT (three complex FFTs for the six real rows).
+__global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
+                            const double* __restrict__ delta2, double re, int ineg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* bA = reinterpret_cast<double2*>(smem_raw);
+  double2* bB = bA + (size_t)G.nx * 3;
+  const int m = blockIdx.x, y = blockIdx.y;
+  const int n = G.nx;
+  const size_t fs10 = (size_t)G.nyp * G.nz * G.nx;
+  const size_t prow = ((size_t)y * G.nz + m) * G.nx;
+  const double gd2 = 1. / (double)(G.nx * G.nz);
+  const double d2 = delta2[y];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double dr = B.cxy[(size_t)y * G.nx + j] * B.phys10[9 * fs10 + prow + j] * d2;
+    if (ineg == 2 && dr < -1. / re) dr = -1. / re;
+    const double d1 = -2. * dr * gd2;
+    double t[6];
+    for (int l = 0; l < 6; ++l) t[l] = d1 * B.phys10[(size_t)(3 + l) * fs10 + prow + j];
+    for (int c = 0; c < 3; ++c) bA[j * 3 + c] = double2{t[2 * c], t[2 * c + 1]};
+  }
+  __syncthreads();
+  double2* res = fft_columns<double, 3>(bA, bB, plan, tw, -1);
+  const size_t fs = (size_t)G.nyp * G.nz * G.nx2;
+  const size_t row = ((size_t)y * G.nz + m) * G.nx2;
+  for (int t = threadIdx.x; t < G.nx2 * 3; t += blockDim.x) {
+    const int k = t / 3, c = t - 3 * (t / 3);
+    const double2 a = res[k * 3 + c];
+    const double2 b = res[((n - k) % n) * 3 + c];
+    B.tauz6[(size_t)(2 * c) * fs + row + k] = double2{(a.x + b.x) * .5, (a.y - b.y) * .5};
+    B.tauz6[(size_t)(2 * c + 1) * fs + row + k] = double2{(a.y + b.y) * .5, (b.x - a.x) * .5};
+  }
+}
+
+// Forward z FFT of tau; the oddball kz = -nz/2 is zeroed (les.f:1576-1590).
+template <int KB>
+__global__ void k_sgs_zfwd(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* b0 = reinterpret_cast<double2*>(smem_raw);
+  double2* b1 = b0 + (size_t)G.nz * KB;
+  const int y = blockIdx.y;
+  const int kx0 = blockIdx.x * KB;
+  const size_t fs = (size_t)G.nyp * G.nz * G.nx2;
+  const size_t slot = (size_t)G.nyp * G.NP;
+  for (int f = 0; f < 6; ++f) {
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int m = t / KB;
+      const int kx = kx0 + t - m * KB;
+      b0[t] = (kx < G.nx2) ? B.tauz6[(size_t)f * fs + ((size_t)y * G.nz + m) * G.nx2 + kx] : double2{0.0, 0.0};
+    }
+    __syncthreads();
+    double2* res = fft_columns<double, KB>(b0, b1, plan, tw, -1);
+    for (int t = threadIdx.x; t < G.nz * KB; t += blockDim.x) {
+      const int iz = t / KB;
+      const int kx = kx0 + t - iz * KB;
+      if (kx < G.nx2)
+        B.tau[(size_t)f * slot + (size_t)y * G.NP + (size_t)iz * G.nx2 + kx] =
+            (iz == G.zodd) ? double2{0.0, 0.0} : res[t];
+    }
+    __syncthreads();
+  }
+}
+
+// sigma_i on Chebyshev coefficients (bla/sgs_stress.f): tc = Chebyshev
+// coefficients of tau [6][nyp][NP], sc = output [3][nyp][NP].
+__global__ void k_sgs_sigma(const double2* __restrict__ tc, double2* __restrict__ sc, SgsGrid G,
+                            const double* __restrict__ alfa, const double* __restrict__ beta) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= G.NP) return;
+  const int kx = p % G.nx2, iz = p / G.nx2;
+  const double a = alfa[kx], b = beta[iz];
+  const size_t fld = (size_t)G.nyp * G.NP;
+  // sigma_1 = i a tau11 + i b tau13 + D tau12; sigma_2 = i a tau12 + i b tau23
+  // + D tau22; sigma_3 = i a tau13 + i b tau33 + D tau23
+  const int cx[3] = {0, 1, 2}, cz[3] = {2, 4, 5}, cy[3] = {1, 3, 4};
+  for (int i = 0; i < 3; ++i) {
+    for (int y = 0; y < G.nyp; ++y) {
+      const double2 tx = tc[(size_t)cx[i] * fld + (size_t)y * G.NP + p];
+      const double2 tz = tc[(size_t)cz[i] * fld + (size_t)y * G.NP + p];
+      sc[(size_t)i * fld + (size_t)y * G.NP + p] = double2{-a * tx.y - b * tz.y, a * tx.x + b * tz.x};
+    }
+    // + D tau_i2 (derivative in coefficient space, bla/dcheb.f), real and
+    // imaginary parts as separate columns; the result goes through a scratch
+    // column: the derivative of column cy[i] into sc's spare slot 3
+    double2* dst = const_cast<double2*>(sc) + 3 * fld;
+    cheb_deriv(Col{reinterpret_cast<double*>(dst) + 2 * (size_t)p, 2 * (size_t)G.NP},
+               Col{const_cast<double*>(reinterpret_cast<const double*>(tc + (size_t)cy[i] * fld)) + 2 * (size_t)p,
+                   2 * (size_t)G.NP},
+               G.nyp);
+    cheb_deriv(Col{reinterpret_cast<double*>(dst) + 2 * (size_t)p + 1, 2 * (size_t)G.NP},
+               Col{const_cast<double*>(reinterpret_cast<const double*>(tc + (size_t)cy[i] * fld)) + 2 * (size_t)p + 1,
+                   2 * (size_t)G.NP},
+               G.nyp);
+    for (int y = 0; y < G.nyp; ++y) {
+      const size_t o = (size_t)y * G.NP + p;
+      const double2 d = dst[o];
+      double2 s = sc[(size_t)i * fld + o];
+      s.x = s.x + d.x;
+      s.y = s.y + d.y;
+      sc[(size_t)i * fld + o] = s;
+    }
+  }
+}
+
+}  // namespace sb

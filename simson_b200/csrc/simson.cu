@@ -18,6 +18,7 @@
 #include "stats.cuh"
 #include "les.cuh"
 #include "les_filter.h"
+#include "les_dyn.cuh"
 
 using namespace sb;
 
@@ -71,8 +72,14 @@ struct sgpu_ctx {
   double* les_lpf = nullptr;   // [NP] L_xz
   double* les_filt = nullptr;  // [NP] F_xz
   double les_fact2 = 0.0, les_factm2 = 0.0;
+  // eddy-viscosity LES (iles = 2): buffers on the unpadded nx x nz grid
+  SgsBufs sgs{};
+  double* sgs_delta2 = nullptr;  // [nyp] Delta^2 (bla/preprbl.f:62-71)
+  double les_cs = 0.0;
+  int les_ineg = 1;
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
+  Tw sgs_twz, sgs_twx;  // lengths nz and nx (iles = 2)
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
   int it = 1;
@@ -323,7 +330,9 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+  void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
+                  c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
+                  c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -481,10 +490,49 @@ static void les_filter_velocity(sgpu_ctx* c, int skip_oddball) {
   c->launches++;
 }
 
+static SgsGrid sgs_grid(const sgpu_ctx* c) {
+  const Dims& g = c->g;
+  return SgsGrid{g.nx, g.nz, g.nx2, g.nx / 4, g.nyp, g.NP, g.zodd};
+}
+
+// Eddy-viscosity SGS force sigma_i = d tau_ij/dx_j of the current state into
+// les_gu (bla/les.f + bla/sgs_stress.f, before nonlinbl in every substep).
+static void enqueue_sgs(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const SgsGrid G = sgs_grid(c);
+  constexpr int KB = 4;
+  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+  const size_t sx11 = 2 * (size_t)g.nx * 11 * sizeof(double2);
+  const size_t sx3 = 2 * (size_t)g.nx * 3 * sizeof(double2);
+  prof_mark(c, K_OTHER);
+  dim3 gz((g.nx2 + KB - 1) / KB, g.nyp), gz4((G.nx4 + KB - 1) / KB, g.nyp), gx(g.nz, g.nyp);
+  if (c->mixed)
+    k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                       c->beta);
+  else
+    k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                        c->beta);
+  k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+  k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
+  k_sgs_xpass2<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+  k_sgs_coef<<<dim3((g.nx + 127) / 128, g.nyp), 128, 0, c->stream>>>(c->sgs, G, c->les_cs, c->les_ineg);
+  k_sgs_tau_x<<<gx, 128, sx3, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, c->prm.re,
+                                           c->les_ineg);
+  k_sgs_zfwd<KB><<<gz, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
+  c->launches += 7;
+  // sigma on Chebyshev coefficients of tau (sgs_stress.f), back to physical y
+  const size_t fld = (size_t)g.nyp * g.NP;
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->sgs.tau, fld, czf(c, 0), fld, 6, 0, 1.0, 0, c->twy.d);
+  k_sgs_sigma<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(czf(c, 0), czf(c, 6), G, c->alfa, c->beta);
+  c->launches++;
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 6), fld, c->les_gu, fld, 3, 1, 1.0, 0, c->twy.d);
+}
+
 static int enqueue_nonlin(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   c->tc = c->t + c->cnp1;
+  if (c->iles == 2) enqueue_sgs(c);
   // CFL partial maxima only on the substeps the reference evaluates them
   // (nonlinbl.f: mod(it-1,icfl) == 0); the device word keeps the last one.
   const bool do_cfl = (P.icfl > 0) && ((c->it - 1) % P.icfl == 0);
@@ -531,15 +579,16 @@ static int enqueue_nonlin(sgpu_ctx* c) {
         c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr, 0.0);
   }
   c->launches += 3;
-  if (c->iles == 1) {
-    // ADM-RT relaxation term -chi gu on H (bla/nonlinbl.f:920-965)
+  if (c->iles == 1 || c->iles == 2) {
+    // ADM-RT relaxation term -chi gu on H (bla/nonlinbl.f:920-965), or the
+    // eddy-viscosity SGS force -sigma (chi = 1, :1011-1048)
     const size_t n3 = 3 * (size_t)g.nyp * g.NP;
     const unsigned nb = (unsigned)((n3 + 255) / 256);
     prof_mark(c, K_OTHER);
     if (c->mixed)
-      k_les_relax<float2><<<nb, 256, 0, c->stream>>>(c->stf, c->les_gu, g, c->les_chi);
+      k_les_relax<float2><<<nb, 256, 0, c->stream>>>(c->stf, c->les_gu, g, c->iles == 2 ? 1.0 : c->les_chi);
     else
-      k_les_relax<double2><<<nb, 256, 0, c->stream>>>(c->st, c->les_gu, g, c->les_chi);
+      k_les_relax<double2><<<nb, 256, 0, c->stream>>>(c->st, c->les_gu, g, c->iles == 2 ? 1.0 : c->les_chi);
     c->launches++;
   }
   if (do_cfl) c->cfl_pending = true;
@@ -793,22 +842,72 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
     c->iles = 0;
     return SGPU_OK;
   }
+  const Dims& g = c->g;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  if (p->iles == 2) {
+    // eddy viscosity: cs = 0 dynamic (Germano/Lilly), else fixed C = cs^2
+    if (p->ineg < 0 || p->ineg > 2 || (p->cs != 0.0 && p->ineg != 1) || !(p->cs >= 0.0) || g.nx % 4 || g.nz % 4)
+      return SGPU_E_PARAM;
+    constexpr int KB = 4;
+    const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+    const size_t sx11 = 2 * (size_t)g.nx * 11 * sizeof(double2);
+    if (sz > 227 * 1024 || sx11 > 227 * 1024) return SGPU_E_PARAM;
+    if (!c->sgs.spec9) {
+      int rc;
+      if ((rc = make_tw(c->sgs_twz, g.nz)) || (rc = make_tw(c->sgs_twx, g.nx))) return rc;
+      const size_t pl = (size_t)g.nyp * g.nz * g.nx;  // one real field on the nx x nz grid
+      if (cudaMalloc(&c->sgs.spec9, 9 * fld * sizeof(double2)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.phys10, 10 * pl * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.filt21, 21 * (size_t)g.nyp * g.nz * (g.nx / 4) * sizeof(double2)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.numden, 2 * pl * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.cxy, (size_t)g.nyp * g.nx * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.tauz6, 6 * fld * sizeof(double2)) != cudaSuccess ||
+          cudaMalloc(&c->sgs.tau, 6 * fld * sizeof(double2)) != cudaSuccess ||
+          cudaMalloc(&c->sgs_delta2, (size_t)g.nyp * sizeof(double)) != cudaSuccess)
+        return SGPU_E_CUDA;
+      if (!c->les_gu) {
+        if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) return SGPU_E_CUDA;
+        CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
+      }
+      const int sm[3] = {(int)sz, (int)sx11, (int)(2 * (size_t)g.nx * 3 * sizeof(double2))};
+      cudaFuncSetAttribute(k_sgs_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+      cudaFuncSetAttribute(k_sgs_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+      cudaFuncSetAttribute(k_sgs_zfilt<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+      cudaFuncSetAttribute(k_sgs_zfwd<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+      cudaFuncSetAttribute(k_sgs_xpass1, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
+      cudaFuncSetAttribute(k_sgs_xpass2, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
+      cudaFuncSetAttribute(k_sgs_tau_x, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[2]);
+    }
+    // Delta^2 = (dx dz dy)^(2/3), dy the geometric mean of the two
+    // neighbouring Gauss-Lobatto spacings, 1 - eta_2 at the walls
+    const double pi = 3.1415926535897932385;
+    std::vector<double> eta(g.nyp), d2(g.nyp);
+    for (int y = 0; y < g.nyp; ++y) eta[y] = cos(pi * (double)y / (double)(g.nyp - 1));
+    for (int y = 0; y < g.nyp; ++y) {
+      const double dy = (y == 0 || y == g.nyp - 1) ? 1. - eta[1] : sqrt((eta[y + 1] - eta[y]) * (eta[y] - eta[y - 1]));
+      d2[y] = pow(c->prm.xl / (double)g.nx * c->prm.zl / (double)g.nz * dy, 2. / 3.);
+    }
+    CK(cudaMemcpyAsync(c->sgs_delta2, d2.data(), g.nyp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->les_cs = p->cs;
+    c->les_ineg = p->ineg;
+    c->iles = 2;
+    return SGPU_OK;
+  }
   if (p->iles != 1) {
-    fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0 or 1)\n", p->iles);
+    fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0, 1 or 2)\n", p->iles);
     return SGPU_E_PARAM;
   }
   if (!(p->cutoff_inv >= 1.0) || p->iord < 0 || p->iord > 5 || p->ihighorder < 0 || p->ihighorder > 2 ||
       !(p->chi >= 0.0))
     return SGPU_E_PARAM;
-  const Dims& g = c->g;
   if (g.nyp < 7) return SGPU_E_PARAM;
   LesFilter F;
   if (!les_filter_build(g.nyp, g.nx, g.nz, 1.0 / p->cutoff_inv, p->iord, F)) return SGPU_E_PARAM;
   std::vector<double> rows;
   les_filter_rows(F, rows);
-  const size_t fld = (size_t)g.nyp * g.NP;
-  if (!c->les_gu) {
-    if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess ||
+  if (!c->les_coef) {
+    if ((!c->les_gu && cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) ||
         cudaMalloc(&c->les_coef, rows.size() * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->les_lpf, (size_t)g.NP * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->les_filt, (size_t)g.NP * sizeof(double)) != cudaSuccess)
@@ -833,13 +932,28 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
 // filtered velocities the next step 2 relaxes towards zero.
 extern "C" int sgpu_download_les(sgpu_ctx* c, double* gr, double* gi) {
   if (!c || !gr || !gi) return SGPU_E_PARAM;
-  if (c->iles != 1) return SGPU_E_STATE;
+  if (c->iles != 1 && c->iles != 2) return SGPU_E_STATE;
   const size_t n = 3 * (size_t)c->g.nyp * c->g.NP;
   k_to_ref<<<592, 256, 0, c->stream>>>(c->les_gu, c->stage, c->stage + n, c->g, 3);
   c->launches++;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(gr, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(gi, c->stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+// tau_ij of the last eddy-viscosity evaluation (taur, taui slots 1..6:
+// 11 12 13 22 23 33) in the reference layout.
+extern "C" int sgpu_download_sgs_stress(sgpu_ctx* c, double* tr, double* ti) {
+  if (!c || !tr || !ti) return SGPU_E_PARAM;
+  if (c->iles != 2) return SGPU_E_STATE;
+  const size_t n = 6 * (size_t)c->g.nyp * c->g.NP;  // the staging area holds 7 slots
+  k_to_ref<<<592, 256, 0, c->stream>>>(c->sgs.tau, c->stage, c->stage + n, c->g, 6);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(tr, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(ti, c->stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
 }

@@ -123,3 +123,68 @@ def test_les_mixed_close_to_fp64():
     keep[nz // 2] = False
     err = rel_l2(np.stack(out[MIXED])[:, keep], np.stack(out[FP64])[:, keep])
     assert err < 1e-5, err
+
+
+# --- eddy-viscosity model (iles = 2, dynamic Smagorinsky) -------------------
+
+def _tau_errors(ref, gpu, nz):
+    keep = np.ones(nz, bool)
+    keep[nz // 2] = False
+    t = gpu.sgs_stress()
+    out = []
+    for c in range(6):
+        r = ref.tau(c + 1)
+        out.append(float(np.linalg.norm(t[c][keep] - r[keep]) / max(np.linalg.norm(r[keep]), 1e-300)))
+    return out
+
+
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_dynamic_smagorinsky_stress_matches_reference(grid, need_ref):
+    """tau_ij of les.f and sigma_i of sgs_stress.f on the start-up state
+    (evaluated inside the first substep), then the state after it."""
+    nx, ny, nz = grid
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 6, need_ref, iles=2)
+    ref.substep()
+    gpu.substep()
+    te = _tau_errors(ref, gpu, nz)
+    assert max(te) < 1e-11, te
+    se = _gu_errors(ref, gpu, nz)
+    assert max(se) < 1e-11, se
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+def test_dynamic_smagorinsky_substeps(need_ref):
+    nx, ny, nz = 16, 17, 16
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 7, need_ref, iles=2)
+    for _ in range(6):
+        ref.substep()
+        gpu.substep()
+        e = _state_errors(ref, gpu)
+        assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+def test_dynamic_smagorinsky_config_d(need_ref):
+    """The LES configuration 64x97x64, 2pi x 2 x pi, ten RK3 steps."""
+    nx, ny, nz = 64, 97, 64
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 4, need_ref, iles=2)
+    for _ in range(30):
+        ref.substep()
+        gpu.substep()
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+    assert max(_tau_errors(ref, gpu, nz)) < 1e-10
+
+
+@pytest.mark.parametrize("cs,ineg", [(0.1, 1), (0.0, 0), (0.0, 2)])
+def test_smagorinsky_variants(cs, ineg, need_ref):
+    """Fixed Smagorinsky constant, and the dynamic model without clipping and
+    with the nu_t + nu >= 0 clip."""
+    nx, ny, nz = 16, 17, 16
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 8, need_ref, iles=2, cs=cs, ineg=ineg)
+    for _ in range(3):
+        ref.substep()
+        gpu.substep()
+    assert max(_tau_errors(ref, gpu, nz)) < 1e-10
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
