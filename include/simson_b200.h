@@ -123,6 +123,28 @@ int sgpu_download_les(sgpu_ctx* ctx, double* gr, double* gi);
  * last substep, components 11 12 13 22 23 33 (bla/les.f:1620-1640). */
 int sgpu_download_sgs_stress(sgpu_ctx* ctx, double* tr, double* ti);
 
+/* Learned SGS model (no counterpart in the reference): an MLP from the
+ * resolved velocity gradient and the wall distance to the SGS stress,
+ *   x_(3i+j) = s_in du_i/dx_j,  x_9 = s_y (1 - |y|)
+ *   tau = s_out (W3 tanh(W2 tanh(W1 x + b1) + b2) + b3)
+ * (w1 [64][10], w2 [64][64], w3 [6][64] row-major, biases b1[64], b2[64],
+ * b3[6]; tau components 11 12 13 22 23 33).  Weights and activations are
+ * used in BF16 with FP32 accumulation.  The stress takes the place of the
+ * eddy-viscosity stress (bla/les.f:1620-1640): its divergence is formed as
+ * bla/sgs_stress.f does and subtracted from H in step 2. */
+typedef struct {
+  const float *w1, *b1, *w2, *b2, *w3, *b3;
+  float s_in, s_y, s_out;
+} sgpu_sgs_mlp;
+
+/* Enables the learned model for the following substeps (replaces any LES
+ * model set with sgpu_set_les).  Needs nx, nz divisible by 4. */
+int sgpu_set_sgs_mlp(sgpu_ctx* ctx, const sgpu_sgs_mlp* p);
+
+/* The MLP alone on n feature rows: x[n][10] -> y[n][6] (host arrays), the
+ * same tensor-core kernel the step runs.  Loads p's weights. */
+int sgpu_sgs_mlp_eval(sgpu_ctx* ctx, const sgpu_sgs_mlp* p, const float* x, float* y, long long n);
+
 /* Statistics of the current state, as bla/boxamp.f and bla/wampbl.f:124-278
  * compute them at the start of a full step when iamp > 0: amp[20*ny] in the
  * layout of amp(nyp,20) (plane averages of squared velocity and vorticity

@@ -45,6 +45,11 @@ class SgpuLesParams(ctypes.Structure):
     ]
 
 
+class SgpuSgsMlp(ctypes.Structure):
+    _fields_ = [(n, ctypes.POINTER(ctypes.c_float)) for n in ("w1", "b1", "w2", "b2", "w3", "b3")] + [
+        ("s_in", ctypes.c_float), ("s_y", ctypes.c_float), ("s_out", ctypes.c_float)]
+
+
 class SimsonError(RuntimeError):
     pass
 
@@ -84,6 +89,9 @@ def load_library(build: bool = True):
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    lib.sgpu_set_sgs_mlp.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp)]
+    lib.sgpu_sgs_mlp_eval.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp), fp, fp, ctypes.c_longlong]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -220,6 +228,29 @@ class Channel:
         im_ = np.empty(shape)
         self._check(self.lib.sgpu_download_les(self._ctx, _dp(re_), _dp(im_)), "download_les")
         return re_ + 1j * im_
+
+    @staticmethod
+    def _mlp_struct(weights, s_in, s_y, s_out):
+        keep = {k: np.ascontiguousarray(weights[k], dtype=np.float32) for k in ("w1", "b1", "w2", "b2", "w3", "b3")}
+        fp = ctypes.POINTER(ctypes.c_float)
+        st = SgpuSgsMlp(*[keep[k].ctypes.data_as(fp) for k in ("w1", "b1", "w2", "b2", "w3", "b3")],
+                        float(s_in), float(s_y), float(s_out))
+        return st, keep
+
+    def set_sgs_mlp(self, weights, s_in=1.0, s_y=1.0, s_out=1.0):
+        """Learned SGS model: weights dict w1 (64,10), b1 (64), w2 (64,64), b2, w3 (6,64), b3 (6)."""
+        st, keep = self._mlp_struct(weights, s_in, s_y, s_out)
+        self._check(self.lib.sgpu_set_sgs_mlp(self._ctx, ctypes.byref(st)), "set_sgs_mlp")
+
+    def sgs_mlp_eval(self, weights, x, s_in=1.0, s_y=1.0, s_out=1.0):
+        """The tensor-core MLP on feature rows x (n, 10) -> (n, 6)."""
+        st, keep = self._mlp_struct(weights, s_in, s_y, s_out)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty((x.shape[0], 6), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.sgpu_sgs_mlp_eval(self._ctx, ctypes.byref(st), x.ctypes.data_as(fp),
+                                               y.ctypes.data_as(fp), x.shape[0]), "sgs_mlp_eval")
+        return y
 
     def sgs_stress(self):
         """tau_ij of the last substep (iles = 2), shape (6, nz, ny, nx//2): 11 12 13 22 23 33."""

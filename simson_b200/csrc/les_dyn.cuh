@@ -49,11 +49,35 @@ struct SgsGrid {
   int nx, nz, nx2, nx4, nyp, NP, zodd;
 };
 
-// u, v, w, S11, S12, S13, S22, S23, S33 spectral at (y, iz, kx)
+// Field set 0: u, v, w, S11, S12, S13, S22, S23, S33; field set 1: the nine
+// gradients du_i/dx_j (i-major), spectral at (y, iz, kx)
 template <class V>
-__device__ __forceinline__ double2 sgs_spec_field(const V* st, size_t slot, size_t off, int f, double a, double b) {
+__device__ __forceinline__ double2 sgs_spec_field(const V* st, size_t slot, size_t off, int f, double a, double b,
+                                                  int set) {
   auto ld = [&](int s) { const V q = st[(size_t)s * slot + off]; return double2{(double)q.x, (double)q.y}; };
   // i k q = (-k q.y, k q.x)
+  if (set == 1) {
+    switch (f) {
+      case 0: { const double2 u = ld(0); return double2{-a * u.y, a * u.x}; }
+      case 1: {
+        const double2 v = ld(1), oz = ld(4);
+        return double2{-a * v.y - oz.x, a * v.x - oz.y};
+      }
+      case 2: { const double2 u = ld(0); return double2{-b * u.y, b * u.x}; }
+      case 3: { const double2 v = ld(1); return double2{-a * v.y, a * v.x}; }
+      case 4: {
+        const double2 u = ld(0), w = ld(2);
+        return double2{a * u.y + b * w.y, -a * u.x - b * w.x};
+      }
+      case 5: { const double2 v = ld(1); return double2{-b * v.y, b * v.x}; }
+      case 6: { const double2 w = ld(2); return double2{-a * w.y, a * w.x}; }
+      case 7: {
+        const double2 v = ld(1), ox = ld(3);
+        return double2{ox.x - b * v.y, ox.y + b * v.x};
+      }
+      default: { const double2 w = ld(2); return double2{-b * w.y, b * w.x}; }
+    }
+  }
   switch (f) {
     case 0: return ld(0);
     case 1: return ld(1);
@@ -87,7 +111,7 @@ __device__ __forceinline__ double2 sgs_spec_field(const V* st, size_t slot, size
 template <class V, int KB>
 __global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPlan plan,
                            const double2* __restrict__ tw, const double* __restrict__ alfa,
-                           const double* __restrict__ beta) {
+                           const double* __restrict__ beta, int set) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* b0 = reinterpret_cast<double2*>(smem_raw);
   double2* b1 = b0 + (size_t)G.nz * KB;
@@ -100,7 +124,7 @@ __global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPl
       const int kx = kx0 + t - iz * KB;
       double2 val{0.0, 0.0};
       if (kx < G.nx2 && iz != G.zodd)
-        val = sgs_spec_field(st, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz]);
+        val = sgs_spec_field(st, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz], set);
       b0[t] = val;
     }
     __syncthreads();
@@ -201,6 +225,34 @@ __global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
     // spectra of the real and imaginary rows
     B.filt21[(size_t)(2 * c) * fs21 + frow + k] = double2{(a.x + b.x) * .5, (a.y - b.y) * .5};
     if (2 * c + 1 < 21) B.filt21[(size_t)(2 * c + 1) * fs21 + frow + k] = double2{(a.y + b.y) * .5, (b.x - a.x) * .5};
+  }
+}
+
+// The nine gradient rows of one z row back to physical x (learned model):
+// phys10 fields 0..8.
+__global__ void k_sgs_xinv9(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* bA = reinterpret_cast<double2*>(smem_raw);
+  double2* bB = bA + (size_t)G.nx * 5;
+  const int m = blockIdx.x, y = blockIdx.y;
+  const int n = G.nx;
+  const size_t fs9 = (size_t)G.nyp * G.nz * G.nx2;
+  const size_t row = ((size_t)y * G.nz + m) * G.nx2;
+  for (int t = threadIdx.x; t < n * 5; t += blockDim.x) {
+    const int k = t / 5, c = t - 5 * (t / 5);
+    const double2* a = B.spec9 + (size_t)(2 * c) * fs9 + row;
+    const double2* b = (2 * c + 1 < 9) ? B.spec9 + (size_t)(2 * c + 1) * fs9 + row : nullptr;
+    bA[k * 5 + c] = sgs_pair(a, b, k, n, G.nx2);
+  }
+  __syncthreads();
+  double2* res = fft_columns<double, 5>(bA, bB, plan, tw, +1);
+  const size_t fs10 = (size_t)G.nyp * G.nz * G.nx;
+  const size_t prow = ((size_t)y * G.nz + m) * G.nx;
+  for (int t = threadIdx.x; t < n * 5; t += blockDim.x) {
+    const int j = t / 5, c = t - 5 * (t / 5);
+    const double2 z = res[j * 5 + c];
+    B.phys10[(size_t)(2 * c) * fs10 + prow + j] = z.x;
+    if (2 * c + 1 < 9) B.phys10[(size_t)(2 * c + 1) * fs10 + prow + j] = z.y;
   }
 }
 
@@ -323,8 +375,11 @@ __global__ void k_sgs_coef(SgsBufs B, SgsGrid G, double cs, int ineg) {
 
 // tau_ij / (nx nz) = -2 C Delta^2 |S| S_ij / (nx nz) in physical space, then
 // the forward x FFT (three complex FFTs for the six real rows).
+// tau_phys != nullptr: the stress is given in physical space ([6][nyp*nz*nx],
+// the learned model) instead of -2 C Delta^2 |S| S_ij.
 __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
-                            const double* __restrict__ delta2, double re, int ineg) {
+                            const double* __restrict__ delta2, double re, int ineg,
+                            const double* __restrict__ tau_phys) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* bA = reinterpret_cast<double2*>(smem_raw);
   double2* bB = bA + (size_t)G.nx * 3;
@@ -335,11 +390,15 @@ __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
   const double gd2 = 1. / (double)(G.nx * G.nz);
   const double d2 = delta2[y];
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    double dr = B.cxy[(size_t)y * G.nx + j] * B.phys10[9 * fs10 + prow + j] * d2;
-    if (ineg == 2 && dr < -1. / re) dr = -1. / re;
-    const double d1 = -2. * dr * gd2;
     double t[6];
-    for (int l = 0; l < 6; ++l) t[l] = d1 * B.phys10[(size_t)(3 + l) * fs10 + prow + j];
+    if (tau_phys != nullptr) {
+      for (int l = 0; l < 6; ++l) t[l] = tau_phys[(size_t)l * fs10 + prow + j] * gd2;
+    } else {
+      double dr = B.cxy[(size_t)y * G.nx + j] * B.phys10[9 * fs10 + prow + j] * d2;
+      if (ineg == 2 && dr < -1. / re) dr = -1. / re;
+      const double d1 = -2. * dr * gd2;
+      for (int l = 0; l < 6; ++l) t[l] = d1 * B.phys10[(size_t)(3 + l) * fs10 + prow + j];
+    }
     for (int c = 0; c < 3; ++c) bA[j * 3 + c] = double2{t[2 * c], t[2 * c + 1]};
   }
   __syncthreads();

@@ -19,6 +19,7 @@
 #include "les.cuh"
 #include "les_filter.h"
 #include "les_dyn.cuh"
+#include "sgs_mlp.cuh"
 
 using namespace sb;
 
@@ -77,6 +78,11 @@ struct sgpu_ctx {
   double* sgs_delta2 = nullptr;  // [nyp] Delta^2 (bla/preprbl.f:62-71)
   double les_cs = 0.0;
   int les_ineg = 1;
+  // learned SGS model (sgpu_set_sgs_mlp; internal iles = 4)
+  unsigned char* mlp_image = nullptr;
+  double* mlp_tau = nullptr;  // [6][nyp][nz][nx] physical tau
+  int* mlp_err = nullptr;
+  float mlp_s_in = 1.f, mlp_s_y = 1.f, mlp_s_out = 1.f;
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   Tw sgs_twz, sgs_twx;  // lengths nz and nx (iles = 2)
@@ -332,7 +338,8 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
-                  c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+                  c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->mlp_image, c->mlp_tau,
+                  c->mlp_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -506,20 +513,47 @@ static void enqueue_sgs(sgpu_ctx* c) {
   const size_t sx3 = 2 * (size_t)g.nx * 3 * sizeof(double2);
   prof_mark(c, K_OTHER);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp), gz4((G.nx4 + KB - 1) / KB, g.nyp), gx(g.nz, g.nyp);
+  const int set = (c->iles == 4) ? 1 : 0;
   if (c->mixed)
     k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                       c->beta);
+                                                       c->beta, set);
   else
     k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                        c->beta);
+                                                        c->beta, set);
+  if (c->iles == 4) {
+    // learned model: gradients to physical space, MLP on the tensor cores,
+    // tau / (nx nz) back to Fourier space
+    k_sgs_xinv9<<<gx, 128, 2 * (size_t)g.nx * 5 * sizeof(double2), c->stream>>>(c->sgs, G, c->sgs_twx.plan,
+                                                                                 c->sgs_twx.d);
+    MlpArgs A{};
+    A.image = c->mlp_image;
+    A.mode = 1;
+    A.n = (long long)g.nyp * g.nz * g.nx;
+    A.grad = c->sgs.phys10;
+    A.tau = c->mlp_tau;
+    A.plane = g.nz * g.nx;
+    A.nyp = g.nyp;
+    A.s_in = c->mlp_s_in;
+    A.s_y = c->mlp_s_y;
+    A.s_out = c->mlp_s_out;
+    A.err = c->mlp_err;
+    const long long tiles = (A.n + MLP_ROWS - 1) / MLP_ROWS;
+    const int blocks = (int)std::min<long long>(tiles, 148 * 4);
+    k_sgs_mlp<<<blocks, 128, MLP_SMEM_LAUNCH, c->stream>>>(A);
+    k_sgs_tau_x<<<gx, 128, sx3, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, c->prm.re,
+                                             c->les_ineg, c->mlp_tau);
+    k_sgs_zfwd<KB><<<gz, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
+    c->launches += 5;
+  } else {
   k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
   k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
   k_sgs_xpass2<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
   k_sgs_coef<<<dim3((g.nx + 127) / 128, g.nyp), 128, 0, c->stream>>>(c->sgs, G, c->les_cs, c->les_ineg);
   k_sgs_tau_x<<<gx, 128, sx3, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, c->prm.re,
-                                           c->les_ineg);
+                                           c->les_ineg, nullptr);
   k_sgs_zfwd<KB><<<gz, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
   c->launches += 7;
+  }
   // sigma on Chebyshev coefficients of tau (sgs_stress.f), back to physical y
   const size_t fld = (size_t)g.nyp * g.NP;
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->sgs.tau, fld, czf(c, 0), fld, 6, 0, 1.0, 0, c->twy.d);
@@ -532,7 +566,7 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   c->tc = c->t + c->cnp1;
-  if (c->iles == 2) enqueue_sgs(c);
+  if (c->iles == 2 || c->iles == 4) enqueue_sgs(c);
   // CFL partial maxima only on the substeps the reference evaluates them
   // (nonlinbl.f: mod(it-1,icfl) == 0); the device word keeps the last one.
   const bool do_cfl = (P.icfl > 0) && ((c->it - 1) % P.icfl == 0);
@@ -579,16 +613,16 @@ static int enqueue_nonlin(sgpu_ctx* c) {
         c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr, 0.0);
   }
   c->launches += 3;
-  if (c->iles == 1 || c->iles == 2) {
+  if (c->iles >= 1) {
     // ADM-RT relaxation term -chi gu on H (bla/nonlinbl.f:920-965), or the
     // eddy-viscosity SGS force -sigma (chi = 1, :1011-1048)
     const size_t n3 = 3 * (size_t)g.nyp * g.NP;
     const unsigned nb = (unsigned)((n3 + 255) / 256);
     prof_mark(c, K_OTHER);
     if (c->mixed)
-      k_les_relax<float2><<<nb, 256, 0, c->stream>>>(c->stf, c->les_gu, g, c->iles == 2 ? 1.0 : c->les_chi);
+      k_les_relax<float2><<<nb, 256, 0, c->stream>>>(c->stf, c->les_gu, g, c->iles == 1 ? c->les_chi : 1.0);
     else
-      k_les_relax<double2><<<nb, 256, 0, c->stream>>>(c->st, c->les_gu, g, c->iles == 2 ? 1.0 : c->les_chi);
+      k_les_relax<double2><<<nb, 256, 0, c->stream>>>(c->st, c->les_gu, g, c->iles == 1 ? c->les_chi : 1.0);
     c->launches++;
   }
   if (do_cfl) c->cfl_pending = true;
@@ -834,6 +868,57 @@ extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
   return SGPU_OK;
 }
 
+// Buffers, transforms and Delta^2 of the eddy-viscosity and learned models.
+static int sgs_setup(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  if (g.nx % 4 || g.nz % 4) return SGPU_E_PARAM;
+  constexpr int KB = 4;
+  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+  const size_t sx11 = 2 * (size_t)g.nx * 11 * sizeof(double2);
+  if (sz > 227 * 1024 || sx11 > 227 * 1024) return SGPU_E_PARAM;
+  if (!c->sgs.spec9) {
+    int rc;
+    if ((rc = make_tw(c->sgs_twz, g.nz)) || (rc = make_tw(c->sgs_twx, g.nx))) return rc;
+    const size_t pl = (size_t)g.nyp * g.nz * g.nx;  // one real field on the nx x nz grid
+    if (cudaMalloc(&c->sgs.spec9, 9 * fld * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.phys10, 10 * pl * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.filt21, 21 * (size_t)g.nyp * g.nz * (g.nx / 4) * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.numden, 2 * pl * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.cxy, (size_t)g.nyp * g.nx * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.tauz6, 6 * fld * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&c->sgs.tau, 6 * fld * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&c->sgs_delta2, (size_t)g.nyp * sizeof(double)) != cudaSuccess)
+      return SGPU_E_CUDA;
+    if (!c->les_gu) {
+      if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) return SGPU_E_CUDA;
+      CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
+    }
+    const int sm[4] = {(int)sz, (int)sx11, (int)(2 * (size_t)g.nx * 3 * sizeof(double2)),
+                       (int)(2 * (size_t)g.nx * 5 * sizeof(double2))};
+    cudaFuncSetAttribute(k_sgs_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+    cudaFuncSetAttribute(k_sgs_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+    cudaFuncSetAttribute(k_sgs_zfilt<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+    cudaFuncSetAttribute(k_sgs_zfwd<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
+    cudaFuncSetAttribute(k_sgs_xpass1, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
+    cudaFuncSetAttribute(k_sgs_xpass2, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
+    cudaFuncSetAttribute(k_sgs_tau_x, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[2]);
+    cudaFuncSetAttribute(k_sgs_xinv9, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[3]);
+  }
+  // Delta^2 = (dx dz dy)^(2/3), dy the geometric mean of the two
+  // neighbouring Gauss-Lobatto spacings, 1 - eta_2 at the walls
+  const double pi = 3.1415926535897932385;
+  std::vector<double> eta(g.nyp), d2(g.nyp);
+  for (int y = 0; y < g.nyp; ++y) eta[y] = cos(pi * (double)y / (double)(g.nyp - 1));
+  for (int y = 0; y < g.nyp; ++y) {
+    const double dy = (y == 0 || y == g.nyp - 1) ? 1. - eta[1] : sqrt((eta[y + 1] - eta[y]) * (eta[y] - eta[y - 1]));
+    d2[y] = pow(c->prm.xl / (double)g.nx * c->prm.zl / (double)g.nz * dy, 2. / 3.);
+  }
+  CK(cudaMemcpyAsync(c->sgs_delta2, d2.data(), g.nyp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
 // ADM-RT large-eddy model (bla/rparamles.f, bla/bla.f:1489-1518, 2212-2231):
 // filter tables on the host (les_filter.h), gu and the tables on the device.
 extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
@@ -846,49 +931,9 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
   const size_t fld = (size_t)g.nyp * g.NP;
   if (p->iles == 2) {
     // eddy viscosity: cs = 0 dynamic (Germano/Lilly), else fixed C = cs^2
-    if (p->ineg < 0 || p->ineg > 2 || (p->cs != 0.0 && p->ineg != 1) || !(p->cs >= 0.0) || g.nx % 4 || g.nz % 4)
-      return SGPU_E_PARAM;
-    constexpr int KB = 4;
-    const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
-    const size_t sx11 = 2 * (size_t)g.nx * 11 * sizeof(double2);
-    if (sz > 227 * 1024 || sx11 > 227 * 1024) return SGPU_E_PARAM;
-    if (!c->sgs.spec9) {
-      int rc;
-      if ((rc = make_tw(c->sgs_twz, g.nz)) || (rc = make_tw(c->sgs_twx, g.nx))) return rc;
-      const size_t pl = (size_t)g.nyp * g.nz * g.nx;  // one real field on the nx x nz grid
-      if (cudaMalloc(&c->sgs.spec9, 9 * fld * sizeof(double2)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.phys10, 10 * pl * sizeof(double)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.filt21, 21 * (size_t)g.nyp * g.nz * (g.nx / 4) * sizeof(double2)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.numden, 2 * pl * sizeof(double)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.cxy, (size_t)g.nyp * g.nx * sizeof(double)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.tauz6, 6 * fld * sizeof(double2)) != cudaSuccess ||
-          cudaMalloc(&c->sgs.tau, 6 * fld * sizeof(double2)) != cudaSuccess ||
-          cudaMalloc(&c->sgs_delta2, (size_t)g.nyp * sizeof(double)) != cudaSuccess)
-        return SGPU_E_CUDA;
-      if (!c->les_gu) {
-        if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) return SGPU_E_CUDA;
-        CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
-      }
-      const int sm[3] = {(int)sz, (int)sx11, (int)(2 * (size_t)g.nx * 3 * sizeof(double2))};
-      cudaFuncSetAttribute(k_sgs_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
-      cudaFuncSetAttribute(k_sgs_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
-      cudaFuncSetAttribute(k_sgs_zfilt<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
-      cudaFuncSetAttribute(k_sgs_zfwd<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
-      cudaFuncSetAttribute(k_sgs_xpass1, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
-      cudaFuncSetAttribute(k_sgs_xpass2, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[1]);
-      cudaFuncSetAttribute(k_sgs_tau_x, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[2]);
-    }
-    // Delta^2 = (dx dz dy)^(2/3), dy the geometric mean of the two
-    // neighbouring Gauss-Lobatto spacings, 1 - eta_2 at the walls
-    const double pi = 3.1415926535897932385;
-    std::vector<double> eta(g.nyp), d2(g.nyp);
-    for (int y = 0; y < g.nyp; ++y) eta[y] = cos(pi * (double)y / (double)(g.nyp - 1));
-    for (int y = 0; y < g.nyp; ++y) {
-      const double dy = (y == 0 || y == g.nyp - 1) ? 1. - eta[1] : sqrt((eta[y + 1] - eta[y]) * (eta[y] - eta[y - 1]));
-      d2[y] = pow(c->prm.xl / (double)g.nx * c->prm.zl / (double)g.nz * dy, 2. / 3.);
-    }
-    CK(cudaMemcpyAsync(c->sgs_delta2, d2.data(), g.nyp * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    if (p->ineg < 0 || p->ineg > 2 || (p->cs != 0.0 && p->ineg != 1) || !(p->cs >= 0.0)) return SGPU_E_PARAM;
+    int rc = sgs_setup(c);
+    if (rc) return rc;
     c->les_cs = p->cs;
     c->les_ineg = p->ineg;
     c->iles = 2;
@@ -932,7 +977,7 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
 // filtered velocities the next step 2 relaxes towards zero.
 extern "C" int sgpu_download_les(sgpu_ctx* c, double* gr, double* gi) {
   if (!c || !gr || !gi) return SGPU_E_PARAM;
-  if (c->iles != 1 && c->iles != 2) return SGPU_E_STATE;
+  if (c->iles < 1) return SGPU_E_STATE;
   const size_t n = 3 * (size_t)c->g.nyp * c->g.NP;
   k_to_ref<<<592, 256, 0, c->stream>>>(c->les_gu, c->stage, c->stage + n, c->g, 3);
   c->launches++;
@@ -947,7 +992,7 @@ extern "C" int sgpu_download_les(sgpu_ctx* c, double* gr, double* gi) {
 // 11 12 13 22 23 33) in the reference layout.
 extern "C" int sgpu_download_sgs_stress(sgpu_ctx* c, double* tr, double* ti) {
   if (!c || !tr || !ti) return SGPU_E_PARAM;
-  if (c->iles != 2) return SGPU_E_STATE;
+  if (c->iles != 2 && c->iles != 4) return SGPU_E_STATE;
   const size_t n = 6 * (size_t)c->g.nyp * c->g.NP;  // the staging area holds 7 slots
   k_to_ref<<<592, 256, 0, c->stream>>>(c->sgs.tau, c->stage, c->stage + n, c->g, 6);
   c->launches++;
@@ -956,4 +1001,82 @@ extern "C" int sgpu_download_sgs_stress(sgpu_ctx* c, double* tr, double* ti) {
   CK(cudaMemcpyAsync(ti, c->stage + n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
+}
+
+// Learned SGS model (no counterpart in the reference): weights and scalings,
+// then every substep uses it in place of the eddy-viscosity stress.
+static int mlp_image_upload(sgpu_ctx* c, const sgpu_sgs_mlp* p) {
+  if (!p->w1 || !p->b1 || !p->w2 || !p->b2 || !p->w3 || !p->b3) return SGPU_E_PARAM;
+  std::vector<unsigned char> img(MLP_IMAGE_BYTES);
+  mlp_build_image(p->w1, p->b1, p->w2, p->b2, p->w3, p->b3, img.data());
+  if (!c->mlp_image) {
+    if (cudaMalloc(&c->mlp_image, MLP_IMAGE_BYTES) != cudaSuccess ||
+        cudaMalloc(&c->mlp_err, sizeof(int)) != cudaSuccess)
+      return SGPU_E_CUDA;
+    cudaFuncSetAttribute(k_sgs_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM_LAUNCH);
+  }
+  CK(cudaMemcpyAsync(c->mlp_image, img.data(), MLP_IMAGE_BYTES, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->mlp_err, 0, sizeof(int), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->mlp_s_in = p->s_in;
+  c->mlp_s_y = p->s_y;
+  c->mlp_s_out = p->s_out;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_set_sgs_mlp(sgpu_ctx* c, const sgpu_sgs_mlp* p) {
+  if (!c || !p) return SGPU_E_PARAM;
+  int rc = mlp_image_upload(c, p);
+  if (rc) return rc;
+  if ((rc = sgs_setup(c))) return rc;
+  if (!c->mlp_tau && cudaMalloc(&c->mlp_tau, 6 * (size_t)c->g.nyp * c->g.nz * c->g.nx * sizeof(double)) != cudaSuccess)
+    return SGPU_E_CUDA;
+  c->iles = 4;
+  return SGPU_OK;
+}
+
+// The MLP alone on n host feature rows x[n][10] -> y[n][6] (the kernel the
+// step uses, features given instead of formed from the velocity gradient).
+extern "C" int sgpu_sgs_mlp_eval(sgpu_ctx* c, const sgpu_sgs_mlp* p, const float* x, float* y, long long n) {
+  if (!c || !p || !x || !y || n < 0) return SGPU_E_PARAM;
+  if (n == 0) return SGPU_OK;
+  int rc = mlp_image_upload(c, p);
+  if (rc) return rc;
+  float *dx = nullptr, *dy = nullptr;
+  if (cudaMalloc(&dx, (size_t)n * MLP_IN * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&dy, (size_t)n * MLP_OUT * sizeof(float)) != cudaSuccess) {
+    cudaFree(dx);
+    return SGPU_E_CUDA;
+  }
+  MlpArgs A{};
+  A.image = c->mlp_image;
+  A.mode = 0;
+  A.n = n;
+  A.x = dx;
+  A.y = dy;
+  A.s_in = p->s_in;
+  A.s_y = p->s_y;
+  A.s_out = p->s_out;
+  A.err = c->mlp_err;
+  int err = 0;
+  rc = SGPU_OK;
+  if (cudaMemcpyAsync(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    rc = SGPU_E_CUDA;
+  if (!rc) {
+    const long long tiles = (n + MLP_ROWS - 1) / MLP_ROWS;
+    k_sgs_mlp<<<(int)std::min<long long>(tiles, 148 * 4), 128, MLP_SMEM_LAUNCH, c->stream>>>(A);
+    c->launches++;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(y, dy, (size_t)n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&err, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+      rc = SGPU_E_CUDA;
+  }
+  cudaFree(dx);
+  cudaFree(dy);
+  if (!rc && err) {
+    fprintf(stderr, "simson_b200: sgpu_sgs_mlp_eval: tensor-core wait timed out\n");
+    rc = SGPU_E_CUDA;
+  }
+  return rc;
 }

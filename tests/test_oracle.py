@@ -105,3 +105,10 @@ def test_amp_row_laminar_channel():
     assert row[15] == 2.0 and row[18] == 0.0
     # displacement thickness of 1 - y^2 over [-1, 1]: 2 - 4/3
     assert abs(row[16] - 2.0 / 3.0) < 1e-13
+
+
+def test_bf16_rounding_of_the_mlp_oracle():
+    from sgs_mlp import bf16
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 0.0], np.float32)
+    # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: to even (1); 1 + 3 * 2^-8 -> 1 + 2^-6
+    np.testing.assert_array_equal(bf16(x), np.array([1.0, 1.0, 1.0 + 2 ** -6, -2.5, 0.0], np.float32))
