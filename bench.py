@@ -119,12 +119,17 @@ def kernel_bytes(name, w, precision="fp64"):
     fld = nx2 * ny * nz * c          # one spectral field
     fine = nx2 * ny * nzp * c        # one z-transformed field on the 3/2 z grid
     f64 = nx2 * ny * nz * 16         # a field kept in FP64 (Chebyshev-space scratch of step 3)
+    # Chebyshev-space fields of step 3: FP64, or FP32 for H and for the
+    # u, v, w, omega outputs under the mixed path
+    cf = f64 if precision == "fp64" else fld
     return {
         "zinv": 5 * fld + 6 * fine,
         "xpass": 6 * fine + 3 * fine,
         "zfwd": 3 * fine + 3 * fld,
-        "cheb_fwd": 3 * fld + 3 * f64,
-        "cheb_inv": 5 * f64 + 5 * fld,
+        "cheb_fwd": 3 * fld + 3 * cf,
+        # H1-H3 and p_v, p_omega in; u, v, w, omega_x, omega_z and p_v, p_omega out
+        "pencil": 3 * cf + 2 * f64 + 5 * cf + 2 * f64,
+        "cheb_inv": 5 * cf + 5 * fld,
     }.get(name)
 
 
@@ -182,6 +187,46 @@ def own_arm(args, rank, world, precision):
     ch.close()
     return dict(ms=ms, launches=launches, clocks=clocks, prof=prof, e2e_s=e2e_s, e2e_steps=e2e_steps,
                 e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw)
+
+
+LES_WORKLOAD = dict(nx=64, ny=97, nz=64, re=4200.0, xl=2 * np.pi, zl=np.pi, dt=0.005, rms=0.1, seed=4)
+
+
+def les_arm(steps, warmup):
+    """RK3 steps/s of the LES configuration 64x97x64 with each SGS model
+    (reported beside the headline; ADM-RT, dynamic Smagorinsky and the learned
+    model as the reference's sgs.i defaults / a fixed weight set)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from sgs_mlp import viscosity_weights
+    from simson_b200.bla import Channel, FP64, MIXED
+    from simson_b200.fields import channel_field
+    w = LES_WORKLOAD
+    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"], kmax=30)
+    out = {}
+    variants = [("no_model_fp64", FP64, None), ("adm_rt_fp64", FP64, "adm"), ("dyn_smagorinsky_fp64", FP64, "dyn"),
+                ("learned_mlp_fp64", FP64, "mlp"), ("learned_mlp_mixed", MIXED, "mlp"), ("no_model_mixed", MIXED, None)]
+    for tag, prec, model in variants:
+        ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], precision=prec)
+        if model == "adm":
+            ch.set_les(iles=1)
+        elif model == "dyn":
+            ch.set_les(iles=2)
+        ch.set_velocity(u, v, wv)
+        ch.prhs()
+        if model == "mlp":
+            ch.set_sgs_mlp(viscosity_weights(1e-5), s_in=0.2)
+        for _ in range(warmup):
+            ch.step(1)
+        ch.sync()
+        ch.record(0)
+        ch.step(steps)
+        ch.record(1)
+        ms = ch.elapsed_ms(0, 1)
+        out[tag] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps}
+        ch.close()
+    return {"workload": "temporal channel 64x97x64, 2pi x 2 x pi, Re_cl 4200, dt 0.005, seeded rms 0.1 "
+                        "broadband perturbation (the LES configuration)", "steps": steps, "warmup": warmup,
+            "variants": out}
 
 
 def dist_barrier(world):
@@ -323,6 +368,8 @@ def main():
         line["mixed_vs_fp64_rel_l2_uvw"] = {"after_steps": args.warmup + args.steps, "u": errs[0], "v": errs[1],
                                             "w": errs[2]}
         line["gpu_launches"] += r64["launches"]
+    if world == 1:
+        line["les"] = les_arm(max(args.steps, 20), max(args.warmup, 3))
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference(1, threads, "bounded sample")

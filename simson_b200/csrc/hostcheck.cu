@@ -112,3 +112,27 @@ extern "C" int sbh_les_yfilter(int nyp, double cutoff, int hpf, const double* in
       Y, hpf != 0, [&](int j) { return double2{in[j], 0.0}; }, Z.data(), 1, [&](int j, double2 x) { out[j] = x.x; });
   return 0;
 }
+
+// The reordered-sum variant of the tau solve used by the mixed path, with the
+// derivative parity sums; dsum[2*q + 0/1] = sum over even / odd j of (D x_q)_j.
+extern "C" void sbh_tau_solve_fast(double lam, int n, int m, const double* f, double* x, const double* bc1,
+                                   const double* bc2, double* cp, double* dsum) {
+  Col F[5], X[5];
+  for (int q = 0; q < m; ++q) {
+    F[q] = Col{const_cast<double*>(f) + (size_t)q * n, 1};
+    X[q] = Col{x + (size_t)q * n, 1};
+  }
+  Col C{cp, 1}, W{nullptr, 1};
+  double ds[5][2] = {};
+  switch (m) {
+    case 1: tau_solve<1, double, double, true>(lam, n, F, X, bc1, bc2, C, W, ds); break;
+    case 2: tau_solve<2, double, double, true>(lam, n, F, X, bc1, bc2, C, W, ds); break;
+    case 3: tau_solve<3, double, double, true>(lam, n, F, X, bc1, bc2, C, W, ds); break;
+    case 4: tau_solve<4, double, double, true>(lam, n, F, X, bc1, bc2, C, W, ds); break;
+    default: tau_solve<5, double, double, true>(lam, n, F, X, bc1, bc2, C, W, ds); break;
+  }
+  for (int q = 0; q < m; ++q) {
+    dsum[2 * q] = ds[q][0];
+    dsum[2 * q + 1] = ds[q][1];
+  }
+}

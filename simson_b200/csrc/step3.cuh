@@ -15,6 +15,8 @@
 // velocity-vorticity recovery and the next partial right-hand side, in the
 // order linearbl.f:257-1860 uses for the channel (ibc = 0, tau).
 #pragma once
+#include <type_traits>
+
 #include "fft.cuh"
 #include "layout.cuh"
 
@@ -98,9 +100,17 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 //   3. forward (rows 3..n): x(i) -= c'(i-2) x(i-2).
 // cp, wt: per-pencil scratch columns (n entries each).  f[q].a == nullptr
 // means a zero right-hand side.
-template <int M, class S = double, class FS = S>
+//
+// FAST (the mixed-precision path): the boundary sums are accumulated during
+// the backward sweep (descending order, W kept in registers, wt unused) and,
+// if dsum != nullptr, the forward sweep also returns the parity sums of the
+// derivative coefficients, dsum[q][0] = sum_{j even} (D x)_j =
+// sum_{k odd} k^2 x_k and dsum[q][1] = sum_{j odd} (D x)_j = sum_{k even}
+// k^2 x_k (D x at y = +-1), so no column of D x is formed.  Two column passes
+// fewer per solution; the same arithmetic in a different summation order.
+template <int M, class S = double, class FS = S, bool FAST = false>
 SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S* bc1, const S* bc2, ColT<S> cp,
-                     ColT<S> wt) {
+                     ColT<S> wt, S (*dsum)[2] = nullptr) {
   // every column is a distinct array: restrict-qualified raw pointers let the
   // loads of a sweep run ahead of its stores
   const FS* __restrict__ fp[M];
@@ -119,8 +129,9 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   S xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
   S q1 = (S)0.0, q2 = (S)0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
   S w1 = (S)0.0, w2 = (S)0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
+  S bs_odd[M], bs_even[M], xn[M], xn1[M];  // FAST: boundary sums, x(n), x(n-1)
 #pragma unroll
-  for (int q = 0; q < M; ++q) xa[q] = xb[q] = (S)0.0;
+  for (int q = 0; q < M; ++q) xa[q] = xb[q] = bs_odd[q] = bs_even[q] = xn[q] = xn1[q] = (S)0.0;
   for (int i = n; i >= 3; --i) {
     S dinv = (S)1.0, cnew = (S)0.0, wnew = (S)0.0;
     if (i <= n - 2) {
@@ -129,7 +140,7 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       cnew = tau_c(m, lam) * dinv;
       cpp[(size_t)(m - 1) * cs] = cnew;
       wnew = (i >= n - 3) ? (S)1.0 - tau_c(i, lam) : (S)1.0 - q2 * w2;
-      wtp[(size_t)(i - 1) * ws] = wnew;
+      if (!FAST) wtp[(size_t)(i - 1) * ws] = wnew;
     }
     const S di = (S)i;
     const S ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
@@ -155,6 +166,16 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       else if (i <= n - 2)
         r = r * dinv;
       xp[q][(size_t)(i - 1) * xs[q]] = r;
+      if (FAST) {
+        if (i == n) xn[q] = r;
+        if (i == n - 1) xn1[q] = r;
+        if (i <= n - 2) {
+          if (i & 1)
+            bs_odd[q] = bs_odd[q] + r * wnew;
+          else
+            bs_even[q] = bs_even[q] + r * wnew;
+        }
+      }
       xb[q] = xa[q];
       xa[q] = r;
     }
@@ -166,6 +187,51 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   // c'(n-3), c'(n-2) are the unscaled c (d = 1 in the truncated rows)
   cpp[(size_t)(n - 4) * cs] = tau_c(n - 3, lam);
   cpp[(size_t)(n - 3) * cs] = tau_c(n - 2, lam);
+  if (FAST) {
+    // after the sweep q1 = c'(1), q2 = c'(2), w1 = W(3), w2 = W(4)
+    const S d1 = (S)1.0 / ((S)1.0 - q1 * w1);
+    const S d2 = (S)1.0 / ((S)1.0 - q2 * w2);
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      S* __restrict__ X = xp[q];
+      const size_t st = xs[q];
+      xa[q] = (bc1[q] - xn[q] - bs_odd[q]) * d1;   // x(1)
+      xb[q] = (bc2[q] - xn1[q] - bs_even[q]) * d2;  // x(2)
+      X[0] = xa[q];
+      X[st] = xb[q];
+    }
+    S ds0[M], ds1[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      ds0[q] = xb[q];  // k = 1 (odd): 1^2 x_1
+      ds1[q] = (S)0.0;
+    }
+#pragma unroll 4
+    for (int i = 3; i <= n; ++i) {
+      const S c = cpp[(size_t)(i - 3) * cs];
+      const S kk = (S)(i - 1) * (S)(i - 1);
+#pragma unroll
+      for (int q = 0; q < M; ++q) {
+        const size_t o = (size_t)(i - 1) * xs[q];
+        const S v = xp[q][o] - c * xa[q];
+        xp[q][o] = v;
+        xa[q] = xb[q];
+        xb[q] = v;
+        if (i & 1)
+          ds1[q] = ds1[q] + kk * v;  // k = i-1 even
+        else
+          ds0[q] = ds0[q] + kk * v;  // k odd
+      }
+    }
+    if (dsum != nullptr) {
+#pragma unroll
+      for (int q = 0; q < M; ++q) {
+        dsum[q][0] = ds0[q];
+        dsum[q][1] = ds1[q];
+      }
+    }
+    return;
+  }
   const S d1 = (S)1.0 / ((S)1.0 - cpp[0] * wtp[2 * ws]);
   const S d2 = (S)1.0 / ((S)1.0 - cpp[cs] * wtp[3 * ws]);
 #pragma unroll
@@ -289,6 +355,10 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   const double k2i = 1.0 / k2;
   const double lam = k2 + 2.0 * re / (rk.an + rk.bn);
   const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
+  // the mixed path (FP32 forcing columns) takes the reordered sums of
+  // tau_solve<..., FAST>; the FP64 path keeps the reference's order
+  constexpr bool FAST = !std::is_same<FC, double>::value;
+  double dsum[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   // this pencil's column of each array; all arrays are distinct
 #define COLP(name) double2* __restrict__ name = B.name + p
   COLP(PV); COLP(PW); COLP(V); COLP(DV);
@@ -346,20 +416,28 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     const ColT<FC> f[5] = {fre(B.FV), fim(B.FV), fre(B.FW), fim(B.FW), ColT<FC>{nullptr, 0}};
     const ColT<SC> x[5] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM), crl(B.PHIH)};
     const SC bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
-    tau_solve<5, SC, FC>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
+    tau_solve<5, SC, FC, FAST>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
     // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
     const ColT<SC> fv[3] = {cre(B.PHI), cim(B.PHI), crl(B.PHIH)};
     const Col xv[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
     const double b0[3] = {0, 0, 0};
-    tau_solve<3, double, SC>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP));
+    tau_solve<3, double, SC, FAST>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
   }
+  double cvr[2], cvi[2];
+  if (FAST) {
+    // parity sums of dv from v itself (returned by the v solve)
+    for (int is = 0; is < 2; ++is) {
+      const double cinv = 1.0 / dsum[2][is];
+      cvr[1 - is] = (0.0 - dsum[0][is]) * cinv;
+      cvi[1 - is] = (0.0 - dsum[1][is]) * cinv;
+    }
+  } else {
   // dv/dy = 0 at the walls: add the homogeneous solution per parity
   // (linearbl.f:1020-1085).  The parity sums of dv run in ascending order as
   // in the reference, so dv and dvh are stored by a backward derivative sweep.
   cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
   cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
   cheb_deriv(col_r(B.DVH, p, NP), col_r(B.VH, p, NP), n);
-  double cvr[2], cvi[2];
   for (int is = 0; is < 2; ++is) {
     double sr = 0.0, si = 0.0, sh = 0.0;
     for (int j = is; j < n; j += 2) {
@@ -371,6 +449,7 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     const double cinv = 1.0 / sh;
     cvr[1 - is] = (0.0 - sr) * cinv;
     cvi[1 - is] = (0.0 - si) * cinv;
+  }
   }
   // One backward sweep for everything after the superposition: the final v,
   // its first and second derivative, phi = D^2 v - k^2 v (tau, linearbl.f:

@@ -10,6 +10,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    config.addinivalue_line("markers", "slow: long GPU run (minutes of device time at most)")
 
 
 def reference_available(nx, ny, nz):

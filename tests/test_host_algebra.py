@@ -108,3 +108,32 @@ def test_fft_passes_match_numpy(n):
         assert host.sbh_fft(n, P(inp), P(out), sign) > 0
         y = out[0::2] + 1j * out[1::2]
         assert np.abs(y - ref).max() <= 1e-15 * n * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n", [17, 65, 193])
+@pytest.mark.parametrize("lam", [0.0, 3.7, 1.6e6, 6.3e6])
+def test_tau_solver_reordered_sums(libs, n, lam):
+    """The mixed path's tau solve (boundary sums accumulated in the backward
+    sweep, derivative parity sums from the solution) against the reference's
+    setmacrhs + trid: the same solution up to the summation order, and the
+    parity sums of D x equal to those of the reference's dcheb."""
+    ref, host = libs
+    host.sbh_tau_solve_fast.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp]
+    rng = np.random.default_rng(7 * n + int(lam))
+    m = 5
+    f = rng.standard_normal((m, n)) * np.exp(-0.1 * np.arange(n))
+    bc1 = rng.standard_normal(m)
+    bc2 = rng.standard_normal(m)
+    xr = ref_tau(ref, lam, f, bc1, bc2)
+    x = np.zeros((m, n))
+    cp = np.zeros(n)
+    ds = np.zeros(2 * m)
+    host.sbh_tau_solve_fast(lam, n, m, P(np.ascontiguousarray(f)), P(x), P(bc1), P(bc2), P(cp), P(ds))
+    scale = np.abs(xr).max(axis=1, keepdims=True)
+    assert np.all(np.abs(x - xr) <= 1e-9 * scale), (np.abs(x - xr) / scale).max()
+    for q in range(m):
+        d = np.zeros(n)
+        ref.f_dcheb(P(d), P(np.ascontiguousarray(xr[q])), I(n), I(1), I(1))
+        dsc = np.abs(d).sum()
+        assert abs(ds[2 * q] - d[0::2].sum()) <= 1e-9 * dsc
+        assert abs(ds[2 * q + 1] - d[1::2].sum()) <= 1e-9 * dsc
