@@ -276,6 +276,7 @@ def main():
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: time FP64 and mixed; value is the mixed-precision step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration timings")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -368,7 +369,7 @@ def main():
         line["mixed_vs_fp64_rel_l2_uvw"] = {"after_steps": args.warmup + args.steps, "u": errs[0], "v": errs[1],
                                             "w": errs[2]}
         line["gpu_launches"] += r64["launches"]
-    if world == 1:
+    if world == 1 and not args.no_les:
         line["les"] = les_arm(max(args.steps, 20), max(args.warmup, 3))
     if world == 1 and not args.no_cpu_baseline:
         try:
