@@ -136,3 +136,35 @@ extern "C" void sbh_tau_solve_fast(double lam, int n, int m, const double* f, do
     dsum[2 * q + 1] = ds[q][1];
   }
 }
+
+// Four interleaved columns (the paired-column passes), FP64 or FP32 (prec 1):
+// in/out complex interleaved, element i of column b at [(i*4 + b)].
+template <class T>
+static int host_fft4(int n, const double* in, double* out, int sign) {
+  typedef typename C2<T>::type V;
+  const FFTPlan plan = fft_make_plan(n);
+  if (plan.npass < 0) return -1;
+  std::vector<V> tw(n), a(4 * (size_t)n), b(4 * (size_t)n);
+  for (int m = 0; m < n; ++m) {
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+    tw[m] = V{(T)cosl(ang), (T)sinl(ang)};
+  }
+  for (size_t i = 0; i < 4 * (size_t)n; ++i) a[i] = V{(T)in[2 * i], (T)in[2 * i + 1]};
+  V* src = a.data();
+  V* dst = b.data();
+  for (int p = 0; p < plan.npass; ++p) {
+    fft_pass<T, 4>(src, dst, plan, p, tw.data(), sign, 0, 1);
+    V* t = src;
+    src = dst;
+    dst = t;
+  }
+  for (size_t i = 0; i < 4 * (size_t)n; ++i) {
+    out[2 * i] = (double)src[i].x;
+    out[2 * i + 1] = (double)src[i].y;
+  }
+  return plan.npass;
+}
+
+extern "C" int sbh_fft4(int n, const double* in, double* out, int sign, int prec) {
+  return prec ? host_fft4<float>(n, in, out, sign) : host_fft4<double>(n, in, out, sign);
+}

@@ -137,3 +137,21 @@ def test_tau_solver_reordered_sums(libs, n, lam):
         dsc = np.abs(d).sum()
         assert abs(ds[2 * q] - d[0::2].sum()) <= 1e-9 * dsc
         assert abs(ds[2 * q + 1] - d[1::2].sum()) <= 1e-9 * dsc
+
+
+@pytest.mark.parametrize("n", [9, 12, 96, 192, 576])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_fft_paired_columns_match_numpy(n, prec):
+    """Four interleaved columns through the paired-column passes (the layout
+    of the CTA tiles), FP64 and FP32, both signs."""
+    host = ctypes.CDLL(sbuild.build_hostcheck())
+    host.sbh_fft4.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int]
+    rng = np.random.default_rng(n + 7 * prec)
+    x = rng.standard_normal((n, 4)) + 1j * rng.standard_normal((n, 4))
+    inp = np.ascontiguousarray(np.stack([x.real, x.imag], -1).ravel())
+    out = np.zeros(2 * 4 * n)
+    tol = (1e-15 if prec == 0 else 2e-6) * n
+    for sign, ref in ((-1, np.fft.fft(x, axis=0)), (1, np.fft.ifft(x, axis=0) * n)):
+        assert host.sbh_fft4(n, P(inp), P(out), sign, prec) > 0
+        y = (out[0::2] + 1j * out[1::2]).reshape(n, 4)
+        assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
