@@ -11,6 +11,7 @@
 // tw[m] = exp(-2 pi i m / n); sign = -1 is the forward (analysis) transform,
 // +1 the backward (synthesis) transform.  No normalisation is applied.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -224,11 +225,37 @@ SB_HD __forceinline__ void stockham_pass(const typename C2<T>::type* __restrict_
     for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * B + b];
     if (jm != 0) {
       const int e = jm * tstep;
+      if constexpr (std::is_same<T, float>::value) {
+        // FP32: two table loads, the other powers by products of depth <= 2
+        // (w^k for k <= 8 from w, w^2: a few ulp), fewer load-pipe requests
+        V w[9];
+        w[1] = tw[e];
+        w[2] = tw[2 * e];
+        if (S > 0) {
+          w[1].y = -w[1].y;
+          w[2].y = -w[2].y;
+        }
+        if (R > 3) {
+          w[3] = cmul(w[1], w[2]);
+          w[4] = cmul(w[2], w[2]);
+        }
+        if (R > 5) {
+          w[5] = cmul(w[1], w[4]);
+          w[6] = cmul(w[3], w[3]);
+        }
+        if (R > 7) {
+          w[7] = cmul(w[3], w[4]);
+          w[8] = cmul(w[4], w[4]);
+        }
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        V w = tw[r * e];
-        if (S > 0) w.y = -w.y;
-        v[r] = cmul(v[r], w);
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+      } else {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          V w = tw[r * e];
+          if (S > 0) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
       }
     }
     dft_small<T, V>(v, R, S);

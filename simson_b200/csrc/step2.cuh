@@ -120,8 +120,10 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
   __syncthreads();
   V* res = fft_columns<T, 3 * RB>(bA, bB, plan, tw, +1);
   V* oth = (res == bA) ? bB : bA;
-  // products in physical space, H into (H1 + i H2, H3 + 0i), CFL
-  const int B2 = 2 * RB;
+  // products in physical space, H into (H1 + i H2) per row and, for an even
+  // number of rows, the H3 of rows 2q and 2q+1 paired as H3 + i H3' (one
+  // complex FFT for two real rows); a single row keeps (H3 + 0i).  CFL.
+  constexpr int B2 = (RB % 2 == 0) ? RB + RB / 2 : 2 * RB;
   double cmax = 0.0;
   const double dy = dyi[y];
   const T r2 = (T)(2.0 * rot);
@@ -151,23 +153,40 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
       ut += mean[0 * g.nyp + y];
       wt += mean[1 * g.nyp + y];
     }
-    oth[j * B2 + 2 * r + 0] = V{h1, h2};
-    oth[j * B2 + 2 * r + 1] = V{h3, (T)0};
+    if constexpr (RB % 2 == 0) {
+      oth[j * B2 + r] = V{h1, h2};
+      T* h3p = reinterpret_cast<T*>(&oth[j * B2 + RB + r / 2]);
+      h3p[r & 1] = h3;
+    } else {
+      oth[j * B2 + 2 * r + 0] = V{h1, h2};
+      oth[j * B2 + 2 * r + 1] = V{h3, (T)0};
+    }
     if (m0 + r < g.nzp) {
       const double cl = fabs(ut) * dxi + fabs((double)v) * dy + fabs(wt) * dzi;
       cmax = fmax(cmax, cl);
     }
   }
   __syncthreads();
-  V* fres = fft_columns<T, 2 * RB>(oth, res, plan, tw, -1);
+  V* fres = fft_columns<T, B2>(oth, res, plan, tw, -1);
   for (int t = threadIdx.x; t < g.nx2 * RB; t += blockDim.x) {
     const int k = t / RB;
     const int r = t - k * RB;
     const int m = m0 + r;
     if (m >= g.nzp) continue;
-    const V a = fres[k * B2 + 2 * r];
-    const V b = fres[((n - k) % n) * B2 + 2 * r];
-    const V h3 = fres[k * B2 + 2 * r + 1];
+    const int kk = (n - k) % n;
+    V a, b, h3;
+    if constexpr (RB % 2 == 0) {
+      a = fres[k * B2 + r];
+      b = fres[kk * B2 + r];
+      // spectra of the real and imaginary rows of the paired H3 column
+      const V c3 = fres[k * B2 + RB + r / 2], d3 = fres[kk * B2 + RB + r / 2];
+      h3 = (r & 1) ? V{(c3.y + d3.y) * (T)0.5, (d3.x - c3.x) * (T)0.5}
+                   : V{(c3.x + d3.x) * (T)0.5, (c3.y - d3.y) * (T)0.5};
+    } else {
+      a = fres[k * B2 + 2 * r];
+      b = fres[kk * B2 + 2 * r];
+      h3 = fres[k * B2 + 2 * r + 1];
+    }
     const V h1 = V{(a.x + b.x) * (T)0.5, (a.y - b.y) * (T)0.5};
     const V h2 = V{(a.y + b.y) * (T)0.5, (b.x - a.x) * (T)0.5};
     const size_t o = ((size_t)y * g.nzp + m) * g.nx2 + k;
