@@ -311,22 +311,27 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
   const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
   const size_t s_y = smem_fft(2 * (g.nyp - 1), c->pb, sizeof(double2));
-  if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024) return fail(SGPU_E_PARAM);
+  const size_t s_zf = smem_fft(g.nzp, sgpu_ctx::kbf, sizeof(float2));
+  const size_t s_xf = smem_fft(g.nxp, 3 * sgpu_ctx::rbf, sizeof(float2));
+  const size_t s_yf = smem_fft(2 * (g.nyp - 1), sgpu_ctx::pbf, sizeof(float2));
+  if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024 || s_zf > 227 * 1024 || s_xf > 227 * 1024 ||
+      s_yf > 227 * 1024)
+    return fail(SGPU_E_PARAM);
   cudaFuncSetAttribute(k_zinv<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
   cudaFuncSetAttribute(k_zfwd<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
   cudaFuncSetAttribute(k_xpass<double, sgpu_ctx::rb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
   cudaFuncSetAttribute(k_cheb<double, sgpu_ctx::pb, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_y);
-  // FP32 variants: twice the columns in the same shared memory
-  cudaFuncSetAttribute(k_zinv<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_xpass<float, sgpu_ctx::rbf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
+  // FP32 variants (their own tiles)
+  cudaFuncSetAttribute(k_zinv<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_zf);
+  cudaFuncSetAttribute(k_zfwd<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_zf);
+  cudaFuncSetAttribute(k_xpass<float, sgpu_ctx::rbf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_xf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)s_y);
+                       (int)s_yf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)s_y);
+                       (int)s_yf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)s_y);
+                       (int)s_yf);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -580,6 +585,8 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
   const size_t s_x = smem_fft(g.nxp, 3 * c->rb, sizeof(double2));
+  const size_t s_zf = smem_fft(g.nzp, sgpu_ctx::kbf, sizeof(float2));
+  const size_t s_xf = smem_fft(g.nxp, 3 * sgpu_ctx::rbf, sizeof(float2));
   unsigned long long* cflp = do_cfl ? c->cfl_bits : nullptr;
   if (c->mixed) {
     // FP32 transforms and products on the FP32 velocity/vorticity fields
@@ -591,13 +598,13 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     // products analytically and their mean-mean product in FP64
     prof_mark(c, K_ZINV);
     k_mean_profiles<float><<<(g.nyp + 127) / 128, 128, 0, c->stream>>>(c->stf, c->meanp, g);
-    k_zinv<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+    k_zinv<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_zf, c->stream>>>(
         c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta, 1);
     prof_mark(c, K_XPASS);
-    k_xpass<float, sgpu_ctx::rbf><<<gxf, sgpu_ctx::fft_threads, s_x, c->stream>>>(
+    k_xpass<float, sgpu_ctx::rbf><<<gxf, sgpu_ctx::fft_threads, s_xf, c->stream>>>(
         zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
     prof_mark(c, K_ZFWD);
-    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_z, c->stream>>>(
+    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_zf, c->stream>>>(
         xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp, P.rot);
     c->launches++;
   } else {
