@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "cheb_tc.cuh"
 #include "les.cuh"
 #include "les_filter.h"
 #include "step3.cuh"
@@ -167,4 +168,18 @@ static int host_fft4(int n, const double* in, double* out, int sign) {
 
 extern "C" int sbh_fft4(int n, const double* in, double* out, int sign, int prec) {
   return prec ? host_fft4<float>(n, in, out, sign) : host_fft4<double>(n, in, out, sign);
+}
+
+// The tensor-core Chebyshev matrix image decoded back to row-major hi and lo
+// parts (n x n each), for the CPU check of its layout and accuracy.
+extern "C" int sbh_chb_matrix(int n, int inverse, double scale, float* hi, float* lo) {
+  std::vector<unsigned char> img;
+  chb_build_matrix(n, inverse, scale, img);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) {
+      const unsigned char* base = img.data() + (size_t)(c / CHB_KC) * CHB_CHUNK_BYTES;
+      memcpy(&hi[(size_t)r * n + c], base + chb_canon(r, c % CHB_KC), 4);
+      memcpy(&lo[(size_t)r * n + c], base + CHB_A_BYTES + chb_canon(r, c % CHB_KC), 4);
+    }
+  return (int)(img.size() / CHB_CHUNK_BYTES);
 }

@@ -20,6 +20,7 @@
 #include "les_filter.h"
 #include "les_dyn.cuh"
 #include "sgs_mlp.cuh"
+#include "cheb_tc.cuh"
 
 using namespace sb;
 
@@ -83,6 +84,10 @@ struct sgpu_ctx {
   double* mlp_tau = nullptr;  // [6][nyp][nz][nx] physical tau
   int* mlp_err = nullptr;
   float mlp_s_in = 1.f, mlp_s_y = 1.f, mlp_s_out = 1.f;
+  // mixed path: Chebyshev transform matrices for the tensor cores (cheb_tc.cuh)
+  unsigned char* chb_fwd = nullptr;  // forward, scale 1/(nxp nzp)
+  unsigned char* chb_inv = nullptr;  // inverse
+  int* chb_err = nullptr;
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   Tw sgs_twz, sgs_twx;  // lengths nz and nx (iles = 2)
@@ -283,6 +288,20 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   if (c->mixed && (cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess ||
                    cudaMalloc(&c->meanp, 4 * (size_t)g.nyp * sizeof(double)) != cudaSuccess))
     return fail(SGPU_E_CUDA);
+  if (c->mixed && g.nyp <= CHB_MROWS) {
+    // the step's two Chebyshev transforms as tensor-core GEMMs (up to
+    // CHB_MROWS points in y; larger grids keep the FFT transforms)
+    std::vector<unsigned char> mf, mi;
+    chb_build_matrix(g.nyp, 0, 1.0 / ((double)g.nxp * (double)g.nzp), mf);
+    chb_build_matrix(g.nyp, 1, 1.0, mi);
+    if (cudaMalloc(&c->chb_fwd, mf.size()) != cudaSuccess || cudaMalloc(&c->chb_inv, mi.size()) != cudaSuccess ||
+        cudaMalloc(&c->chb_err, sizeof(int)) != cudaSuccess)
+      return fail(SGPU_E_CUDA);
+    cudaMemcpy(c->chb_fwd, mf.data(), mf.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->chb_inv, mi.data(), mi.size(), cudaMemcpyHostToDevice);
+    cudaMemset(c->chb_err, 0, sizeof(int));
+    cudaFuncSetAttribute(k_cheb_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CHB_SMEM);
+  }
   cudaMemset(c->st, 0, 7 * fld * sizeof(double2));
   cudaMemset(c->puw, 0, 2 * g.ny * sizeof(double));
   // wavenumbers (bla/preprbl.f:36-43) and CFL grid spacing (bla/boxcfl.f:25-56)
@@ -344,7 +363,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->mlp_image, c->mlp_tau,
-                  c->mlp_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+                  c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -422,11 +441,38 @@ static void launch_cheb_t(sgpu_ctx* c, const typename C2<SI>::type* in, size_t i
 
 // Chebyshev transform of nfields y-pencil fields.  Physical-y fields live in
 // the state (FP64, or FP32 under SGPU_MIXED); Chebyshev-y fields are FP64.
+// Mixed path: the FP32 transforms as a 3xTF32 tensor-core GEMM over all
+// pencils (cheb_tc.cuh); fields are float2 arrays seen as 2 NP float columns.
+static void launch_cheb_tc(sgpu_ctx* c, const float2* in, size_t in_fs, float2* out, size_t out_fs, int nfields,
+                           const unsigned char* mat, int skip_oddball) {
+  const Dims& g = c->g;
+  ChebTCArgs A{};
+  A.in = reinterpret_cast<const float*>(in);
+  A.in_fs = 2 * in_fs;
+  A.out = reinterpret_cast<float*>(out);
+  A.out_fs = 2 * out_fs;
+  A.ncol = 2 * g.NP;
+  A.n = g.nyp;
+  A.nchunks = (g.nyp + CHB_KC - 1) / CHB_KC;
+  A.mat = mat;
+  A.skip_oddball = skip_oddball;
+  A.nx2 = g.nx2;
+  A.zodd = g.zodd;
+  A.err = c->chb_err;
+  dim3 grid((A.ncol + CHB_TILE - 1) / CHB_TILE, nfields);
+  k_cheb_tc<<<grid, 256, CHB_SMEM, c->stream>>>(A);
+  c->launches++;
+}
+
 static void cheb_to_spec(sgpu_ctx* c, int slot0, double2* out, int nfields, double scale) {
   const size_t fld = (size_t)c->g.nyp * c->g.NP;
-  if (c->mixed)  // FP32 Chebyshev coefficients of H (the pencil kernel reads them as float2)
+  const double step_scale = 1.0 / ((double)c->g.nxp * (double)c->g.nzp);
+  if (c->mixed && c->chb_fwd && scale == step_scale)  // FP32 Chebyshev coefficients of H (read as float2)
     // the output fields sit where the FP64 scratch fields would (stride fld
-    // double2 = 2*fld float2), so the pencil kernel addresses them as usual
+    // double2 = 2*fld float2), so the pencil kernel addresses them as usual;
+    // the prepared matrix carries the step's scale 1/(nxp nzp)
+    launch_cheb_tc(c, c->stf + slot0 * fld, fld, reinterpret_cast<float2*>(out), 2 * fld, nfields, c->chb_fwd, 0);
+  else if (c->mixed)
     launch_cheb_t<float, sgpu_ctx::pbf, float, float>(c, c->stf + slot0 * fld, fld, reinterpret_cast<float2*>(out),
                                                       2 * fld, nfields, 0, scale, 0, c->twy.f);
   else
@@ -437,7 +483,10 @@ static void cheb_to_spec(sgpu_ctx* c, int slot0, double2* out, int nfields, doub
 static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields, int skip_oddball,
                          bool fp32_input = false) {
   const size_t fld = (size_t)c->g.nyp * c->g.NP;
-  if (c->mixed && fp32_input)
+  if (c->mixed && fp32_input && c->chb_inv)
+    launch_cheb_tc(c, reinterpret_cast<const float2*>(in), 2 * fld, c->stf + slot0 * fld, fld, nfields, c->chb_inv,
+                   skip_oddball);
+  else if (c->mixed && fp32_input)
     launch_cheb_t<float, sgpu_ctx::pbf, float, float>(c, reinterpret_cast<const float2*>(in), 2 * fld,
                                                       c->stf + slot0 * fld, fld, nfields, 1, 1.0, skip_oddball,
                                                       c->twy.f);
@@ -743,10 +792,16 @@ extern "C" int sgpu_get_scalars(sgpu_ctx* c, double* out, int n) {
   if (!c || !out) return SGPU_E_PARAM;
   int r = collect_cfl(c);
   double sc[4];
+  int tc_err = 0;
   CK(cudaMemcpyAsync(sc, c->scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+  if (c->chb_err) CK(cudaMemcpyAsync(&tc_err, c->chb_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const double v[12] = {sc[0], sc[1], c->t, c->cfl, c->an, c->bn, c->anp1, c->bnp1, c->cnp1, (double)c->it, c->tc, c->dtn};
   for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
+  if (tc_err) {
+    fprintf(stderr, "simson_b200: tensor-core Chebyshev transform: a wait timed out\n");
+    return SGPU_E_CUDA;
+  }
   return r;
 }
 

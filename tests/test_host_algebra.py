@@ -155,3 +155,32 @@ def test_fft_paired_columns_match_numpy(n, prec):
         assert host.sbh_fft4(n, P(inp), P(out), sign, prec) > 0
         y = (out[0::2] + 1j * out[1::2]).reshape(n, 4)
         assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n", [17, 65, 193])
+def test_tensor_core_chebyshev_matrix(n):
+    """The 3xTF32 matrices of the mixed path's tensor-core Chebyshev
+    transforms: decoded from their tile layout, hi + lo is the exact DCT-I
+    matrix to ~2^-22, hi and lo are TF32 values (13 low bits zero), and
+    forward then inverse is the identity."""
+    host = ctypes.CDLL(sbuild.build_hostcheck())
+    fp = ctypes.POINTER(ctypes.c_float)
+    host.sbh_chb_matrix.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, fp, fp]
+    N = n - 1
+    j = np.arange(n)
+    cosm = np.cos(np.pi * np.outer(j, j) / N)
+    w = np.where((j == 0) | (j == N), 1.0, 2.0)
+    cb = np.where((j == 0) | (j == N), 2.0, 1.0)
+    scale = 1.0 / 3.0
+    exact = {0: scale * cosm * w[None, :] / (N * cb[:, None]), 1: cosm}
+    mats = {}
+    for inv in (0, 1):
+        hi = np.zeros((n, n), np.float32)
+        lo = np.zeros((n, n), np.float32)
+        host.sbh_chb_matrix(n, inv, scale if inv == 0 else 1.0, hi.ctypes.data_as(fp), lo.ctypes.data_as(fp))
+        for part in (hi, lo):
+            assert np.all(part.view(np.uint32) & 0x1FFF == 0)
+        m = hi.astype(np.float64) + lo.astype(np.float64)
+        assert np.abs(m - exact[inv]).max() <= 2.0 ** -21 * np.abs(exact[inv]).max()
+        mats[inv] = m
+    np.testing.assert_allclose(mats[1] @ mats[0], scale * np.eye(n), atol=1e-5 * scale)
