@@ -85,25 +85,39 @@ __device__ __forceinline__ void chb_bulk_load(unsigned dst, const void* src, uns
                : "memory");
 }
 
-// Input chunk q (rows q*KC .. +KC of columns c0 .. c0+127) split into hi/lo
-// TF32 tiles; each thread stores two 16-byte groups of four rows.
-__device__ __forceinline__ void chb_stage_input(const ChebTCArgs& a, const float* __restrict__ in, int c0, int q,
-                                                unsigned char* Bhi, unsigned char* Blo) {
-  for (int it = threadIdx.x; it < CHB_TILE * (CHB_KC / 4); it += blockDim.x) {
+// Input chunk q (rows q*KC .. +KC of columns c0 .. c0+127): each thread
+// loads CHB_ITEMS groups of four rows of one column into registers, and later
+// stores them split into hi/lo TF32 (one 16-byte store per group and part).
+constexpr int CHB_ITEMS = CHB_TILE * (CHB_KC / 4) / 256;
+
+__device__ __forceinline__ void chb_load_input(const ChebTCArgs& a, const float* __restrict__ in, int c0, int q,
+                                               float (&x)[CHB_ITEMS][4]) {
+#pragma unroll
+  for (int k = 0; k < CHB_ITEMS; ++k) {
+    const int it = threadIdx.x + 256 * k;
     const int r = it % CHB_TILE;
     const int g4 = it / CHB_TILE;
     const int col = c0 + r;
-    float x[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int row = q * CHB_KC + 4 * g4 + i;
-      x[i] = (row < a.n && col < a.ncol) ? in[(size_t)row * a.ncol + col] : 0.f;
+      x[k][i] = (row < a.n && col < a.ncol) ? in[(size_t)row * a.ncol + col] : 0.f;
     }
+  }
+}
+
+__device__ __forceinline__ void chb_store_input(const float (&x)[CHB_ITEMS][4], unsigned char* Bhi,
+                                                unsigned char* Blo) {
+#pragma unroll
+  for (int k = 0; k < CHB_ITEMS; ++k) {
+    const int it = threadIdx.x + 256 * k;
+    const int r = it % CHB_TILE;
+    const int g4 = it / CHB_TILE;
     float4 hi, lo;
-    hi.x = to_tf32(x[0]); lo.x = to_tf32(x[0] - hi.x);
-    hi.y = to_tf32(x[1]); lo.y = to_tf32(x[1] - hi.y);
-    hi.z = to_tf32(x[2]); lo.z = to_tf32(x[2] - hi.z);
-    hi.w = to_tf32(x[3]); lo.w = to_tf32(x[3] - hi.w);
+    hi.x = to_tf32(x[k][0]); lo.x = to_tf32(x[k][0] - hi.x);
+    hi.y = to_tf32(x[k][1]); lo.y = to_tf32(x[k][1] - hi.y);
+    hi.z = to_tf32(x[k][2]); lo.z = to_tf32(x[k][2] - hi.z);
+    hi.w = to_tf32(x[k][3]); lo.w = to_tf32(x[k][3] - hi.w);
     *reinterpret_cast<float4*>(Bhi + chb_canon(r, 4 * g4)) = hi;
     *reinterpret_cast<float4*>(Blo + chb_canon(r, 4 * g4)) = lo;
   }
@@ -143,9 +157,12 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   constexpr unsigned IDESC = chb_idesc(CHB_TILE, CHB_MROWS);
   const int nch = a.nchunks;
   auto par = [](int c) { return (unsigned)((c >> 1) & 1); };
-  // chunk 0 into stage 0
+  // chunk 0 into stage 0; chunk 1's input into registers
+  float xr[CHB_ITEMS][4];
   if (t == 0) chb_bulk_load(smem_u32(Mhi(0)), a.mat, CHB_CHUNK_BYTES, full0);
-  chb_stage_input(a, in, c0, 0, Dhi(0), Dlo(0));
+  chb_load_input(a, in, c0, 0, xr);
+  chb_store_input(xr, Dhi(0), Dlo(0));
+  if (nch > 1) chb_load_input(a, in, c0, 1, xr);
   int last = -1;  // last committed chunk
   for (int q = 0; q < nch; ++q) {
     const int s = q & 1;
@@ -178,7 +195,10 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
       tc_fence_after();
       if (t == 0)
         chb_bulk_load(smem_u32(Mhi(s ^ 1)), a.mat + (size_t)(q + 1) * CHB_CHUNK_BYTES, CHB_CHUNK_BYTES, full0 + 8 * (s ^ 1));
-      chb_stage_input(a, in, c0, q + 1, Dhi(s ^ 1), Dlo(s ^ 1));
+      // chunk q+1's input (loaded an iteration ago) into the free stage, then
+      // the loads of chunk q+2 stay in flight until the next iteration
+      chb_store_input(xr, Dhi(s ^ 1), Dlo(s ^ 1));
+      if (q + 2 < nch) chb_load_input(a, in, c0, q + 2, xr);
     }
   }
   // all MMAs of the tile (they complete in order): the last chunk's barrier
