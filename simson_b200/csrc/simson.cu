@@ -101,7 +101,7 @@ struct sgpu_ctx {
   // threads per CTA of the FFT kernels (measured on B200: 256 everywhere but
   // the FP64 x-pass, whose register use prefers 128)
   static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 256, xpass64_threads = 128;
-  static constexpr int kbf = 8, rbf = 2, pbf = 8;  // FP32 tiles (same shared memory as FP64)
+  static constexpr int kbf = 4, rbf = 2, pbf = 8;  // FP32 tiles (measured: 4 z-columns beat 8)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
   std::vector<cudaEvent_t> pev;
