@@ -132,7 +132,17 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   S bs_odd[M], bs_even[M], xn[M], xn1[M];  // FAST: boundary sums, x(n), x(n-1)
 #pragma unroll
   for (int q = 0; q < M; ++q) xa[q] = xb[q] = bs_odd[q] = bs_even[q] = xn[q] = xn1[q] = (S)0.0;
+  // right-hand-side window: row i reads f(i-3), f(i-1), f(i+1) (0-based);
+  // per row parity the last two stay in registers, so each row loads one
+  // value per column (row i-2 reuses f(i-1) and f(i-3)). Used by the FP64
+  // path; in the reordered (FAST) variant the extra registers spill and the
+  // plain three loads are faster.
+  constexpr bool WIN = !FAST;
+  S wlo0[M], whi0[M], wlo1[M], whi1[M];  // even / odd rows (selects keep them in registers)
+#pragma unroll
+  for (int q = 0; q < M; ++q) wlo0[q] = wlo1[q] = whi0[q] = whi1[q] = (S)0.0;
   for (int i = n; i >= 3; --i) {
+    const int pr = i & 1;
     S dinv = (S)1.0, cnew = (S)0.0, wnew = (S)0.0;
     if (i <= n - 2) {
       const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
@@ -150,7 +160,25 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       S r = (S)0.0;
-      if (fp[q] != nullptr) {
+      if (fp[q] != nullptr && WIN) {
+        const S fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];  // f(i-3)
+        const S fm = pr ? wlo1[q] : wlo0[q];               // f(i-1)
+        const S fpl = pr ? whi1[q] : whi0[q];              // f(i+1)
+        if (i == 3) {
+          r = (S)0.25 * fnew + fpl / (S)24.0 - fm / (S)6.0;
+        } else {
+          r = ca * fnew;
+          if (i <= n - 2) r += cb * fm;
+          if (i <= n - 4) r += cc * fpl;
+        }
+        if (pr) {
+          whi1[q] = fm;
+          wlo1[q] = fnew;
+        } else {
+          whi0[q] = fm;
+          wlo0[q] = fnew;
+        }
+      } else if (fp[q] != nullptr) {
         const FS* __restrict__ F = fp[q];
         const size_t st = fs[q];
         if (i == 3) {
