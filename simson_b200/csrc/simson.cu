@@ -259,7 +259,13 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   auto fail = [&](int r) { sgpu_finalize(c); return r; };
   if (cudaSetDevice(P.device) != cudaSuccess) return fail(SGPU_E_CUDA);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(SGPU_E_CUDA);
-  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) return fail(SGPU_E_CUDA);
+  // the mean-flow block goes on a high-priority stream: launched at the same
+  // time as the pencil grid (one full wave), it must be placed first, or it
+  // waits for the whole wave to retire and the overlap is lost
+  int prio_lo = 0, prio_hi = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) return fail(SGPU_E_CUDA);
+  if (cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess)
+    return fail(SGPU_E_CUDA);
   if (cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess)
     return fail(SGPU_E_CUDA);

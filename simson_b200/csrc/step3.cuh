@@ -34,6 +34,20 @@ struct ColT {
 };
 typedef ColT<double> Col;
 
+// L2 prefetch of a row a few iterations ahead of a sweep: the sweeps are
+// serial in y, so without it each row's loads wait a full DRAM latency.
+// The prefetch holds no register; callers pass in-range addresses only.
+#ifndef SB_PF_ROWS
+#define SB_PF_ROWS 3
+#endif
+SB_HD __forceinline__ void pf_l2(const void* ptr) {
+#ifdef __CUDA_ARCH__
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(ptr)));
+#else
+  (void)ptr;
+#endif
+}
+
 __device__ __forceinline__ Col col_re(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p, 2 * (size_t)NP}; }
 __device__ __forceinline__ Col col_im(double2* arr, int p, int NP) { return Col{reinterpret_cast<double*>(arr) + 2 * (size_t)p + 1, 2 * (size_t)NP}; }
 __device__ __forceinline__ Col col_r(double* arr, int p, int NP) { return Col{arr + p, (size_t)NP}; }
@@ -51,6 +65,7 @@ SB_HD inline void cheb_deriv(Col b, Col a, int n) {
   bp[(size_t)(n - 3) * sb] = bp1;
 #pragma unroll 8
   for (int j = n - 4; j >= 0; --j) {
+    if (j + 1 - SB_PF_ROWS >= 0) pf_l2(ap + (size_t)(j + 1 - SB_PF_ROWS) * sa);
     const double v = bp2 + 2.0 * (double)(j + 1) * ap[(size_t)(j + 1) * sa];
     bp2 = bp1;
     bp1 = v;
@@ -160,6 +175,7 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       S r = (S)0.0;
+      if (fp[q] != nullptr && i - 3 - SB_PF_ROWS >= 0) pf_l2(fp[q] + (size_t)(i - 3 - SB_PF_ROWS) * fs[q]);
       if (fp[q] != nullptr && WIN) {
         const S fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];  // f(i-3)
         const S fm = pr ? wlo1[q] : wlo0[q];               // f(i-1)
@@ -236,11 +252,13 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     }
 #pragma unroll 4
     for (int i = 3; i <= n; ++i) {
+      if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(cpp + (size_t)(i - 3 + SB_PF_ROWS) * cs);
       const S c = cpp[(size_t)(i - 3) * cs];
       const S kk = (S)(i - 1) * (S)(i - 1);
 #pragma unroll
       for (int q = 0; q < M; ++q) {
         const size_t o = (size_t)(i - 1) * xs[q];
+        if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(xp[q] + o + (size_t)SB_PF_ROWS * xs[q]);
         const S v = xp[q][o] - c * xa[q];
         xp[q][o] = v;
         xa[q] = xb[q];
@@ -279,10 +297,12 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   }
 #pragma unroll 4
   for (int i = 3; i <= n; ++i) {
+    if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(cpp + (size_t)(i - 3 + SB_PF_ROWS) * cs);
     const S c = cpp[(size_t)(i - 3) * cs];
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       const size_t o = (size_t)(i - 1) * xs[q];
+      if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(xp[q] + o + (size_t)SB_PF_ROWS * xs[q]);
       const S v = xp[q][o] - c * xa[q];
       xp[q][o] = v;
       xa[q] = xb[q];
@@ -411,6 +431,10 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
     for (int j = n - 1; j >= 0; --j) {
       const size_t o = j * NP;
+      if (j >= SB_PF_ROWS) {
+        const size_t op = o - (size_t)SB_PF_ROWS * NP;
+        pf_l2(H1 + op); pf_l2(H2 + op); pf_l2(H3 + op); pf_l2(PV + op); pf_l2(PW + op);
+      }
       const IO h1i = H1[o], h2i = H2[o], h3i = H3[o];
       const double2 h1 = {(double)h1i.x, (double)h1i.y}, h2 = {(double)h2i.x, (double)h2i.y};
       const double2 h3 = {(double)h3i.x, (double)h3i.y};
@@ -508,6 +532,10 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     };
     for (int j = n - 1; j >= 0; --j) {
       const size_t o = j * NP;
+      if (j >= SB_PF_ROWS) {
+        const size_t op = o - (size_t)SB_PF_ROWS * NP;
+        pf_l2(VH + op); pf_l2(V + op); pf_l2(OM + op); pf_l2(HV + op); pf_l2(HOM + op);
+      }
       const double vh = VH[o];
       const double2 vp = V[o];
       const double2 v = double2{vp.x + cvr[j & 1] * vh, vp.y + cvi[j & 1] * vh};
