@@ -206,6 +206,44 @@ SB_HD __forceinline__ unsigned umulhi_(unsigned a, unsigned b) {
 #endif
 }
 
+// v[r] *= w^(r e), w = exp(S 2 pi i / n), from the table tw[m] = exp(-2 pi i m / n).
+template <class T, int R, int S>
+SB_HD __forceinline__ void twiddle(typename C2<T>::type* v, const typename C2<T>::type* __restrict__ tw, int e) {
+  typedef typename C2<T>::type V;
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32: two table loads, the other powers by products of depth <= 2
+    // (w^k for k <= 8 from w, w^2: a few ulp), fewer load-pipe requests
+    V w[9];
+    w[1] = tw[e];
+    w[2] = tw[2 * e];
+    if (S > 0) {
+      w[1].y = -w[1].y;
+      w[2].y = -w[2].y;
+    }
+    if (R > 3) {
+      w[3] = cmul(w[1], w[2]);
+      w[4] = cmul(w[2], w[2]);
+    }
+    if (R > 5) {
+      w[5] = cmul(w[1], w[4]);
+      w[6] = cmul(w[3], w[3]);
+    }
+    if (R > 7) {
+      w[7] = cmul(w[3], w[4]);
+      w[8] = cmul(w[4], w[4]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      V w = tw[r * e];
+      if (S > 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+  }
+}
+
 // S: transform sign (compile time), so the twiddle conjugation and the
 // +-i rotations of the small DFTs fold into the arithmetic.
 template <class T, int B, int R, int S>
@@ -223,41 +261,7 @@ SB_HD __forceinline__ void stockham_pass(const typename C2<T>::type* __restrict_
     V v[9];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * B + b];
-    if (jm != 0) {
-      const int e = jm * tstep;
-      if constexpr (std::is_same<T, float>::value) {
-        // FP32: two table loads, the other powers by products of depth <= 2
-        // (w^k for k <= 8 from w, w^2: a few ulp), fewer load-pipe requests
-        V w[9];
-        w[1] = tw[e];
-        w[2] = tw[2 * e];
-        if (S > 0) {
-          w[1].y = -w[1].y;
-          w[2].y = -w[2].y;
-        }
-        if (R > 3) {
-          w[3] = cmul(w[1], w[2]);
-          w[4] = cmul(w[2], w[2]);
-        }
-        if (R > 5) {
-          w[5] = cmul(w[1], w[4]);
-          w[6] = cmul(w[3], w[3]);
-        }
-        if (R > 7) {
-          w[7] = cmul(w[3], w[4]);
-          w[8] = cmul(w[4], w[4]);
-        }
-#pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
-      } else {
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-          V w = tw[r * e];
-          if (S > 0) w.y = -w.y;
-          v[r] = cmul(v[r], w);
-        }
-      }
-    }
+    if (jm != 0) twiddle<T, R, S>(v, tw, jm * tstep);
     dft_small<T, V>(v, R, S);
     const int base = jg * Ns * R + jm;
 #pragma unroll
@@ -347,6 +351,105 @@ inline FFTPlan fft_make_plan(int n) {
     ns *= p.radix[i];
   }
   return p;
+}
+
+// ---------------------------------------------------------------------------
+// Compile-time plans.  For the transform lengths of the production grids the
+// length N, the radix sequence, every Ns and the thread count NT are template
+// constants: the element addresses of a pass become one base register plus
+// immediate offsets, the index divisions become multiplies by constants, and
+// the work-item loop has a known trip count.  Same radix order, twiddles and
+// butterflies as the runtime plan above.
+// ---------------------------------------------------------------------------
+struct CPlanData {
+  int npass;
+  int radix[12];
+  int ns[12];
+};
+
+constexpr CPlanData cplan_make(int n) {
+  CPlanData p{};
+  int m = n, k = 0;
+  const int order[7] = {9, 8, 6, 4, 2, 3, 5};
+  for (int oi = 0; oi < 7; ++oi)
+    while (m % order[oi] == 0 && k < 12) {
+      p.radix[k++] = order[oi];
+      m /= order[oi];
+    }
+  p.npass = (m == 1) ? k : -1;
+  int ns = 1;
+  for (int i = 0; i < k; ++i) {
+    p.ns[i] = ns;
+    ns *= p.radix[i];
+  }
+  return p;
+}
+
+// largest number of butterflies of one column in any pass (n / smallest radix)
+constexpr int cplan_max_nb(int n) {
+  const CPlanData p = cplan_make(n);
+  int mx = 0;
+  for (int i = 0; i < p.npass; ++i) mx = (n / p.radix[i] > mx) ? n / p.radix[i] : mx;
+  return mx;
+}
+
+// One radix-R pass of an N-point transform over B interleaved columns; work
+// items t0, t0 + NT, ...
+template <class T, int B, int N, int R, int NS, int S, int NT>
+SB_HD __forceinline__ void cpass(const typename C2<T>::type* __restrict__ src, typename C2<T>::type* __restrict__ dst,
+                                 const typename C2<T>::type* __restrict__ tw, int t0) {
+  typedef typename C2<T>::type V;
+  constexpr int nb = N / R;
+  constexpr int items = nb * B;
+  constexpr int tstep = N / (NS * R);
+  constexpr int iters = (items + NT - 1) / NT;
+#pragma unroll
+  for (int it = 0; it < iters; ++it) {
+    const int t = t0 + it * NT;
+    if (items % NT != 0 && t >= items) break;
+    const unsigned j = (unsigned)t / B;
+    const unsigned b = (unsigned)t - j * B;
+    const unsigned jg = j / NS;
+    const unsigned jm = j - jg * NS;
+    V v[9];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[t + r * nb * B];
+    if (NS > 1 && jm != 0) twiddle<T, R, S>(v, tw, (int)(jm * tstep));
+    dft_small<T, V>(v, R, S);
+    V* __restrict__ d = dst + (size_t)((jg * NS * R + jm) * B + b);
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[r * NS * B] = v[r];
+  }
+}
+
+// All passes of the N-point transform of the B columns in src (dst is
+// scratch); returns the buffer holding the result.  On the device every pass
+// ends with a barrier (the caller syncs before the first).
+template <class T, int B, int N, int S, int NT, int P = 0>
+SB_HD __forceinline__ typename C2<T>::type* cfft(typename C2<T>::type* src, typename C2<T>::type* dst,
+                                                 const typename C2<T>::type* __restrict__ tw, int t0) {
+  constexpr CPlanData pl = cplan_make(N);
+  static_assert(pl.npass > 0, "transform length must factor into 2, 3, 5");
+  if constexpr (P >= pl.npass) {
+    return src;
+  } else {
+    cpass<T, B, N, pl.radix[P], pl.ns[P], S, NT>(src, dst, tw, t0);
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+#endif
+    return cfft<T, B, N, S, NT, P + 1>(dst, src, tw, t0);
+  }
+}
+
+// runtime plan (N == 0) or compile-time plan, same interface
+template <class T, int B, int N, int NT, int S>
+__device__ __forceinline__ typename C2<T>::type* fft_any(typename C2<T>::type* buf0, typename C2<T>::type* buf1,
+                                                        const FFTPlan& plan,
+                                                        const typename C2<T>::type* __restrict__ tw) {
+  if constexpr (N == 0)
+    return fft_columns_s<T, B, S>(buf0, buf1, plan, tw);
+  else
+    return cfft<T, B, N, S, NT>(buf0, buf1, tw, threadIdx.x);
 }
 
 }  // namespace sb

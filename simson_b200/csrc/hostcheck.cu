@@ -170,6 +170,46 @@ extern "C" int sbh_fft4(int n, const double* in, double* out, int sign, int prec
   return prec ? host_fft4<float>(n, in, out, sign) : host_fft4<double>(n, in, out, sign);
 }
 
+// The compile-time plan (cfft) of the fixed transform lengths over B = 3, 4
+// or 6 interleaved columns, sequentially on the host; in/out as sbh_fft4.
+template <class T, int B, int N>
+static int host_cfft(const double* in, double* out, int sign) {
+  typedef typename C2<T>::type V;
+  std::vector<V> tw(N), a(B * (size_t)N), b(B * (size_t)N);
+  for (int m = 0; m < N; ++m) {
+    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)N;
+    tw[m] = V{(T)cosl(ang), (T)sinl(ang)};
+  }
+  for (size_t i = 0; i < B * (size_t)N; ++i) a[i] = V{(T)in[2 * i], (T)in[2 * i + 1]};
+  V* res = sign > 0 ? cfft<T, B, N, 1, 1>(a.data(), b.data(), tw.data(), 0)
+                    : cfft<T, B, N, -1, 1>(a.data(), b.data(), tw.data(), 0);
+  for (size_t i = 0; i < B * (size_t)N; ++i) {
+    out[2 * i] = (double)res[i].x;
+    out[2 * i + 1] = (double)res[i].y;
+  }
+  return cplan_make(N).npass;
+}
+
+template <class T, int N>
+static int host_cfft_b(int cols, const double* in, double* out, int sign) {
+  switch (cols) {
+    case 3: return host_cfft<T, 3, N>(in, out, sign);
+    case 4: return host_cfft<T, 4, N>(in, out, sign);
+    case 6: return host_cfft<T, 6, N>(in, out, sign);
+    default: return -1;
+  }
+}
+
+extern "C" int sbh_cfft(int n, int cols, const double* in, double* out, int sign, int prec) {
+  switch (n) {
+#define SB_CASE(N) \
+  case N: return prec ? host_cfft_b<float, N>(cols, in, out, sign) : host_cfft_b<double, N>(cols, in, out, sign);
+    SB_CASE(72) SB_CASE(96) SB_CASE(240) SB_CASE(288) SB_CASE(576)
+#undef SB_CASE
+    default: return -1;
+  }
+}
+
 // The tensor-core Chebyshev matrix image decoded back to row-major hi and lo
 // parts (n x n each), for the CPU check of its layout and accuracy.
 extern "C" int sbh_chb_matrix(int n, int inverse, double scale, float* hi, float* lo) {

@@ -342,21 +342,21 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   if (s_z > 227 * 1024 || s_x > 227 * 1024 || s_y > 227 * 1024 || s_zf > 227 * 1024 || s_xf > 227 * 1024 ||
       s_yf > 227 * 1024)
     return fail(SGPU_E_PARAM);
-  cudaFuncSetAttribute(k_zinv<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<double, sgpu_ctx::kb, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_xpass<double, sgpu_ctx::rb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
   cudaFuncSetAttribute(k_cheb<double, sgpu_ctx::pb, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_y);
   // FP32 variants (their own tiles)
-  cudaFuncSetAttribute(k_zinv<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_zf);
-  cudaFuncSetAttribute(k_zfwd<float, sgpu_ctx::kbf, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_zf);
-  cudaFuncSetAttribute(k_xpass<float, sgpu_ctx::rbf>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_xf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
+  // The pencil grid fills every SM and uses no shared memory; with the
+  // default carveout its SMs hold no room for the concurrent mean-flow block
+  // (12 columns of nyp doubles in shared memory), which then starts only when
+  // the pencil wave retires.  Keep a shared-memory carveout beside it.
+  cudaFuncSetAttribute(k_pencil<float2, double, float>, cudaFuncAttributePreferredSharedMemoryCarveout, 25);
+  cudaFuncSetAttribute(k_pencil<double2, double, double>, cudaFuncAttributePreferredSharedMemoryCarveout, 25);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -622,6 +622,92 @@ static void enqueue_sgs(sgpu_ctx* c) {
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 6), fld, c->les_gu, fld, 3, 1, 1.0, 0, c->twy.d);
 }
 
+// Transform lengths with compile-time FFT plans (fft.cuh cfft): the
+// production grid's 576 (3/2 x 384) and the test, LES and channel grids' 3/2
+// lengths; any other length takes the runtime plan.
+#define SB_FIXED_LENGTHS(X) X(72) X(96) X(240) X(288) X(576)
+
+// threads per CTA for B columns of an N-point compile-time transform: one
+// butterfly per thread in the widest pass (halved while above 512), a
+// multiple of 32
+constexpr int fixed_threads(int n, int b) {
+  int items = cplan_max_nb(n) * b;
+  while (items > 512) items = (items + 1) / 2;
+  return ((items + 31) / 32) * 32;
+}
+
+template <class T, int KB, class S, int N, int NT>
+static void zinv_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<S>::type* in,
+                   typename C2<T>::type* zb, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
+                   const double* alfa, const double* beta, int drop) {
+  cudaFuncSetAttribute(k_zinv<T, KB, S, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zinv<T, KB, S, N, NT><<<grid, NT, smem, st>>>(in, zb, g, plan, tw, alfa, beta, drop);
+}
+template <class T, int KB, class S>
+static void launch_zinv(dim3 grid, size_t smem, cudaStream_t st, const typename C2<S>::type* in,
+                        typename C2<T>::type* zb, const Dims& g, const FFTPlan& plan,
+                        const typename C2<T>::type* tw, const double* alfa, const double* beta, int drop) {
+  switch (g.nzp) {
+#define SB_CASE(n)                                                                                 \
+  case n:                                                                                          \
+    zinv_n<T, KB, S, n, fixed_threads(n, KB)>(grid, smem, st, in, zb, g, plan, tw, alfa, beta, drop); \
+    return;
+    SB_FIXED_LENGTHS(SB_CASE)
+#undef SB_CASE
+    default:
+      zinv_n<T, KB, S, 0, sgpu_ctx::fft_threads>(grid, smem, st, in, zb, g, plan, tw, alfa, beta, drop);
+  }
+}
+
+template <class T, int KB, class S, int N, int NT>
+static void zfwd_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* xb,
+                   typename C2<S>::type* out, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
+                   const double* mean, double rot) {
+  cudaFuncSetAttribute(k_zfwd<T, KB, S, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zfwd<T, KB, S, N, NT><<<grid, NT, smem, st>>>(xb, out, g, plan, tw, mean, rot);
+}
+template <class T, int KB, class S>
+static void launch_zfwd(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* xb,
+                        typename C2<S>::type* out, const Dims& g, const FFTPlan& plan,
+                        const typename C2<T>::type* tw, const double* mean, double rot) {
+  switch (g.nzp) {
+#define SB_CASE(n)                                                                          \
+  case n:                                                                                   \
+    zfwd_n<T, KB, S, n, fixed_threads(n, KB)>(grid, smem, st, xb, out, g, plan, tw, mean, rot); \
+    return;
+    SB_FIXED_LENGTHS(SB_CASE)
+#undef SB_CASE
+    default:
+      zfwd_n<T, KB, S, 0, sgpu_ctx::fft_threads>(grid, smem, st, xb, out, g, plan, tw, mean, rot);
+  }
+}
+
+template <class T, int RB, int N, int NT>
+static void xpass_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
+                    typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
+                    const double* dyi, double dxi, double dzi, double rot, unsigned long long* cfl,
+                    const double* mean) {
+  cudaFuncSetAttribute(k_xpass<T, RB, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_xpass<T, RB, N, NT><<<grid, NT, smem, st>>>(zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
+}
+template <class T, int RB, int NT0>
+static void launch_xpass(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
+                         typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan,
+                         const typename C2<T>::type* tw, const double* dyi, double dxi, double dzi, double rot,
+                         unsigned long long* cfl, const double* mean) {
+  switch (g.nxp) {
+#define SB_CASE(n)                                                                                        \
+  case n:                                                                                                 \
+    xpass_n<T, RB, n, fixed_threads(n, 3 * RB)>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, \
+                                                mean);                                                    \
+    return;
+    SB_FIXED_LENGTHS(SB_CASE)
+#undef SB_CASE
+    default:
+      xpass_n<T, RB, 0, NT0>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
+  }
+}
+
 static int enqueue_nonlin(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
@@ -653,26 +739,26 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     // products analytically and their mean-mean product in FP64
     prof_mark(c, K_ZINV);
     k_mean_profiles<float><<<(g.nyp + 127) / 128, 128, 0, c->stream>>>(c->stf, c->meanp, g);
-    k_zinv<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_zf, c->stream>>>(
-        c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta, 1);
+    launch_zinv<float, sgpu_ctx::kbf, float>(gzf, s_zf, c->stream, c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa,
+                                             c->beta, 1);
     prof_mark(c, K_XPASS);
-    k_xpass<float, sgpu_ctx::rbf><<<gxf, sgpu_ctx::fft_threads, s_xf, c->stream>>>(
-        zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
+    launch_xpass<float, sgpu_ctx::rbf, sgpu_ctx::fft_threads>(gxf, s_xf, c->stream, zbf, xbf, g, c->twx.plan,
+                                                              c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
     prof_mark(c, K_ZFWD);
-    k_zfwd<float, sgpu_ctx::kbf, float><<<gzf, sgpu_ctx::fft_threads, s_zf, c->stream>>>(
-        xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp, P.rot);
+    launch_zfwd<float, sgpu_ctx::kbf, float>(gzf, s_zf, c->stream, xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp,
+                                             P.rot);
     c->launches++;
   } else {
     prof_mark(c, K_ZINV);
-    k_zinv<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
-        c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa, c->beta, 0);
+    launch_zinv<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa,
+                                              c->beta, 0);
     dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
     prof_mark(c, K_XPASS);
-    k_xpass<double, sgpu_ctx::rb><<<gx, sgpu_ctx::xpass64_threads, s_x, c->stream>>>(
-        c->zb, c->xb, g, c->twx.plan, c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
+    launch_xpass<double, sgpu_ctx::rb, sgpu_ctx::xpass64_threads>(gx, s_x, c->stream, c->zb, c->xb, g, c->twx.plan,
+                                                                  c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
     prof_mark(c, K_ZFWD);
-    k_zfwd<double, sgpu_ctx::kb, double><<<gz, sgpu_ctx::fft_threads, s_z, c->stream>>>(
-        c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr, 0.0);
+    launch_zfwd<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr,
+                                              0.0);
   }
   c->launches += 3;
   if (c->iles >= 1) {

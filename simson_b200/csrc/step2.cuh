@@ -25,14 +25,21 @@ namespace sb {
 
 // drop_mean: leave out the kx = kz = 0 mode (the mean profiles U, W,
 // Omega_x, Omega_z), which the mixed-precision path adds back analytically.
-template <class T, int KB, class S>
-__global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
-                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       const double* __restrict__ alfa, const double* __restrict__ beta, int drop_mean) {
+// N > 0: the z length g.nzp is N, transformed with the compile-time plan by
+// NT threads per CTA; N = 0: runtime plan, any block size.
+// (the FP64 fixed-length variant is held to three CTAs per SM: unbounded it
+// takes ~130 registers and one CTA per SM)
+template <class T, int KB, class S, int N = 0, int NT = 0>
+__global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) ? 3 : 0)
+    k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
+           FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ alfa,
+           const double* __restrict__ beta, int drop_mean) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nzp = N > 0 ? N : g.nzp;
+  const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* b0 = reinterpret_cast<V*>(smem_raw);
-  V* b1 = b0 + (size_t)g.nzp * KB;
+  V* b1 = b0 + (size_t)nzp * KB;
   const int y = blockIdx.y;
   const int kx0 = blockIdx.x * KB;
   const int nzh = g.nz / 2;
@@ -40,15 +47,18 @@ __global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<
   // fine-grid fields: 0 u, 1 v, 2 w, 3 omega_x, 4 omega_y, 5 omega_z
   const int src_slot[6] = {0, 1, 2, 3, -1, 4};
   for (int f = 0; f < 6; ++f) {
-    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+    // two loads in flight per thread; a full unroll of the fixed-length loop
+    // costs occupancy (measured)
+#pragma unroll(N > 0 ? 2 : 1)
+    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
       const int m = t / KB;
       const int b = t - m * KB;
       const int kx = kx0 + b;
       int iz = -1;
       if (m < nzh)
         iz = m;
-      else if (m > g.nzp - nzh)
-        iz = m - (g.nzp - g.nz);
+      else if (m > nzp - nzh)
+        iz = m - (nzp - g.nz);
       V val = V{(T)0, (T)0};
       if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
         const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
@@ -65,12 +75,12 @@ __global__ void k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<
       b0[t] = val;
     }
     __syncthreads();
-    V* res = fft_columns<T, KB>(b0, b1, plan, tw, +1);
-    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+    V* res = fft_any<T, KB, N, NT, 1>(b0, b1, plan, tw);
+    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
       const int m = t / KB;
       const int b = t - m * KB;
       const int kx = kx0 + b;
-      if (kx < g.nx2) zb[(((size_t)f * g.nyp + y) * g.nzp + m) * g.nx2 + kx] = res[t];
+      if (kx < g.nx2) zb[(((size_t)f * g.nyp + y) * nzp + m) * g.nx2 + kx] = res[t];
     }
     __syncthreads();
   }
@@ -81,21 +91,23 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-template <class T, int RB>
-__global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb,
-                        Dims g, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                        const double* __restrict__ dyi, double dxi, double dzi, double rot,
-                        unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean) {
+// N > 0: the x length g.nxp is N (compile-time plan, NT threads per CTA).
+template <class T, int RB, int N = 0, int NT = 0>
+__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+    k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb, Dims g,
+            FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ dyi, double dxi,
+            double dzi, double rot, unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int B = 3 * RB;
+  constexpr int B = 3 * RB;
+  const int n = N > 0 ? N : g.nxp;
+  const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* bA = reinterpret_cast<V*>(smem_raw);
-  V* bB = bA + (size_t)g.nxp * B;
+  V* bB = bA + (size_t)n * B;
   const int y = blockIdx.y;
   const int m0 = blockIdx.x * RB;
-  const int n = g.nxp;
   // Hermitian completion of two half spectra into one complex spectrum
-  for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
+  for (int t = threadIdx.x; t < n * B; t += nthr) {
     const int k = t / B;
     const int c = t - k * B;
     const int r = c / 3, q = c - 3 * (c / 3);
@@ -118,7 +130,7 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
     bA[t] = z;
   }
   __syncthreads();
-  V* res = fft_columns<T, 3 * RB>(bA, bB, plan, tw, +1);
+  V* res = fft_any<T, B, N, NT, 1>(bA, bB, plan, tw);
   V* oth = (res == bA) ? bB : bA;
   // products in physical space, H into (H1 + i H2) per row and, for an even
   // number of rows, the H3 of rows 2q and 2q+1 paired as H3 + i H3' (one
@@ -127,7 +139,7 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
   double cmax = 0.0;
   const double dy = dyi[y];
   const T r2 = (T)(2.0 * rot);
-  for (int t = threadIdx.x; t < n * RB; t += blockDim.x) {
+  for (int t = threadIdx.x; t < n * RB; t += nthr) {
     const int j = t / RB;
     const int r = t - j * RB;
     const V z0 = res[j * B + 3 * r + 0];
@@ -167,8 +179,8 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
     }
   }
   __syncthreads();
-  V* fres = fft_columns<T, B2>(oth, res, plan, tw, -1);
-  for (int t = threadIdx.x; t < g.nx2 * RB; t += blockDim.x) {
+  V* fres = fft_any<T, B2, N, NT, -1>(oth, res, plan, tw);
+  for (int t = threadIdx.x; t < g.nx2 * RB; t += nthr) {
     const int k = t / RB;
     const int r = t - k * RB;
     const int m = m0 + r;
@@ -209,34 +221,36 @@ __global__ void k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2
 
 // mean != nullptr: add nxp*nzp*(W Omega_x - U (Omega_z + 2 rot)) to the
 // kx = kz = 0 mode of H2 in FP64 (the mean-mean product left out by k_xpass).
-template <class T, int KB, class S>
-__global__ void k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<S>::type* __restrict__ st, Dims g,
-                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
-                       const double* __restrict__ mean, double rot) {
+template <class T, int KB, class S, int N = 0, int NT = 0>
+__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+    k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<S>::type* __restrict__ st, Dims g,
+           FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ mean, double rot) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nzp = N > 0 ? N : g.nzp;
+  const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* b0 = reinterpret_cast<V*>(smem_raw);
-  V* b1 = b0 + (size_t)g.nzp * KB;
+  V* b1 = b0 + (size_t)nzp * KB;
   const int y = blockIdx.y;
   const int kx0 = blockIdx.x * KB;
   const int nzh = g.nz / 2;
-  const size_t fs = (size_t)g.nyp * g.nzp * g.nx2;
+  const size_t fs = (size_t)g.nyp * nzp * g.nx2;
   const size_t slot = (size_t)g.nyp * g.NP;
   for (int f = 0; f < 3; ++f) {
-    for (int t = threadIdx.x; t < g.nzp * KB; t += blockDim.x) {
+    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
       const int m = t / KB;
       const int b = t - m * KB;
       const int kx = kx0 + b;
-      b0[t] = (kx < g.nx2) ? xb[f * fs + ((size_t)y * g.nzp + m) * g.nx2 + kx] : V{(T)0, (T)0};
+      b0[t] = (kx < g.nx2) ? xb[f * fs + ((size_t)y * nzp + m) * g.nx2 + kx] : V{(T)0, (T)0};
     }
     __syncthreads();
-    V* res = fft_columns<T, KB>(b0, b1, plan, tw, -1);
-    for (int t = threadIdx.x; t < g.nz * KB; t += blockDim.x) {
+    V* res = fft_any<T, KB, N, NT, -1>(b0, b1, plan, tw);
+    for (int t = threadIdx.x; t < g.nz * KB; t += nthr) {
       const int iz = t / KB;
       const int b = t - iz * KB;
       const int kx = kx0 + b;
       if (kx >= g.nx2) continue;
-      const int m = (iz < nzh) ? iz : iz + (g.nzp - g.nz);
+      const int m = (iz < nzh) ? iz : iz + (nzp - g.nz);
       const V h = res[m * KB + b];
       double hx = (double)h.x, hy = (double)h.y;
       if (mean != nullptr && f == 1 && iz == 0 && kx == 0) {

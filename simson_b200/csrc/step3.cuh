@@ -36,13 +36,15 @@ typedef ColT<double> Col;
 
 // L2 prefetch of a row a few iterations ahead of a sweep: the sweeps are
 // serial in y, so without it each row's loads wait a full DRAM latency.
-// The prefetch holds no register; callers pass in-range addresses only.
+// The prefetch holds no register; callers pass in-range addresses only, and
+// addresses outside the global window (the mean-flow solve keeps its columns
+// in shared memory) are skipped.
 #ifndef SB_PF_ROWS
 #define SB_PF_ROWS 3
 #endif
 SB_HD __forceinline__ void pf_l2(const void* ptr) {
 #ifdef __CUDA_ARCH__
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(ptr)));
+  if (__isGlobal(ptr)) asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(ptr)));
 #else
   (void)ptr;
 #endif
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
 // ---------------------------------------------------------------------------
 // kx = kz = 0: mean flow with the constant-flux pressure gradient
 // (linearbl.f:1214-1470 tau branch, ibc = 0; next partial RHS :1712-1733)
-// One thread; FP64.  scratch: 12 columns of n doubles.
+// One warp (lane 0 solves); FP64.  scratch: 12 columns of n doubles in shared memory.
 // ---------------------------------------------------------------------------
 struct MeanArgs {
   double2 *H1, *H3;        // Chebyshev nonlinear term
@@ -583,7 +585,11 @@ struct MeanArgs {
 template <class IO>
 __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
   extern __shared__ double msm[];  // 12 columns of n doubles
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // one warp: the lanes move the columns between global and shared memory
+  // (strided by NP, so a serial loop would wait one DRAM latency per row);
+  // lane 0 does the solves in shared memory in the reference's order
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
   const int n = g.nyp;
   const int NP = g.NP;
   A.scr = msm;
@@ -591,40 +597,48 @@ __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
   Col U{A.scr + 4 * n, 1}, W{A.scr + 5 * n, 1}, DU{A.scr + 6 * n, 1}, DW{A.scr + 7 * n, 1};
   Col cp{A.scr + 8 * n, 1}, wt{A.scr + 9 * n, 1}, t1{A.scr + 10 * n, 1}, t2{A.scr + 11 * n, 1};
   const double c1 = 2.0 * re / (rk.an + rk.bn) * rk.an;
-  double px = A.scal[0];
-  const double mflux = A.scal[1];
-  for (int j = 0; j < n; ++j) {
+  for (int j = lane; j < n; j += 32) {
     huw1[j] = (double)reinterpret_cast<const IO*>(A.H1)[(size_t)j * NP].x;
     huw2[j] = (double)reinterpret_cast<const IO*>(A.H3)[(size_t)j * NP].x;
     fu[j] = A.puw[j] - c1 * huw1[j];
     fw[j] = A.puw[n + j] - c1 * huw2[j];
   }
-  fu[0] = fu[0] + 2.0 * re * px;
-  const double lam = 0.0 + 2.0 * re / (rk.an + rk.bn);
-  const double bz[1] = {0.0};
-  {
-    const Col f[2] = {fu, fw};
-    const Col x[2] = {U, W};
-    const double b0[2] = {0.0, 0.0};
-    tau_solve<2>(lam, n, f, x, b0, b0, cp, wt);
-  }
-  if (A.cflux) {
-    double m1 = 0.0;
-    for (int j = 0; j < n; j += 2) m1 = m1 - U[j] * 2.0 / (double)(j * j - 1);
+  __syncwarp();
+  if (lane == 0) {
+    double px = A.scal[0];
+    const double mflux = A.scal[1];
     fu[0] = fu[0] + 2.0 * re * px;
-    tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
-    double m2 = 0.0;
-    for (int j = 0; j < n; j += 2) m2 = m2 - U[j] * 2.0 / (double)(j * j - 1);
-    fu[0] = fu[0] - 4.0 * re * px;
-    px = px * (1.0 + (mflux - m1) / (m2 - m1));
-    fu[0] = fu[0] + 2.0 * re * px;
-    tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
-    A.scal[0] = px;
+    const double lam = 0.0 + 2.0 * re / (rk.an + rk.bn);
+    const double bz[1] = {0.0};
+    {
+      const Col f[2] = {fu, fw};
+      const Col x[2] = {U, W};
+      const double b0[2] = {0.0, 0.0};
+      tau_solve<2>(lam, n, f, x, b0, b0, cp, wt);
+    }
+    if (A.cflux) {
+      double m1 = 0.0;
+      for (int j = 0; j < n; j += 2) m1 = m1 - U[j] * 2.0 / (double)(j * j - 1);
+      fu[0] = fu[0] + 2.0 * re * px;
+      tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
+      double m2 = 0.0;
+      for (int j = 0; j < n; j += 2) m2 = m2 - U[j] * 2.0 / (double)(j * j - 1);
+      fu[0] = fu[0] - 4.0 * re * px;
+      px = px * (1.0 + (mflux - m1) / (m2 - m1));
+      fu[0] = fu[0] + 2.0 * re * px;
+      tau_solve<1>(lam, n, &fu, &U, bz, bz, cp, wt);
+      A.scal[0] = px;
+    }
+    cheb_deriv(DU, U, n);
+    cheb_deriv(DW, W, n);
+    cheb_deriv(t1, DU, n);
+    cheb_deriv(t2, DW, n);
   }
-  cheb_deriv(DU, U, n);
-  cheb_deriv(DW, W, n);
+  __syncwarp();
   typedef decltype(IO::x) R;
-  for (int j = 0; j < n; ++j) {
+  const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
+  const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
+  for (int j = lane; j < n; j += 32) {
     reinterpret_cast<IO*>(A.OU)[(size_t)j * NP] = IO{(R)U[j], (R)0};
     reinterpret_cast<IO*>(A.OW)[(size_t)j * NP] = IO{(R)W[j], (R)0};
     reinterpret_cast<IO*>(A.OV)[(size_t)j * NP] = IO{(R)0, (R)0};
@@ -632,12 +646,6 @@ __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
     reinterpret_cast<IO*>(A.OZ)[(size_t)j * NP] = IO{(R)(-DU[j]), (R)0};
     A.PV[(size_t)j * NP] = double2{0.0, 0.0};
     A.PW[(size_t)j * NP] = double2{0.0, 0.0};
-  }
-  const double c1n = 2.0 * re / (rk.anp1 + rk.bnp1);
-  const double c2 = 2.0 * re * rk.bnp1 / (rk.anp1 + rk.bnp1);
-  cheb_deriv(t1, DU, n);
-  cheb_deriv(t2, DW, n);
-  for (int j = 0; j < n; ++j) {
     A.puw[j] = -t1[j] - c1n * U[j] - c2 * huw1[j];
     A.puw[n + j] = -t2[j] - c1n * W[j] - c2 * huw2[j];
   }

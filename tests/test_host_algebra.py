@@ -157,6 +157,31 @@ def test_fft_paired_columns_match_numpy(n, prec):
         assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("n", [72, 96, 240, 288, 576])
+@pytest.mark.parametrize("prec", [0, 1])
+def test_fixed_length_fft(n, prec):
+    """The compile-time plans of the production transform lengths over 3, 4
+    and 6 interleaved columns against numpy, both signs; with 4 columns they
+    equal the runtime plan bit for bit (same passes, twiddles, butterflies)."""
+    host = ctypes.CDLL(sbuild.build_hostcheck())
+    host.sbh_cfft.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int]
+    host.sbh_fft4.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int]
+    tol = (1e-15 if prec == 0 else 2e-6) * n
+    for cols in (3, 4, 6):
+        rng = np.random.default_rng(n + 7 * prec + 100 * cols)
+        x = rng.standard_normal((n, cols)) + 1j * rng.standard_normal((n, cols))
+        inp = np.ascontiguousarray(np.stack([x.real, x.imag], -1).ravel())
+        out = np.zeros(2 * cols * n)
+        for sign, ref in ((-1, np.fft.fft(x, axis=0)), (1, np.fft.ifft(x, axis=0) * n)):
+            assert host.sbh_cfft(n, cols, P(inp), P(out), sign, prec) > 0
+            y = (out[0::2] + 1j * out[1::2]).reshape(n, cols)
+            assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
+            if cols == 4:
+                out4 = np.zeros_like(out)
+                assert host.sbh_fft4(n, P(inp), P(out4), sign, prec) > 0
+                assert np.array_equal(out, out4)
+
+
 @pytest.mark.parametrize("n", [17, 65, 193])
 def test_tensor_core_chebyshev_matrix(n):
     """The 3xTF32 matrices of the mixed path's tensor-core Chebyshev
