@@ -351,12 +351,6 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
                        (int)s_yf);
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
-  // The pencil grid fills every SM and uses no shared memory; with the
-  // default carveout its SMs hold no room for the concurrent mean-flow block
-  // (12 columns of nyp doubles in shared memory), which then starts only when
-  // the pencil wave retires.  Keep a shared-memory carveout beside it.
-  cudaFuncSetAttribute(k_pencil<float2, double, float>, cudaFuncAttributePreferredSharedMemoryCarveout, 25);
-  cudaFuncSetAttribute(k_pencil<double2, double, double>, cudaFuncAttributePreferredSharedMemoryCarveout, 25);
   c->dtn = P.dt;
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
@@ -808,16 +802,16 @@ static int enqueue_linear(sgpu_ctx* c) {
   if (c->prof) {
     prof_mark(c, K_MEAN);
     if (c->mixed)
-      k_mean<float2><<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
+      k_mean<float2><<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
     else
-      k_mean<double2><<<1, 32, 12 * g.nyp * sizeof(double), c->stream>>>(M, g, P.re, rk);
+      k_mean<double2><<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
   } else {
     cudaEventRecord(c->fork, c->stream);
     cudaStreamWaitEvent(c->side, c->fork, 0);
     if (c->mixed)
-      k_mean<float2><<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
+      k_mean<float2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
     else
-      k_mean<double2><<<1, 32, 12 * g.nyp * sizeof(double), c->side>>>(M, g, P.re, rk);
+      k_mean<double2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
     cudaEventRecord(c->join, c->side);
   }
   prof_mark(c, K_PENCIL);

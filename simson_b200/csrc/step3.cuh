@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
 // ---------------------------------------------------------------------------
 // kx = kz = 0: mean flow with the constant-flux pressure gradient
 // (linearbl.f:1214-1470 tau branch, ibc = 0; next partial RHS :1712-1733)
-// One warp (lane 0 solves); FP64.  scratch: 12 columns of n doubles in shared memory.
+// One warp (lane 0 solves); FP64.  scratch: 12 columns of n doubles.
 // ---------------------------------------------------------------------------
 struct MeanArgs {
   double2 *H1, *H3;        // Chebyshev nonlinear term
@@ -584,15 +584,16 @@ struct MeanArgs {
 
 template <class IO>
 __global__ void k_mean(MeanArgs A, Dims g, double re, RKc rk) {
-  extern __shared__ double msm[];  // 12 columns of n doubles
-  // one warp: the lanes move the columns between global and shared memory
-  // (strided by NP, so a serial loop would wait one DRAM latency per row);
-  // lane 0 does the solves in shared memory in the reference's order
+  // One warp: the lanes move the columns between the state (strided by NP,
+  // so a serial loop would wait one DRAM latency per row) and the contiguous
+  // scratch columns; lane 0 does the solves in the reference's order.  The
+  // scratch is global (L1-cached), not shared memory: this block runs beside
+  // the pencil grid, whose SMs keep no shared-memory carveout, and a block
+  // that needs shared memory would wait for the whole pencil wave to retire.
   if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
   const int n = g.nyp;
   const int NP = g.NP;
-  A.scr = msm;
   Col huw1{A.scr + 0 * n, 1}, huw2{A.scr + 1 * n, 1}, fu{A.scr + 2 * n, 1}, fw{A.scr + 3 * n, 1};
   Col U{A.scr + 4 * n, 1}, W{A.scr + 5 * n, 1}, DU{A.scr + 6 * n, 1}, DW{A.scr + 7 * n, 1};
   Col cp{A.scr + 8 * n, 1}, wt{A.scr + 9 * n, 1}, t1{A.scr + 10 * n, 1}, t2{A.scr + 11 * n, 1};
