@@ -63,6 +63,12 @@ struct sgpu_ctx {
   int ncz = 0;
   double* rz = nullptr;      // real scratch columns, [nrz][nyp][NP]
   int nrz = 0;
+  // homogeneous solutions of the three RK stages (k_pencil_hom): v_h
+  // [3][nyp][NP], parity sums [3][2 NP], keyed by the stage's a_n + b_n
+  double* hom_vh = nullptr;
+  double* hom_s = nullptr;
+  double hom_key[3] = {0.0, 0.0, 0.0};
+  int hom_next = 0;
   double* mscr = nullptr;    // mean-flow scratch
   double* meanp = nullptr;   // [4][nyp] U, W, Omega_x, Omega_z for the mixed step 2
   double* ampd = nullptr;    // [20][nyp] plane statistics
@@ -288,6 +294,8 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->cz, (size_t)c->ncz * fld * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&c->rz, (size_t)c->nrz * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_vh, 3 * fld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_s, 3 * 2 * (size_t)g.NP * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->ampd, 20 * (size_t)g.nyp * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
@@ -364,7 +372,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
-                  c->mscr, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
+                  c->mscr, c->hom_vh, c->hom_s, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 16; ++i)
@@ -814,11 +822,35 @@ static int enqueue_linear(sgpu_ctx* c) {
       k_mean<double2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
     cudaEventRecord(c->join, c->side);
   }
+  // this stage's homogeneous solutions, computed on its first use (a key of
+  // 0 is never a valid a_n + b_n: dt > 0)
+  const double anbn = rk.an + rk.bn;
+  int hs = -1;
+  for (int s = 0; s < 3; ++s)
+    if (c->hom_key[s] == anbn) hs = s;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  if (hs < 0) {
+    hs = c->hom_next;
+    c->hom_next = (c->hom_next + 1) % 3;
+    c->hom_key[hs] = anbn;
+    prof_mark(c, K_OTHER);
+    if (c->mixed)
+      k_pencil_hom<double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
+          B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP);
+    else
+      k_pencil_hom<double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
+          B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP);
+    c->launches++;
+  }
+  const double* vhc = c->hom_vh + hs * fld;
+  const double* hsc = c->hom_s + hs * 2 * (size_t)g.NP;
   prof_mark(c, K_PENCIL);
   if (c->mixed)
-    k_pencil<float2, double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<float2, double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
+                                                                               vhc, hsc);
   else
-    k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk);
+    k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
+                                                                                 vhc, hsc);
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);

@@ -125,9 +125,17 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 // sum_{k odd} k^2 x_k and dsum[q][1] = sum_{j odd} (D x)_j = sum_{k even}
 // k^2 x_k (D x at y = +-1), so no column of D x is formed.  Two column passes
 // fewer per solution; the same arithmetic in a different summation order.
-template <int M, class S = double, class FS = S, bool FAST = false>
+//
+// pre (optional): called at the top of backward row i as pre(i, fnew) and
+// returns in fnew[q] the right-hand side f(i-3) of every column (0-based
+// rows; the caller has produced rows n-1 and n-2 itself), so a right-hand
+// side assembled row by row never goes through memory; f[] is then unused.
+struct NoPre {};
+
+template <int M, class S = double, class FS = S, bool FAST = false, class Pre = NoPre>
 SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S* bc1, const S* bc2, ColT<S> cp,
-                     ColT<S> wt, S (*dsum)[2] = nullptr) {
+                     ColT<S> wt, S (*dsum)[2] = nullptr, Pre pre = Pre()) {
+  constexpr bool HOOK = !std::is_same<Pre, NoPre>::value;
   // every column is a distinct array: restrict-qualified raw pointers let the
   // loads of a sweep run ahead of its stores
   const FS* __restrict__ fp[M];
@@ -135,8 +143,8 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   size_t fs[M], xs[M];
 #pragma unroll
   for (int q = 0; q < M; ++q) {
-    fp[q] = f[q].a;
-    fs[q] = f[q].s;
+    fp[q] = HOOK ? nullptr : f[q].a;
+    fs[q] = HOOK ? 0 : f[q].s;
     xp[q] = x[q].a;
     xs[q] = x[q].s;
   }
@@ -152,14 +160,16 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   // right-hand-side window: row i reads f(i-3), f(i-1), f(i+1) (0-based);
   // per row parity the last two stay in registers, so each row loads one
   // value per column (row i-2 reuses f(i-1) and f(i-3)). Used by the FP64
-  // path; in the reordered (FAST) variant the extra registers spill and the
-  // plain three loads are faster.
-  constexpr bool WIN = !FAST;
+  // path and with pre; in the reordered (FAST) variant without pre the extra
+  // registers spill and the plain three loads are faster.
+  constexpr bool WIN = !FAST || HOOK;
   S wlo0[M], whi0[M], wlo1[M], whi1[M];  // even / odd rows (selects keep them in registers)
 #pragma unroll
   for (int q = 0; q < M; ++q) wlo0[q] = wlo1[q] = whi0[q] = whi1[q] = (S)0.0;
   for (int i = n; i >= 3; --i) {
     const int pr = i & 1;
+    S fh[M];
+    if constexpr (HOOK) pre(i, fh);
     S dinv = (S)1.0, cnew = (S)0.0, wnew = (S)0.0;
     if (i <= n - 2) {
       const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
@@ -178,8 +188,12 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     for (int q = 0; q < M; ++q) {
       S r = (S)0.0;
       if (fp[q] != nullptr && i - 3 - SB_PF_ROWS >= 0) pf_l2(fp[q] + (size_t)(i - 3 - SB_PF_ROWS) * fs[q]);
-      if (fp[q] != nullptr && WIN) {
-        const S fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];  // f(i-3)
+      if ((HOOK || fp[q] != nullptr) && WIN) {
+        S fnew;  // f(i-3)
+        if constexpr (HOOK)
+          fnew = fh[q];
+        else
+          fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];
         const S fm = pr ? wlo1[q] : wlo0[q];               // f(i-1)
         const S fpl = pr ? whi1[q] : whi0[q];              // f(i+1)
         if (i == 3) {
@@ -380,17 +394,70 @@ struct RKc {
   double an, bn, anp1, bnp1;
 };
 
+// Homogeneous solutions of one RK stage, cached: phi_h solves
+// (D^2 - lam) phi_h = 0 with phi_h = 1 at both walls and v_h solves
+// (D^2 - k^2) v_h = phi_h with v_h = 0 (linearbl.f:625-626, 1000-1001 with
+// zero forcing).  They depend on k^2 and lam = k^2 + 2 Re/(a_n + b_n) only,
+// so they are computed once per stage value of a_n + b_n (dt is fixed) with
+// exactly the arithmetic of the per-substep solves (the same tau_solve
+// column operations), and the pencil kernel reads v_h and the two parity
+// sums of D v_h instead of solving for them every substep.
+//   VHc: v_h, n x NP (row-major in y like the fields); HS[2p + s]: FAST: the
+//   parity sums dsum of v_h; FP64 path: sum over j = s, s+2, ... of (D v_h)_j
+//   in ascending order (the reference's order).
+template <class SC, class FC>
+__global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const double* __restrict__ alfa,
+                                                    const double* __restrict__ beta, double re, double anbn,
+                                                    double* __restrict__ VHc, double* __restrict__ HS) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.NP) return;
+  const int kx = p % g.nx2;
+  const int iz = p / g.nx2;
+  if (iz == g.zodd || p == 0) return;
+  const int n = g.nyp;
+  const size_t NP = g.NP;
+  const double a = alfa[kx], be = beta[iz];
+  const double k2 = a * a + be * be;
+  const double lam = k2 + 2.0 * re / anbn;
+  constexpr bool FAST = !std::is_same<FC, double>::value;
+  const ColT<SC> ph{reinterpret_cast<SC*>(B.PHIH) + p, NP};
+  {
+    const ColT<FC> f[1] = {ColT<FC>{nullptr, 0}};
+    const SC one[1] = {1};
+    tau_solve<1, SC, FC, FAST>((SC)lam, n, f, &ph, one, one, ColT<SC>{reinterpret_cast<SC*>(B.CPL) + p, NP},
+                               ColT<SC>{reinterpret_cast<SC*>(B.WTL) + p, NP});
+  }
+  const Col vh{VHc + p, NP};
+  double dsum[1][2] = {{0, 0}};
+  const double b0[1] = {0};
+  tau_solve<1, double, SC, FAST>(k2, n, &ph, &vh, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
+  if (FAST) {
+    HS[2 * (size_t)p] = dsum[0][0];
+    HS[2 * (size_t)p + 1] = dsum[0][1];
+  } else {
+    const Col dvh = col_r(B.DVH, p, NP);
+    cheb_deriv(dvh, vh, n);
+    for (int is = 0; is < 2; ++is) {
+      double sh = 0.0;
+      for (int j = is; j < n; j += 2) sh = sh + dvh[j];
+      HS[2 * (size_t)p + is] = sh;
+    }
+  }
+}
+
 // IO: storage of the Chebyshev H inputs and of the u, v, w, omega_x, omega_z
 // outputs (double2, or float2 under the mixed-precision path); all algebra
 // and the other columns are FP64.
 // SC: scalar of the omega_y / particular-phi Helmholtz solve; FC: storage of
-// its forcing columns h_v, h_omega, f_v, f_omega (read by the solve and the
-// next partial RHS, never differentiated).  FP64 path: double/double; the
-// mixed-precision path stores the forcing in float.  The fourth-order v solve,
-// the superposition and every derivative are FP64 in both.
+// its forcing columns h_v, h_omega (read by the next partial RHS, never
+// differentiated).  FP64 path: double/double; the mixed-precision path stores
+// the forcing in float.  The fourth-order v solve, the superposition and every
+// derivative are FP64 in both.  VHc, HS: this stage's homogeneous solution
+// (k_pencil_hom).
 template <class IO, class SC, class FC>
 __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
-                                                const double* __restrict__ beta, double re, RKc rk) {
+                                                const double* __restrict__ beta, double re, RKc rk,
+                                                const double* __restrict__ VHc, const double* __restrict__ HS) {
   typedef typename C2<SC>::type SC2;
   typedef typename C2<FC>::type FC2;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -408,99 +475,107 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   // the mixed path (FP32 forcing columns) takes the reordered sums of
   // tau_solve<..., FAST>; the FP64 path keeps the reference's order
   constexpr bool FAST = !std::is_same<FC, double>::value;
-  double dsum[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  double dsum[2][2] = {{0, 0}, {0, 0}};
   // this pencil's column of each array; all arrays are distinct
 #define COLP(name) double2* __restrict__ name = B.name + p
   COLP(PV); COLP(PW); COLP(V); COLP(DV);
 #undef COLP
 #define COLF(name) FC2* __restrict__ name = reinterpret_cast<FC2*>(B.name) + p
-  COLF(HV); COLF(HOM); COLF(FV); COLF(FW);
+  COLF(HV); COLF(HOM);
 #undef COLF
   SC2* __restrict__ OM = reinterpret_cast<SC2*>(B.OM) + p;
 #define COLIO(name) IO* __restrict__ name = reinterpret_cast<IO*>(B.name) + p
   COLIO(H1); COLIO(H2); COLIO(H3); COLIO(OU); COLIO(OV); COLIO(OW); COLIO(OX); COLIO(OZ);
 #undef COLIO
-  double* __restrict__ VH = B.VH + p;
-  double* __restrict__ DVH = B.DVH + p;
+  const double* __restrict__ VH = VHc + p;
 
-  // Nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340) in
-  // one backward sweep: g = i alpha H1 + i beta H3 and its y-derivative by the
-  // dcheb recurrence dg_j = dg_{j+2} + 2(j+1) g_{j+1} (same operations as
-  // cheb_deriv), hv = -(dg + k^2 H2), homy = i beta H1 - i alpha H3,
-  // f_v = p_v - c1 hv, f_omega = p_omega - c1 homy.
-  {
-    double2 g1 = double2{0.0, 0.0};                   // g_{j+1}
-    double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
-    for (int j = n - 1; j >= 0; --j) {
-      const size_t o = j * NP;
-      if (j >= SB_PF_ROWS) {
-        const size_t op = o - (size_t)SB_PF_ROWS * NP;
-        pf_l2(H1 + op); pf_l2(H2 + op); pf_l2(H3 + op); pf_l2(PV + op); pf_l2(PW + op);
-      }
-      const IO h1i = H1[o], h2i = H2[o], h3i = H3[o];
-      const double2 h1 = {(double)h1i.x, (double)h1i.y}, h2 = {(double)h2i.x, (double)h2i.y};
-      const double2 h3 = {(double)h3i.x, (double)h3i.y};
-      const double2 pv = PV[o], pw = PW[o];
-      double2 dg;
-      if (j == n - 1) {
-        dg = double2{0.0, 0.0};
-      } else {
-        const double f = 2.0 * (double)(j + 1);
-        dg = (j == n - 2) ? double2{f * g1.x, f * g1.y} : double2{d2.x + f * g1.x, d2.y + f * g1.y};
-      }
-      d2 = d1;
-      d1 = dg;
-      if (j == 0) dg = double2{0.5 * dg.x, 0.5 * dg.y};
-      g1 = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
-      const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
-      HOM[o] = FC2{(FC)hom.x, (FC)hom.y};
-      FW[o] = FC2{(FC)(pw.x - c1 * hom.x), (FC)(pw.y - c1 * hom.y)};
-      const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
-      HV[o] = FC2{(FC)hv.x, (FC)hv.y};
-      FV[o] = FC2{(FC)(pv.x - c1 * hv.x), (FC)(pv.y - c1 * hv.y)};
+  // Nonlinear forcing of the omega_y and phi equations (linearbl.f:303-340),
+  // one row per call in descending order: g = i alpha H1 + i beta H3 and its
+  // y-derivative by the dcheb recurrence dg_j = dg_{j+2} + 2(j+1) g_{j+1}
+  // (same operations as cheb_deriv), hv = -(dg + k^2 H2),
+  // homy = i beta H1 - i alpha H3 (stored for the next partial RHS), and the
+  // right-hand sides f_v = p_v - c1 hv, f_omega = p_omega - c1 homy returned
+  // to the omega_y/phi solve, which consumes them in the same order: the
+  // forcing never goes through memory.
+  double2 g1 = double2{0.0, 0.0};                           // g_{j+1}
+  double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
+  auto assemble = [&](int j, SC* fr) {
+    const size_t o = j * NP;
+    if (j >= SB_PF_ROWS) {
+      const size_t op = o - (size_t)SB_PF_ROWS * NP;
+      pf_l2(H1 + op); pf_l2(H2 + op); pf_l2(H3 + op); pf_l2(PV + op); pf_l2(PW + op);
     }
-  }
-  // phi (particular, homogeneous) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
+    const IO h1i = H1[o], h2i = H2[o], h3i = H3[o];
+    const double2 h1 = {(double)h1i.x, (double)h1i.y}, h2 = {(double)h2i.x, (double)h2i.y};
+    const double2 h3 = {(double)h3i.x, (double)h3i.y};
+    const double2 pv = PV[o], pw = PW[o];
+    double2 dg;
+    if (j == n - 1) {
+      dg = double2{0.0, 0.0};
+    } else {
+      const double f = 2.0 * (double)(j + 1);
+      dg = (j == n - 2) ? double2{f * g1.x, f * g1.y} : double2{d2.x + f * g1.x, d2.y + f * g1.y};
+    }
+    d2 = d1;
+    d1 = dg;
+    if (j == 0) dg = double2{0.5 * dg.x, 0.5 * dg.y};
+    g1 = double2{-a * h1.y - be * h3.y, a * h1.x + be * h3.x};
+    const double2 hom = double2{-be * h1.y + a * h3.y, be * h1.x - a * h3.x};
+    const FC2 homs = FC2{(FC)hom.x, (FC)hom.y};
+    HOM[o] = homs;
+    const double2 hv = double2{-(dg.x + k2 * h2.x), -(dg.y + k2 * h2.y)};
+    const FC2 hvs = FC2{(FC)hv.x, (FC)hv.y};
+    HV[o] = hvs;
+    // f_v, f_omega rounded to the forcing storage type as when they were stored
+    fr[0] = (SC)(FC)(pv.x - c1 * hv.x);
+    fr[1] = (SC)(FC)(pv.y - c1 * hv.y);
+    fr[2] = (SC)(FC)(pw.x - c1 * hom.x);
+    fr[3] = (SC)(FC)(pw.y - c1 * hom.y);
+  };
+  // phi (particular) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
   {
     auto cre = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p, 2 * NP}; };
     auto cim = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
     auto crl = [&](double* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + p, NP}; };
-    auto fre = [&](double2* arr) { return ColT<FC>{reinterpret_cast<FC*>(arr) + 2 * (size_t)p, 2 * NP}; };
-    auto fim = [&](double2* arr) { return ColT<FC>{reinterpret_cast<FC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
-    const ColT<FC> f[5] = {fre(B.FV), fim(B.FV), fre(B.FW), fim(B.FW), ColT<FC>{nullptr, 0}};
-    const ColT<SC> x[5] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM), crl(B.PHIH)};
-    const SC bc1[5] = {0, 0, 0, 0, 1}, bc2[5] = {0, 0, 0, 0, 1};
-    tau_solve<5, SC, FC, FAST>((SC)lam, n, f, x, bc1, bc2, crl(B.CPL), crl(B.WTL));
+    // rows n-1 and n-2 first; the solve asks for row i-3 at its row i
+    SC fdummy[4];
+    assemble(n - 1, fdummy);
+    assemble(n - 2, fdummy);
+    const ColT<FC> f[4] = {};
+    const ColT<SC> x[4] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM)};
+    const SC bc0[4] = {0, 0, 0, 0};
+    tau_solve<4, SC, FC, FAST>((SC)lam, n, f, x, bc0, bc0, crl(B.CPL), crl(B.WTL), nullptr,
+                               [&](int i, SC* fr) { assemble(i - 3, fr); });
     // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
-    const ColT<SC> fv[3] = {cre(B.PHI), cim(B.PHI), crl(B.PHIH)};
-    const Col xv[3] = {col_re(B.V, p, NP), col_im(B.V, p, NP), col_r(B.VH, p, NP)};
-    const double b0[3] = {0, 0, 0};
-    tau_solve<3, double, SC, FAST>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
+    const ColT<SC> fv[2] = {cre(B.PHI), cim(B.PHI)};
+    const Col xv[2] = {col_re(B.V, p, NP), col_im(B.V, p, NP)};
+    const double b0[2] = {0, 0};
+    tau_solve<2, double, SC, FAST>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
   }
+  const double hs0 = HS[2 * (size_t)p], hs1 = HS[2 * (size_t)p + 1];
   double cvr[2], cvi[2];
   if (FAST) {
     // parity sums of dv from v itself (returned by the v solve)
+    const double hs[2] = {hs0, hs1};
     for (int is = 0; is < 2; ++is) {
-      const double cinv = 1.0 / dsum[2][is];
+      const double cinv = 1.0 / hs[is];
       cvr[1 - is] = (0.0 - dsum[0][is]) * cinv;
       cvi[1 - is] = (0.0 - dsum[1][is]) * cinv;
     }
   } else {
   // dv/dy = 0 at the walls: add the homogeneous solution per parity
   // (linearbl.f:1020-1085).  The parity sums of dv run in ascending order as
-  // in the reference, so dv and dvh are stored by a backward derivative sweep.
+  // in the reference, so dv is stored by a backward derivative sweep.
   cheb_deriv(col_re(B.DV, p, NP), col_re(B.V, p, NP), n);
   cheb_deriv(col_im(B.DV, p, NP), col_im(B.V, p, NP), n);
-  cheb_deriv(col_r(B.DVH, p, NP), col_r(B.VH, p, NP), n);
   for (int is = 0; is < 2; ++is) {
-    double sr = 0.0, si = 0.0, sh = 0.0;
+    double sr = 0.0, si = 0.0;
     for (int j = is; j < n; j += 2) {
       const double2 dv = DV[j * NP];
       sr = sr + dv.x;
       si = si + dv.y;
-      sh = sh + DVH[j * NP];
     }
-    const double cinv = 1.0 / sh;
+    const double cinv = 1.0 / (is == 0 ? hs0 : hs1);
     cvr[1 - is] = (0.0 - sr) * cinv;
     cvi[1 - is] = (0.0 - si) * cinv;
   }
