@@ -441,6 +441,73 @@ SB_HD __forceinline__ typename C2<T>::type* cfft(typename C2<T>::type* src, type
   }
 }
 
+// One pass with accessors instead of shared-memory buffers: ld(m, b) returns
+// element m of column b of the pass input, st(k, b, v) stores element k of
+// column b of its output.  The first pass of cfft_io reads the global arrays
+// through ld and its last pass writes them through st, so the data crosses
+// shared memory only between passes.
+template <class T, int B, int N, int R, int NS, int S, int NT, class Ld, class St>
+SB_HD __forceinline__ void cpass_io(Ld ld, St st, const typename C2<T>::type* __restrict__ tw, int t0) {
+  typedef typename C2<T>::type V;
+  constexpr int nb = N / R;
+  constexpr int items = nb * B;
+  constexpr int tstep = N / (NS * R);
+  constexpr int iters = (items + NT - 1) / NT;
+#pragma unroll
+  for (int it = 0; it < iters; ++it) {
+    const int t = t0 + it * NT;
+    if (items % NT != 0 && t >= items) break;
+    const unsigned j = (unsigned)t / B;
+    const unsigned b = (unsigned)t - j * B;
+    const unsigned jg = j / NS;
+    const unsigned jm = j - jg * NS;
+    V v[9];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ld((int)(j + r * nb), (int)b);
+    if (NS > 1 && jm != 0) twiddle<T, R, S>(v, tw, (int)(jm * tstep));
+    dft_small<T, V>(v, R, S);
+    const int k0 = (int)(jg * NS * R + jm);
+#pragma unroll
+    for (int r = 0; r < R; ++r) st(k0 + r * NS, (int)b, v[r]);
+  }
+}
+
+template <class T, int B>
+struct SmemLd {
+  const typename C2<T>::type* __restrict__ p;
+  SB_HD __forceinline__ typename C2<T>::type operator()(int m, int b) const { return p[m * B + b]; }
+};
+template <class T, int B>
+struct SmemSt {
+  typename C2<T>::type* __restrict__ p;
+  SB_HD __forceinline__ void operator()(int k, int b, typename C2<T>::type v) const { p[k * B + b] = v; }
+};
+
+// N-point transform of B columns from ld to st (at least two passes);
+// buf0/buf1 hold the intermediate passes.  The caller syncs before reusing
+// the buffers.
+template <class T, int B, int N, int S, int NT, int P = 0, class Ld, class St>
+SB_HD __forceinline__ void cfft_io(Ld ld, St st, typename C2<T>::type* buf0, typename C2<T>::type* buf1,
+                                   const typename C2<T>::type* __restrict__ tw, int t0) {
+  constexpr CPlanData pl = cplan_make(N);
+  static_assert(pl.npass >= 2, "cfft_io needs at least two passes");
+  if constexpr (P == 0) {
+    cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT>(ld, SmemSt<T, B>{buf0}, tw, t0);
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+#endif
+    cfft_io<T, B, N, S, NT, 1>(ld, st, buf0, buf1, tw, t0);
+  } else if constexpr (P == pl.npass - 1) {
+    cpass_io<T, B, N, pl.radix[P], pl.ns[P], S, NT>(SmemLd<T, B>{buf0}, st, tw, t0);
+  } else {
+    cpass_io<T, B, N, pl.radix[P], pl.ns[P], S, NT>(SmemLd<T, B>{buf0}, SmemSt<T, B>{buf1}, tw, t0);
+#ifdef __CUDA_ARCH__
+    __syncthreads();
+#endif
+    cfft_io<T, B, N, S, NT, P + 1>(ld, st, buf1, buf0, tw, t0);
+  }
+}
+
 // runtime plan (N == 0) or compile-time plan, same interface
 template <class T, int B, int N, int NT, int S>
 __device__ __forceinline__ typename C2<T>::type* fft_any(typename C2<T>::type* buf0, typename C2<T>::type* buf1,

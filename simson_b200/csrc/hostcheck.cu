@@ -181,9 +181,19 @@ static int host_cfft(const double* in, double* out, int sign) {
     tw[m] = V{(T)cosl(ang), (T)sinl(ang)};
   }
   for (size_t i = 0; i < B * (size_t)N; ++i) a[i] = V{(T)in[2 * i], (T)in[2 * i + 1]};
+  std::vector<V> in2(a), out2(B * (size_t)N), c0(B * (size_t)N), c1(B * (size_t)N);
   V* res = sign > 0 ? cfft<T, B, N, 1, 1>(a.data(), b.data(), tw.data(), 0)
                     : cfft<T, B, N, -1, 1>(a.data(), b.data(), tw.data(), 0);
+  // the accessor form (first pass reads the input array, last pass writes the
+  // output array) must give the same bits
+  SmemLd<T, B> ld{in2.data()};
+  SmemSt<T, B> st{out2.data()};
+  if (sign > 0)
+    cfft_io<T, B, N, 1, 1>(ld, st, c0.data(), c1.data(), tw.data(), 0);
+  else
+    cfft_io<T, B, N, -1, 1>(ld, st, c0.data(), c1.data(), tw.data(), 0);
   for (size_t i = 0; i < B * (size_t)N; ++i) {
+    if (memcmp(&out2[i], &res[i], sizeof(V)) != 0) return -2;
     out[2 * i] = (double)res[i].x;
     out[2 * i + 1] = (double)res[i].y;
   }

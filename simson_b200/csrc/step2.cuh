@@ -46,41 +46,51 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) 
   const size_t slot = (size_t)g.nyp * g.NP;
   // fine-grid fields: 0 u, 1 v, 2 w, 3 omega_x, 4 omega_y, 5 omega_z
   const int src_slot[6] = {0, 1, 2, 3, -1, 4};
-  for (int f = 0; f < 6; ++f) {
-    // two loads in flight per thread; a full unroll of the fixed-length loop
-    // costs occupancy (measured)
-#pragma unroll(N > 0 ? 2 : 1)
-    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
-      const int m = t / KB;
-      const int b = t - m * KB;
-      const int kx = kx0 + b;
-      int iz = -1;
-      if (m < nzh)
-        iz = m;
-      else if (m > nzp - nzh)
-        iz = m - (nzp - g.nz);
-      V val = V{(T)0, (T)0};
-      if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
-        const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
-        if (f == 4) {
-          const auto u = st[off];
-          const auto w = st[2 * slot + off];
-          const double a = alfa[kx], be = beta[iz];
-          val = V{(T)(-be * (double)u.y + a * (double)w.y), (T)(be * (double)u.x - a * (double)w.x)};
-        } else {
-          const auto q = st[src_slot[f] * slot + off];
-          val = V{(T)q.x, (T)q.y};
-        }
+  // element m (padded z index) of column b of field f
+  auto load_elem = [&](int f, int m, int b) -> V {
+    const int kx = kx0 + b;
+    int iz = -1;
+    if (m < nzh)
+      iz = m;
+    else if (m > nzp - nzh)
+      iz = m - (nzp - g.nz);
+    V val = V{(T)0, (T)0};
+    if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
+      const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
+      if (f == 4) {
+        const auto u = st[off];
+        const auto w = st[2 * slot + off];
+        const double a = alfa[kx], be = beta[iz];
+        val = V{(T)(-be * (double)u.y + a * (double)w.y), (T)(be * (double)u.x - a * (double)w.x)};
+      } else {
+        const auto q = st[src_slot[f] * slot + off];
+        val = V{(T)q.x, (T)q.y};
       }
-      b0[t] = val;
     }
-    __syncthreads();
-    V* res = fft_any<T, KB, N, NT, 1>(b0, b1, plan, tw);
-    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
-      const int m = t / KB;
-      const int b = t - m * KB;
-      const int kx = kx0 + b;
-      if (kx < g.nx2) zb[(((size_t)f * g.nyp + y) * nzp + m) * g.nx2 + kx] = res[t];
+    return val;
+  };
+  for (int f = 0; f < 6; ++f) {
+    V* __restrict__ out = zb + ((size_t)f * g.nyp + y) * nzp * g.nx2;
+    if constexpr (N > 0) {
+      // the first pass reads the state, the last writes zb: shared memory
+      // only between passes
+      cfft_io<T, KB, N, 1, NT>([&](int m, int b) { return load_elem(f, m, b); },
+                               [&](int m, int b, V v) {
+                                 if (kx0 + b < g.nx2) out[(size_t)m * g.nx2 + kx0 + b] = v;
+                               },
+                               b0, b1, tw, threadIdx.x);
+    } else {
+      for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
+        const int m = t / KB;
+        b0[t] = load_elem(f, m, t - m * KB);
+      }
+      __syncthreads();
+      V* res = fft_any<T, KB, N, NT, 1>(b0, b1, plan, tw);
+      for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
+        const int m = t / KB;
+        const int kx = kx0 + (t - m * KB);
+        if (kx < g.nx2) out[(size_t)m * g.nx2 + kx] = res[t];
+      }
     }
     __syncthreads();
   }
@@ -237,21 +247,11 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   const size_t fs = (size_t)g.nyp * nzp * g.nx2;
   const size_t slot = (size_t)g.nyp * g.NP;
   for (int f = 0; f < 3; ++f) {
-    for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
-      const int m = t / KB;
-      const int b = t - m * KB;
+    const V* __restrict__ in = xb + f * fs + (size_t)y * nzp * g.nx2;
+    // mode iz of column b (padded index m) into state slot f; the kx = kz = 0
+    // mode of H2 gets the mean-mean product in FP64
+    auto store = [&](int iz, int b, V h) {
       const int kx = kx0 + b;
-      b0[t] = (kx < g.nx2) ? xb[f * fs + ((size_t)y * nzp + m) * g.nx2 + kx] : V{(T)0, (T)0};
-    }
-    __syncthreads();
-    V* res = fft_any<T, KB, N, NT, -1>(b0, b1, plan, tw);
-    for (int t = threadIdx.x; t < g.nz * KB; t += nthr) {
-      const int iz = t / KB;
-      const int b = t - iz * KB;
-      const int kx = kx0 + b;
-      if (kx >= g.nx2) continue;
-      const int m = (iz < nzh) ? iz : iz + (nzp - g.nz);
-      const V h = res[m * KB + b];
       double hx = (double)h.x, hy = (double)h.y;
       if (mean != nullptr && f == 1 && iz == 0 && kx == 0) {
         const double U = mean[0 * g.nyp + y], W = mean[1 * g.nyp + y];
@@ -259,6 +259,34 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
         hx += (double)g.nxp * (double)g.nzp * (W * Ox - U * Oz);
       }
       st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = typename C2<S>::type{(S)hx, (S)hy};
+    };
+    if constexpr (N > 0) {
+      cfft_io<T, KB, N, -1, NT>(
+          [&](int m, int b) { return (kx0 + b < g.nx2) ? in[(size_t)m * g.nx2 + kx0 + b] : V{(T)0, (T)0}; },
+          [&](int m, int b, V v) {
+            // keep the nz stored modes (truncation folded into the store)
+            if (kx0 + b >= g.nx2) return;
+            if (m < nzh)
+              store(m, b, v);
+            else if (m >= nzp - nzh)
+              store(m - (nzp - g.nz), b, v);
+          },
+          b0, b1, tw, threadIdx.x);
+    } else {
+      for (int t = threadIdx.x; t < nzp * KB; t += nthr) {
+        const int m = t / KB;
+        const int kx = kx0 + (t - m * KB);
+        b0[t] = (kx < g.nx2) ? in[(size_t)m * g.nx2 + kx] : V{(T)0, (T)0};
+      }
+      __syncthreads();
+      V* res = fft_any<T, KB, N, NT, -1>(b0, b1, plan, tw);
+      for (int t = threadIdx.x; t < g.nz * KB; t += nthr) {
+        const int iz = t / KB;
+        const int b = t - iz * KB;
+        if (kx0 + b >= g.nx2) continue;
+        const int m = (iz < nzh) ? iz : iz + (nzp - g.nz);
+        store(iz, b, res[m * KB + b]);
+      }
     }
     __syncthreads();
   }
