@@ -508,6 +508,19 @@ SB_HD __forceinline__ void cfft_io(Ld ld, St st, typename C2<T>::type* buf0, typ
   }
 }
 
+// First pass from ld, the others in shared memory; returns the buffer that
+// holds the result (ends with a barrier on the device).
+template <class T, int B, int N, int S, int NT, class Ld>
+SB_HD __forceinline__ typename C2<T>::type* cfft_ld(Ld ld, typename C2<T>::type* buf0, typename C2<T>::type* buf1,
+                                                    const typename C2<T>::type* __restrict__ tw, int t0) {
+  constexpr CPlanData pl = cplan_make(N);
+  cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT>(ld, SmemSt<T, B>{buf0}, tw, t0);
+#ifdef __CUDA_ARCH__
+  __syncthreads();
+#endif
+  return cfft<T, B, N, S, NT, 1>(buf0, buf1, tw, t0);
+}
+
 // runtime plan (N == 0) or compile-time plan, same interface
 template <class T, int B, int N, int NT, int S>
 __device__ __forceinline__ typename C2<T>::type* fft_any(typename C2<T>::type* buf0, typename C2<T>::type* buf1,

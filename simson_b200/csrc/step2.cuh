@@ -116,10 +116,9 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   V* bB = bA + (size_t)n * B;
   const int y = blockIdx.y;
   const int m0 = blockIdx.x * RB;
-  // Hermitian completion of two half spectra into one complex spectrum
-  for (int t = threadIdx.x; t < n * B; t += nthr) {
-    const int k = t / B;
-    const int c = t - k * B;
+  // Hermitian completion of two half spectra into one complex spectrum:
+  // element k of column c = 3 r + q (row m0 + r, fields 2q and 2q+1)
+  auto herm = [&](int k, int c) -> V {
     const int r = c / 3, q = c - 3 * (c / 3);
     const int m = m0 + r;
     V z = V{(T)0, (T)0};
@@ -137,10 +136,20 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
         z = V{a.x + b.y, b.x - a.y};
       }
     }
-    bA[t] = z;
+    return z;
+  };
+  V* res;
+  if constexpr (N > 0) {
+    // the first inverse pass reads the spectra itself
+    res = cfft_ld<T, B, N, 1, NT>(herm, bA, bB, tw, threadIdx.x);
+  } else {
+    for (int t = threadIdx.x; t < n * B; t += nthr) {
+      const int k = t / B;
+      bA[t] = herm(k, t - k * B);
+    }
+    __syncthreads();
+    res = fft_any<T, B, N, NT, 1>(bA, bB, plan, tw);
   }
-  __syncthreads();
-  V* res = fft_any<T, B, N, NT, 1>(bA, bB, plan, tw);
   V* oth = (res == bA) ? bB : bA;
   // products in physical space, H into (H1 + i H2) per row and, for an even
   // number of rows, the H3 of rows 2q and 2q+1 paired as H3 + i H3' (one
