@@ -12,7 +12,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libsimson_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "simson.cu"), os.path.join(HERE, "csrc", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "simson.cu"), os.path.join(HERE, "csrc", "noalloc.cu"),
+           os.path.join(HERE, "csrc", "mixed.cu")]
+# units built with fused multiply-add contraction (the mixed-precision path)
+FMAD_SOURCES = {os.path.join(HERE, "csrc", "mixed.cu")}
 DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "simson_b200.h")]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
@@ -40,12 +43,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
     # arithmetic (gfortran/gcc for x86-64) rounds every product, and the stiff
     # tau solves (lambda ~ 1e6) amplify the difference between fused and
     # separate rounding to ~1e-12.  Set SIMSON_FMAD=1 to allow contraction.
-    fmad = "true" if os.environ.get("SIMSON_FMAD") == "1" else "false"
-    cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", f"-fmad={fmad}", "-Xcompiler", "-fPIC", "-shared",
-           "--expt-relaxed-constexpr", "-o", LIB + ".tmp"] + SOURCES
+    # The mixed-precision unit is built with contraction (it is checked
+    # against the FP64 path at 1e-5, not bit for bit).
+    fmad_all = os.environ.get("SIMSON_FMAD") == "1"
+    objs = []
+    procs = []
+    for src in SOURCES:
+        fmad = "true" if (fmad_all or src in FMAD_SOURCES) else "false"
+        obj = os.path.join(LIB_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+        cmd = [nvcc(), ARCH, "-O3", "-lineinfo", "-std=c++17", f"-fmad={fmad}", "-Xcompiler", "-fPIC",
+               "--expt-relaxed-constexpr", "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    if any(p.wait() != 0 for p in procs):
+        raise subprocess.CalledProcessError(1, "nvcc")
+    cmd = [nvcc(), ARCH, "-shared", "-o", LIB + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    for o in objs:
+        os.remove(o)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

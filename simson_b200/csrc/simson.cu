@@ -20,6 +20,8 @@
 #include "les_filter.h"
 #include "les_dyn.cuh"
 #include "sgs_mlp.cuh"
+#include "mixed.h"
+#include "step2_launch.cuh"
 #include "cheb_tc.cuh"
 
 using namespace sb;
@@ -107,7 +109,7 @@ struct sgpu_ctx {
   // threads per CTA of the FFT kernels (measured on B200: 256 everywhere but
   // the FP64 x-pass, whose register use prefers 128)
   static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 256, xpass64_threads = 128;
-  static constexpr int kbf = 4, rbf = 2, pbf = 8;  // FP32 tiles (measured: 4 z-columns beat 8)
+  static constexpr int kbf = MIXED_KB, rbf = MIXED_RB, pbf = 8;  // FP32 tiles (mixed.h)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
   std::vector<cudaEvent_t> pev;
@@ -624,92 +626,6 @@ static void enqueue_sgs(sgpu_ctx* c) {
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 6), fld, c->les_gu, fld, 3, 1, 1.0, 0, c->twy.d);
 }
 
-// Transform lengths with compile-time FFT plans (fft.cuh cfft): the
-// production grid's 576 (3/2 x 384) and the test, LES and channel grids' 3/2
-// lengths; any other length takes the runtime plan.
-#define SB_FIXED_LENGTHS(X) X(72) X(96) X(240) X(288) X(576)
-
-// threads per CTA for B columns of an N-point compile-time transform: one
-// butterfly per thread in the widest pass (halved while above 512), a
-// multiple of 32
-constexpr int fixed_threads(int n, int b) {
-  int items = cplan_max_nb(n) * b;
-  while (items > 512) items = (items + 1) / 2;
-  return ((items + 31) / 32) * 32;
-}
-
-template <class T, int KB, class S, int N, int NT>
-static void zinv_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<S>::type* in,
-                   typename C2<T>::type* zb, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
-                   const double* alfa, const double* beta, int drop) {
-  cudaFuncSetAttribute(k_zinv<T, KB, S, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zinv<T, KB, S, N, NT><<<grid, NT, smem, st>>>(in, zb, g, plan, tw, alfa, beta, drop);
-}
-template <class T, int KB, class S>
-static void launch_zinv(dim3 grid, size_t smem, cudaStream_t st, const typename C2<S>::type* in,
-                        typename C2<T>::type* zb, const Dims& g, const FFTPlan& plan,
-                        const typename C2<T>::type* tw, const double* alfa, const double* beta, int drop) {
-  switch (g.nzp) {
-#define SB_CASE(n)                                                                                 \
-  case n:                                                                                          \
-    zinv_n<T, KB, S, n, fixed_threads(n, KB)>(grid, smem, st, in, zb, g, plan, tw, alfa, beta, drop); \
-    return;
-    SB_FIXED_LENGTHS(SB_CASE)
-#undef SB_CASE
-    default:
-      zinv_n<T, KB, S, 0, sgpu_ctx::fft_threads>(grid, smem, st, in, zb, g, plan, tw, alfa, beta, drop);
-  }
-}
-
-template <class T, int KB, class S, int N, int NT>
-static void zfwd_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* xb,
-                   typename C2<S>::type* out, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
-                   const double* mean, double rot) {
-  cudaFuncSetAttribute(k_zfwd<T, KB, S, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zfwd<T, KB, S, N, NT><<<grid, NT, smem, st>>>(xb, out, g, plan, tw, mean, rot);
-}
-template <class T, int KB, class S>
-static void launch_zfwd(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* xb,
-                        typename C2<S>::type* out, const Dims& g, const FFTPlan& plan,
-                        const typename C2<T>::type* tw, const double* mean, double rot) {
-  switch (g.nzp) {
-#define SB_CASE(n)                                                                          \
-  case n:                                                                                   \
-    zfwd_n<T, KB, S, n, fixed_threads(n, KB)>(grid, smem, st, xb, out, g, plan, tw, mean, rot); \
-    return;
-    SB_FIXED_LENGTHS(SB_CASE)
-#undef SB_CASE
-    default:
-      zfwd_n<T, KB, S, 0, sgpu_ctx::fft_threads>(grid, smem, st, xb, out, g, plan, tw, mean, rot);
-  }
-}
-
-template <class T, int RB, int N, int NT>
-static void xpass_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
-                    typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
-                    const double* dyi, double dxi, double dzi, double rot, unsigned long long* cfl,
-                    const double* mean) {
-  cudaFuncSetAttribute(k_xpass<T, RB, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_xpass<T, RB, N, NT><<<grid, NT, smem, st>>>(zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
-}
-template <class T, int RB, int NT0>
-static void launch_xpass(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
-                         typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan,
-                         const typename C2<T>::type* tw, const double* dyi, double dxi, double dzi, double rot,
-                         unsigned long long* cfl, const double* mean) {
-  switch (g.nxp) {
-#define SB_CASE(n)                                                                                        \
-  case n:                                                                                                 \
-    xpass_n<T, RB, n, fixed_threads(n, 3 * RB)>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, \
-                                                mean);                                                    \
-    return;
-    SB_FIXED_LENGTHS(SB_CASE)
-#undef SB_CASE
-    default:
-      xpass_n<T, RB, 0, NT0>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
-  }
-}
-
 static int enqueue_nonlin(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
@@ -740,15 +656,12 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     // the FFTs carry only the perturbations; the mean profiles enter the
     // products analytically and their mean-mean product in FP64
     prof_mark(c, K_ZINV);
-    k_mean_profiles<float><<<(g.nyp + 127) / 128, 128, 0, c->stream>>>(c->stf, c->meanp, g);
-    launch_zinv<float, sgpu_ctx::kbf, float>(gzf, s_zf, c->stream, c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa,
-                                             c->beta, 1);
+    mixed_mean_profiles(c->stream, c->stf, c->meanp, g);
+    mixed_zinv(c->stream, gzf, s_zf, c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta);
     prof_mark(c, K_XPASS);
-    launch_xpass<float, sgpu_ctx::rbf, sgpu_ctx::fft_threads>(gxf, s_xf, c->stream, zbf, xbf, g, c->twx.plan,
-                                                              c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
+    mixed_xpass(c->stream, gxf, s_xf, zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
     prof_mark(c, K_ZFWD);
-    launch_zfwd<float, sgpu_ctx::kbf, float>(gzf, s_zf, c->stream, xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp,
-                                             P.rot);
+    mixed_zfwd(c->stream, gzf, s_zf, xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp, P.rot);
     c->launches++;
   } else {
     prof_mark(c, K_ZINV);
@@ -810,14 +723,14 @@ static int enqueue_linear(sgpu_ctx* c) {
   if (c->prof) {
     prof_mark(c, K_MEAN);
     if (c->mixed)
-      k_mean<float2><<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
+      mixed_mean(c->stream, M, g, P.re, rk);
     else
       k_mean<double2><<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
   } else {
     cudaEventRecord(c->fork, c->stream);
     cudaStreamWaitEvent(c->side, c->fork, 0);
     if (c->mixed)
-      k_mean<float2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
+      mixed_mean(c->side, M, g, P.re, rk);
     else
       k_mean<double2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
     cudaEventRecord(c->join, c->side);
@@ -835,8 +748,8 @@ static int enqueue_linear(sgpu_ctx* c) {
     c->hom_key[hs] = anbn;
     prof_mark(c, K_OTHER);
     if (c->mixed)
-      k_pencil_hom<double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
-          B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP);
+      mixed_pencil_hom(c->stream, B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld,
+                       c->hom_s + hs * 2 * (size_t)g.NP);
     else
       k_pencil_hom<double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
           B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP);
@@ -846,8 +759,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   const double* hsc = c->hom_s + hs * 2 * (size_t)g.NP;
   prof_mark(c, K_PENCIL);
   if (c->mixed)
-    k_pencil<float2, double, float><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
-                                                                               vhc, hsc);
+    mixed_pencil(c->stream, B, g, c->alfa, c->beta, P.re, rk, vhc, hsc);
   else
     k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
                                                                                  vhc, hsc);

@@ -737,7 +737,7 @@ struct PrhsBufs {
   double *puw;
 };
 
-__global__ void k_prhs(PrhsBufs B, Dims g, const double* __restrict__ alfa, const double* __restrict__ beta,
+static __global__ void k_prhs(PrhsBufs B, Dims g, const double* __restrict__ alfa, const double* __restrict__ beta,
                        double re, double an) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
