@@ -46,30 +46,33 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) 
   const size_t slot = (size_t)g.nyp * g.NP;
   // fine-grid fields: 0 u, 1 v, 2 w, 3 omega_x, 4 omega_y, 5 omega_z
   const int src_slot[6] = {0, 1, 2, 3, -1, 4};
-  // element m (padded z index) of column b of field f
-  auto load_elem = [&](int f, int m, int b) -> V {
-    const int kx = kx0 + b;
-    int iz = -1;
-    if (m < nzh)
-      iz = m;
-    else if (m > nzp - nzh)
-      iz = m - (nzp - g.nz);
-    V val = V{(T)0, (T)0};
-    if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
-      const size_t off = (size_t)y * g.NP + (size_t)iz * g.nx2 + kx;
-      if (f == 4) {
-        const auto u = st[off];
-        const auto w = st[2 * slot + off];
-        const double a = alfa[kx], be = beta[iz];
-        val = V{(T)(-be * (double)u.y + a * (double)w.y), (T)(be * (double)u.x - a * (double)w.x)};
-      } else {
-        const auto q = st[src_slot[f] * slot + off];
-        val = V{(T)q.x, (T)q.y};
-      }
-    }
-    return val;
-  };
+  typedef typename C2<S>::type SV;
+  const SV* __restrict__ plane = st + (size_t)y * g.NP;  // this y-plane of slot 0
   for (int f = 0; f < 6; ++f) {
+    const SV* __restrict__ src = plane + (size_t)(f == 4 ? 0 : src_slot[f]) * slot;
+    // element m (padded z index) of column b of field f
+    auto load_elem = [&](int f, int m, int b) -> V {
+      const int kx = kx0 + b;
+      int iz = -1;
+      if (m < nzh)
+        iz = m;
+      else if (m > nzp - nzh)
+        iz = m - (nzp - g.nz);
+      V val = V{(T)0, (T)0};
+      if (iz >= 0 && kx < g.nx2 && !(drop_mean && iz == 0 && kx == 0)) {
+        const int off = iz * g.nx2 + kx;
+        if (f == 4) {
+          const SV u = src[off];
+          const SV w = src[2 * slot + off];
+          const double a = alfa[kx], be = beta[iz];
+          val = V{(T)(-be * (double)u.y + a * (double)w.y), (T)(be * (double)u.x - a * (double)w.x)};
+        } else {
+          const SV q = src[off];
+          val = V{(T)q.x, (T)q.y};
+        }
+      }
+      return val;
+    };
     V* __restrict__ out = zb + ((size_t)f * g.nyp + y) * nzp * g.nx2;
     if constexpr (N > 0) {
       // the first pass reads the state, the last writes zb: shared memory
@@ -118,21 +121,22 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   const int m0 = blockIdx.x * RB;
   // Hermitian completion of two half spectra into one complex spectrum:
   // element k of column c = 3 r + q (row m0 + r, fields 2q and 2q+1)
+  const size_t fstride = (size_t)g.nyp * g.nzp * g.nx2;                   // one field of zb
+  const V* __restrict__ zrow = zb + ((size_t)y * g.nzp + m0) * g.nx2;  // row m0 of field 0
   auto herm = [&](int k, int c) -> V {
-    const int r = c / 3, q = c - 3 * (c / 3);
-    const int m = m0 + r;
+    const int r = c / 3, q = c - 3 * r;
     V z = V{(T)0, (T)0};
-    if (m < g.nzp) {
-      const size_t f0 = (((size_t)(2 * q) * g.nyp + y) * g.nzp + m) * g.nx2;
-      const size_t f1 = (((size_t)(2 * q + 1) * g.nyp + y) * g.nzp + m) * g.nx2;
+    if (m0 + r < g.nzp) {
+      const V* __restrict__ p0 = zrow + (size_t)(2 * q) * fstride + r * g.nx2;
+      const V* __restrict__ p1 = p0 + fstride;
       if (k == 0) {
-        z = V{zb[f0].x, zb[f1].x};
+        z = V{p0[0].x, p1[0].x};
       } else if (k < g.nx2) {
-        const V a = zb[f0 + k], b = zb[f1 + k];
+        const V a = p0[k], b = p1[k];
         z = V{a.x - b.y, a.y + b.x};
       } else if (k > n - g.nx2) {
         const int kk = n - k;
-        const V a = zb[f0 + kk], b = zb[f1 + kk];
+        const V a = p0[kk], b = p1[kk];
         z = V{a.x + b.y, b.x - a.y};
       }
     }
@@ -220,11 +224,10 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
     }
     const V h1 = V{(a.x + b.x) * (T)0.5, (a.y - b.y) * (T)0.5};
     const V h2 = V{(a.y + b.y) * (T)0.5, (b.x - a.x) * (T)0.5};
-    const size_t o = ((size_t)y * g.nzp + m) * g.nx2 + k;
-    const size_t fs = (size_t)g.nyp * g.nzp * g.nx2;
-    xb[o] = h1;
-    xb[fs + o] = h2;
-    xb[2 * fs + o] = h3;
+    V* __restrict__ o = xb + ((size_t)y * g.nzp + m0) * g.nx2 + r * g.nx2 + k;
+    o[0] = h1;
+    o[fstride] = h2;
+    o[2 * fstride] = h3;
   }
   // block max of the CFL number
   for (int off = 16; off > 0; off >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
@@ -257,6 +260,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   const size_t slot = (size_t)g.nyp * g.NP;
   for (int f = 0; f < 3; ++f) {
     const V* __restrict__ in = xb + f * fs + (size_t)y * nzp * g.nx2;
+    typename C2<S>::type* __restrict__ dst = st + f * slot + (size_t)y * g.NP;
     // mode iz of column b (padded index m) into state slot f; the kx = kz = 0
     // mode of H2 gets the mean-mean product in FP64
     auto store = [&](int iz, int b, V h) {
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
         const double Ox = mean[2 * g.nyp + y], Oz = mean[3 * g.nyp + y] + 2.0 * rot;
         hx += (double)g.nxp * (double)g.nzp * (W * Ox - U * Oz);
       }
-      st[f * slot + (size_t)y * g.NP + (size_t)iz * g.nx2 + kx] = typename C2<S>::type{(S)hx, (S)hy};
+      dst[iz * g.nx2 + kx] = typename C2<S>::type{(S)hx, (S)hy};
     };
     if constexpr (N > 0) {
       cfft_io<T, KB, N, -1, NT>(
