@@ -159,9 +159,21 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   // number of rows, the H3 of rows 2q and 2q+1 paired as H3 + i H3' (one
   // complex FFT for two real rows); a single row keeps (H3 + 0i).  CFL.
   constexpr int B2 = (RB % 2 == 0) ? RB + RB / 2 : 2 * RB;
-  double cmax = 0.0;
-  const double dy = dyi[y];
+  // Plane means (mixed path): u, w, omega_x, omega_z are perturbations; the
+  // means U, W, Omega_x, Omega_z + 2 rot enter term by term so no product of
+  // two O(1) means is rounded here (their W Omega_x - U Omega_z goes to the
+  // kx = kz = 0 mode in FP64, in k_zfwd).  V = Omega_y = 0.  The CFL number
+  // is formed in T (FP64 path: exactly the reference's sum).
+  T U = (T)0, W = (T)0, Ox = (T)0, Oz = (T)0;
+  if (mean != nullptr) {
+    U = (T)mean[0 * g.nyp + y];
+    W = (T)mean[1 * g.nyp + y];
+    Ox = (T)mean[2 * g.nyp + y];
+    Oz = (T)(mean[3 * g.nyp + y] + 2.0 * rot);
+  }
   const T r2 = (T)(2.0 * rot);
+  const T cx = (T)dxi, cy = (T)dyi[y], cz = (T)dzi;
+  T cmaxt = (T)0;
   for (int t = threadIdx.x; t < n * RB; t += nthr) {
     const int j = t / RB;
     const int r = t - j * RB;
@@ -170,23 +182,14 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
     const V z2 = res[j * B + 3 * r + 2];
     const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
     T h1, h2, h3;
-    double ut = (double)u, wt = (double)w;
     if (mean == nullptr) {
       h1 = v * (oz + r2) - w * oy;
       h2 = w * ox - u * (oz + r2);
       h3 = u * oy - v * ox;
     } else {
-      // u, w, omega_x, omega_z are perturbations; the plane means U, W,
-      // Omega_x, Omega_z + 2 rot enter term by term so no product of two
-      // O(1) means is rounded here (their W Omega_x - U Omega_z goes to the
-      // kx = kz = 0 mode in FP64, in k_zfwd).  V = Omega_y = 0.
-      const T U = (T)mean[0 * g.nyp + y], W = (T)mean[1 * g.nyp + y];
-      const T Ox = (T)mean[2 * g.nyp + y], Oz = (T)(mean[3 * g.nyp + y] + 2.0 * rot);
       h1 = v * Oz + (v * oz - (W + w) * oy);
       h2 = (W * ox + w * Ox - U * oz - u * Oz) + (w * ox - u * oz);
       h3 = U * oy - v * Ox + (u * oy - v * ox);
-      ut += mean[0 * g.nyp + y];
-      wt += mean[1 * g.nyp + y];
     }
     if constexpr (RB % 2 == 0) {
       oth[j * B2 + r] = V{h1, h2};
@@ -197,10 +200,11 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
       oth[j * B2 + 2 * r + 1] = V{h3, (T)0};
     }
     if (m0 + r < g.nzp) {
-      const double cl = fabs(ut) * dxi + fabs((double)v) * dy + fabs(wt) * dzi;
-      cmax = fmax(cmax, cl);
+      const T cl = fabs(u + U) * cx + fabs(v) * cy + fabs(w + W) * cz;
+      cmaxt = fmax(cmaxt, cl);
     }
   }
+  double cmax = (double)cmaxt;
   __syncthreads();
   V* fres = fft_any<T, B2, N, NT, -1>(oth, res, plan, tw);
   for (int t = threadIdx.x; t < g.nx2 * RB; t += nthr) {
