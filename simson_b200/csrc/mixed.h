@@ -25,9 +25,9 @@ void mixed_xpass(cudaStream_t s, dim3 grid, size_t smem, const float2* zb, float
 void mixed_zfwd(cudaStream_t s, dim3 grid, size_t smem, const float2* xb, float2* stf, const Dims& g,
                 const FFTPlan& plan, const float2* tw, const double* meanp, double rot);
 void mixed_pencil_hom(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
-                      double re, double anbn, double* vh, double* hs);
+                      double re, double anbn, double* vh, double* hs, double* cf);
 void mixed_pencil(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
-                  double re, RKc rk, const double* vh, const double* hs);
+                  double re, RKc rk, const double* vh, const double* hs, double* cf);
 void mixed_mean(cudaStream_t s, const MeanArgs& M, const Dims& g, double re, RKc rk);
 
 }  // namespace sb

@@ -69,6 +69,7 @@ struct sgpu_ctx {
   // [3][nyp][NP], parity sums [3][2 NP], keyed by the stage's a_n + b_n
   double* hom_vh = nullptr;
   double* hom_s = nullptr;
+  double* hom_cf = nullptr;  // coefficient columns [3][4][nyp][NP] (k_pencil_hom)
   double hom_key[3] = {0.0, 0.0, 0.0};
   int hom_next = 0;
   double* mscr = nullptr;    // mean-flow scratch
@@ -298,6 +299,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->hom_vh, 3 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->hom_s, 3 * 2 * (size_t)g.NP * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_cf, 3 * 4 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->ampd, 20 * (size_t)g.nyp * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
@@ -374,7 +376,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
-                  c->mscr, c->hom_vh, c->hom_s, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
+                  c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 16; ++i)
@@ -749,20 +751,22 @@ static int enqueue_linear(sgpu_ctx* c) {
     prof_mark(c, K_OTHER);
     if (c->mixed)
       mixed_pencil_hom(c->stream, B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld,
-                       c->hom_s + hs * 2 * (size_t)g.NP);
+                       c->hom_s + hs * 2 * (size_t)g.NP, c->hom_cf + hs * 4 * fld);
     else
       k_pencil_hom<double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
-          B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP);
+          B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP,
+          c->hom_cf + hs * 4 * fld);
     c->launches++;
   }
   const double* vhc = c->hom_vh + hs * fld;
   const double* hsc = c->hom_s + hs * 2 * (size_t)g.NP;
+  double* cfc = c->hom_cf + hs * 4 * fld;
   prof_mark(c, K_PENCIL);
   if (c->mixed)
-    mixed_pencil(c->stream, B, g, c->alfa, c->beta, P.re, rk, vhc, hsc);
+    mixed_pencil(c->stream, B, g, c->alfa, c->beta, P.re, rk, vhc, hsc, cfc);
   else
     k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
-                                                                                 vhc, hsc);
+                                                                                 vhc, hsc, cfc);
   if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);

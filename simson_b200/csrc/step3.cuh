@@ -132,7 +132,11 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 // side assembled row by row never goes through memory; f[] is then unused.
 struct NoPre {};
 
-template <int M, class S = double, class FS = S, bool FAST = false, class Pre = NoPre>
+//
+// CPC: cp (and, for the reference order, wt) already hold this lam's
+// coefficients, written by an earlier solve with the same lam and n: the
+// backward sweep computes them in registers as always but does not store them.
+template <int M, class S = double, class FS = S, bool FAST = false, bool CPC = false, class Pre = NoPre>
 SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S* bc1, const S* bc2, ColT<S> cp,
                      ColT<S> wt, S (*dsum)[2] = nullptr, Pre pre = Pre()) {
   constexpr bool HOOK = !std::is_same<Pre, NoPre>::value;
@@ -175,9 +179,9 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       const int m = i - 2;  // factor row m (trid.f: d(m) = 1/(d(m) - c(m+2) e(m)))
       dinv = (i >= n - 3) ? (S)1.0 / tau_d(m, lam) : (S)1.0 / (tau_d(m, lam) - q2 * tau_e(m, lam));
       cnew = tau_c(m, lam) * dinv;
-      cpp[(size_t)(m - 1) * cs] = cnew;
+      if (!CPC) cpp[(size_t)(m - 1) * cs] = cnew;
       wnew = (i >= n - 3) ? (S)1.0 - tau_c(i, lam) : (S)1.0 - q2 * w2;
-      if (!FAST) wtp[(size_t)(i - 1) * ws] = wnew;
+      if (!FAST && !CPC) wtp[(size_t)(i - 1) * ws] = wnew;
     }
     const S di = (S)i;
     const S ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
@@ -245,8 +249,10 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     w1 = wnew;
   }
   // c'(n-3), c'(n-2) are the unscaled c (d = 1 in the truncated rows)
-  cpp[(size_t)(n - 4) * cs] = tau_c(n - 3, lam);
-  cpp[(size_t)(n - 3) * cs] = tau_c(n - 2, lam);
+  if (!CPC) {
+    cpp[(size_t)(n - 4) * cs] = tau_c(n - 3, lam);
+    cpp[(size_t)(n - 3) * cs] = tau_c(n - 2, lam);
+  }
   if (FAST) {
     // after the sweep q1 = c'(1), q2 = c'(2), w1 = W(3), w2 = W(4)
     const S d1 = (S)1.0 / ((S)1.0 - q1 * w1);
@@ -405,10 +411,14 @@ struct RKc {
 //   VHc: v_h, n x NP (row-major in y like the fields); HS[2p + s]: FAST: the
 //   parity sums dsum of v_h; FP64 path: sum over j = s, s+2, ... of (D v_h)_j
 //   in ascending order (the reference's order).
+//   CF: the coefficient columns of both solves for this stage (c' and the
+//   weights W of the lam solve, c' and W of the v solve; W only for the FP64
+//   path), 4 x (n x NP), read back by k_pencil instead of being rewritten.
 template <class SC, class FC>
 __global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                     const double* __restrict__ beta, double re, double anbn,
-                                                    double* __restrict__ VHc, double* __restrict__ HS) {
+                                                    double* __restrict__ VHc, double* __restrict__ HS,
+                                                    double* __restrict__ CF) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
   const int kx = p % g.nx2;
@@ -421,16 +431,17 @@ __global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const 
   const double lam = k2 + 2.0 * re / anbn;
   constexpr bool FAST = !std::is_same<FC, double>::value;
   const ColT<SC> ph{reinterpret_cast<SC*>(B.PHIH) + p, NP};
+  const size_t fr = (size_t)n * NP;
   {
     const ColT<FC> f[1] = {ColT<FC>{nullptr, 0}};
     const SC one[1] = {1};
-    tau_solve<1, SC, FC, FAST>((SC)lam, n, f, &ph, one, one, ColT<SC>{reinterpret_cast<SC*>(B.CPL) + p, NP},
-                               ColT<SC>{reinterpret_cast<SC*>(B.WTL) + p, NP});
+    tau_solve<1, SC, FC, FAST>((SC)lam, n, f, &ph, one, one, ColT<SC>{reinterpret_cast<SC*>(CF) + p, NP},
+                               ColT<SC>{reinterpret_cast<SC*>(CF + fr) + p, NP});
   }
   const Col vh{VHc + p, NP};
   double dsum[1][2] = {{0, 0}};
   const double b0[1] = {0};
-  tau_solve<1, double, SC, FAST>(k2, n, &ph, &vh, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
+  tau_solve<1, double, SC, FAST>(k2, n, &ph, &vh, b0, b0, Col{CF + 2 * fr + p, NP}, Col{CF + 3 * fr + p, NP}, dsum);
   if (FAST) {
     HS[2 * (size_t)p] = dsum[0][0];
     HS[2 * (size_t)p + 1] = dsum[0][1];
@@ -457,7 +468,8 @@ __global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const 
 template <class IO, class SC, class FC>
 __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                 const double* __restrict__ beta, double re, RKc rk,
-                                                const double* __restrict__ VHc, const double* __restrict__ HS) {
+                                                const double* __restrict__ VHc, const double* __restrict__ HS,
+                                                double* __restrict__ CF) {
   typedef typename C2<SC>::type SC2;
   typedef typename C2<FC>::type FC2;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -536,7 +548,6 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
   {
     auto cre = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p, 2 * NP}; };
     auto cim = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
-    auto crl = [&](double* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + p, NP}; };
     // rows n-1 and n-2 first; the solve asks for row i-3 at its row i
     SC fdummy[4];
     assemble(n - 1, fdummy);
@@ -544,13 +555,17 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
     const ColT<FC> f[4] = {};
     const ColT<SC> x[4] = {cre(B.PHI), cim(B.PHI), cre(B.OM), cim(B.OM)};
     const SC bc0[4] = {0, 0, 0, 0};
-    tau_solve<4, SC, FC, FAST>((SC)lam, n, f, x, bc0, bc0, crl(B.CPL), crl(B.WTL), nullptr,
-                               [&](int i, SC* fr) { assemble(i - 3, fr); });
+    // coefficient columns of this stage from k_pencil_hom (same lam, same n)
+    const size_t fr = (size_t)n * NP;
+    tau_solve<4, SC, FC, FAST, true>((SC)lam, n, f, x, bc0, bc0, ColT<SC>{reinterpret_cast<SC*>(CF) + p, NP},
+                                     ColT<SC>{reinterpret_cast<SC*>(CF + fr) + p, NP}, nullptr,
+                                     [&](int i, SC* fo) { assemble(i - 3, fo); });
     // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
     const ColT<SC> fv[2] = {cre(B.PHI), cim(B.PHI)};
     const Col xv[2] = {col_re(B.V, p, NP), col_im(B.V, p, NP)};
     const double b0[2] = {0, 0};
-    tau_solve<2, double, SC, FAST>(k2, n, fv, xv, b0, b0, col_r(B.CP, p, NP), col_r(B.WT, p, NP), dsum);
+    tau_solve<2, double, SC, FAST, true>(k2, n, fv, xv, b0, b0, Col{CF + 2 * fr + p, NP}, Col{CF + 3 * fr + p, NP},
+                                         dsum);
   }
   const double hs0 = HS[2 * (size_t)p], hs1 = HS[2 * (size_t)p + 1];
   double cvr[2], cvi[2];
