@@ -16,17 +16,20 @@
 //
 // One CTA (256 threads) owns 128 columns (the data is the A operand, M = 128,
 // columns as rows), the matrix is the B operand (N = 208 >= n output rows,
-// rows >= n zero), K = y in chunks of 16 (two MMA steps of 8) through a
-// two-stage shared-memory pipeline: while the tensor cores multiply chunk q,
-// one thread's bulk copy (cp.async.bulk, completing on an mbarrier) brings the
-// prepared matrix chunk q+1 (canonical K-major TF32 tiles, hi and lo, built on
-// the host) and all threads stage input chunk q+1 split into hi/lo TF32 (the
-// transpose to K-major happens in the 16-byte shared-memory stores).  One
-// thread issues the 3xTF32 MMAs and commits each chunk to that stage's
-// mbarrier; every wait is bounded.  Accumulator: 208 TMEM columns (lane = data
-// column, TMEM column = output row); the two warp groups split the output rows
-// in the epilogue, and a warp's stores of one output row cover 32 consecutive
-// columns.  86 KB of shared memory and 256 TMEM columns: two CTAs per SM.
+// rows >= n zero), K = y in chunks of 16 (two MMA steps of 8).  The prepared
+// matrix chunks (canonical K-major TF32 tiles, hi and lo, built on the host)
+// arrive by one thread's bulk copies (cp.async.bulk, completing on an
+// mbarrier) into a three-stage ring, issued two chunks ahead, so their L2
+// latency is hidden behind two chunks of work; the input chunks are split
+// into hi/lo TF32 by all threads into a two-stage ring (the transpose to
+// K-major happens in the 16-byte shared-memory stores), loaded into
+// registers one chunk ahead.  One thread issues the 3xTF32 MMAs and commits
+// each chunk to an mbarrier; every wait is bounded, and on every exit the
+// copies and MMAs in flight are waited for (bounded) before TMEM is freed.
+// Accumulator: 208 TMEM columns (lane = data column, TMEM column = output
+// row); the two warp groups split the output rows in the epilogue, and a
+// warp's stores of one output row cover 32 consecutive columns.  110 KB of
+// shared memory and 256 TMEM columns: two CTAs per SM.
 #pragma once
 #include "sgs_mlp.cuh"
 
@@ -39,8 +42,11 @@ constexpr int CHB_SBO = (CHB_KC / 4) * 128;                   // bytes between 8
 constexpr int CHB_A_BYTES = CHB_MROWS * CHB_KC * 4;           // one TF32 tile of the matrix
 constexpr int CHB_B_BYTES = CHB_TILE * CHB_KC * 4;            // one TF32 tile of the input
 constexpr int CHB_CHUNK_BYTES = 2 * CHB_A_BYTES;              // hi + lo matrix tiles per chunk
-constexpr int CHB_STAGE = 2 * CHB_A_BYTES + 2 * CHB_B_BYTES;  // matrix hi, lo; data hi, lo
-constexpr int CHB_SMEM = 2 * CHB_STAGE + 64;
+constexpr int CHB_MSTAGES = 3;                                // matrix ring
+constexpr int CHB_DSTAGE = 2 * CHB_B_BYTES;                   // data hi, lo
+constexpr int CHB_DATA0 = CHB_MSTAGES * CHB_CHUNK_BYTES;      // offset of the two data stages
+constexpr int CHB_BARS = CHB_DATA0 + 2 * CHB_DSTAGE;          // offset of the mbarriers
+constexpr int CHB_SMEM = CHB_BARS + 64;
 constexpr int CHB_TMEM_COLS = 256;                            // 208 used
 // byte offset of (row r, k) in a canonical K-major TF32 tile with CHB_KC columns
 SB_HD __forceinline__ int chb_canon(int r, int k) { return (r >> 3) * CHB_SBO + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4; }
@@ -125,22 +131,23 @@ __device__ __forceinline__ void chb_store_input(const float (&x)[CHB_ITEMS][4], 
 
 __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  // stage s: matrix hi | matrix lo | data hi | data lo
-  auto Mhi = [&](int s) { return sm + s * CHB_STAGE; };
-  auto Dhi = [&](int s) { return sm + s * CHB_STAGE + 2 * CHB_A_BYTES; };
-  auto Dlo = [&](int s) { return sm + s * CHB_STAGE + 2 * CHB_A_BYTES + CHB_B_BYTES; };
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + 2 * CHB_STAGE);  // full[2], done[2]
-  unsigned* tslot = reinterpret_cast<unsigned*>(sm + 2 * CHB_STAGE + 32);
+  // matrix stage m (hi | lo) at m * CHB_CHUNK_BYTES; data stage d (hi | lo)
+  auto Mhi = [&](int m) { return sm + m * CHB_CHUNK_BYTES; };
+  auto Dhi = [&](int d) { return sm + CHB_DATA0 + d * CHB_DSTAGE; };
+  auto Dlo = [&](int d) { return sm + CHB_DATA0 + d * CHB_DSTAGE + CHB_B_BYTES; };
+  // full[3] (matrix chunk arrived), done[2] (MMAs of a chunk complete)
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + CHB_BARS);
+  unsigned* tslot = reinterpret_cast<unsigned*>(sm + CHB_BARS + 48);
   __shared__ int s_fail;
   const int t = threadIdx.x, warp = t >> 5;
   const int f = blockIdx.y;
   const int c0 = blockIdx.x * CHB_TILE;
   const float* __restrict__ in = a.in + (size_t)f * a.in_fs;
   float* __restrict__ out = a.out + (size_t)f * a.out_fs;
-  const unsigned full0 = smem_u32(&bars[0]), done0 = smem_u32(&bars[2]);
+  const unsigned full0 = smem_u32(&bars[0]), done0 = smem_u32(&bars[3]);
   if (t == 0) {
     s_fail = 0;
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 5; ++i)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[i])), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -156,25 +163,40 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   const unsigned tmem = *tslot;
   constexpr unsigned IDESC = chb_idesc(CHB_TILE, CHB_MROWS);
   const int nch = a.nchunks;
-  auto par = [](int c) { return (unsigned)((c >> 1) & 1); };
-  // chunk 0 into stage 0; chunk 1's input into registers
+  // k-th use of matrix stage q % 3 (chunk q = m + 3k) completes phase k
+  auto mpar = [](int q) { return (unsigned)((q / CHB_MSTAGES) & 1); };
+  auto dpar = [](int q) { return (unsigned)((q >> 1) & 1); };
+  int issued = 0;  // matrix chunks whose bulk copy thread 0 issued
+  auto issue_matrix = [&](int q) {
+    if (t == 0 && q < nch) {
+      chb_bulk_load(smem_u32(Mhi(q % CHB_MSTAGES)), a.mat + (size_t)q * CHB_CHUNK_BYTES, CHB_CHUNK_BYTES,
+                    full0 + 8 * (q % CHB_MSTAGES));
+      issued = q + 1;
+    }
+  };
+  // matrix chunks 0 and 1 in flight, data chunk 0 staged, chunk 1 in registers
   float xr[CHB_ITEMS][4];
-  if (t == 0) chb_bulk_load(smem_u32(Mhi(0)), a.mat, CHB_CHUNK_BYTES, full0);
+  issue_matrix(0);
+  issue_matrix(1);
   chb_load_input(a, in, c0, 0, xr);
   chb_store_input(xr, Dhi(0), Dlo(0));
   if (nch > 1) chb_load_input(a, in, c0, 1, xr);
-  int last = -1;  // last committed chunk
+  int last = -1;      // last committed chunk
+  int consumed = 0;   // matrix chunks thread 0 has waited for
   for (int q = 0; q < nch; ++q) {
-    const int s = q & 1;
-    if (t == 0 && !mlp_wait(full0 + 8 * s, par(q), MLP_WAIT_LIMIT)) s_fail = 1;
+    const int ms = q % CHB_MSTAGES, ds = q & 1;
+    if (t == 0) {
+      if (!mlp_wait(full0 + 8 * ms, mpar(q), MLP_WAIT_LIMIT)) s_fail = 1;
+      else consumed = q + 1;
+    }
     async_proxy_fence();
     tc_fence_before();
     __syncthreads();
     if (s_fail) break;
     if (t == 0) {
       tc_fence_after();
-      const unsigned mh = smem_u32(Mhi(s)), ml = mh + CHB_A_BYTES;
-      const unsigned xh = smem_u32(Dhi(s)), xl = smem_u32(Dlo(s));
+      const unsigned mh = smem_u32(Mhi(ms)), ml = mh + CHB_A_BYTES;
+      const unsigned xh = smem_u32(Dhi(ds)), xl = smem_u32(Dlo(ds));
       for (int k = 0; k < CHB_KC / 8; ++k) {
         const unsigned ko = (unsigned)(k * 256);
         const unsigned long long ah = mlp_desc(xh + ko, 128, CHB_SBO), al = mlp_desc(xl + ko, 128, CHB_SBO);
@@ -183,26 +205,31 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
         chb_mma(tmem, ah, bl, IDESC, 1u);
         chb_mma(tmem, al, bh, IDESC, 1u);
       }
-      mlp_commit(done0 + 8 * s);
+      mlp_commit(done0 + 8 * ds);
     }
     last = q;
     if (q + 1 < nch) {
-      // the other stage is free once chunk q-1's MMAs are done
-      if (t == 0 && q >= 1 && !mlp_wait(done0 + 8 * (s ^ 1), par(q - 1), MLP_WAIT_LIMIT)) s_fail = 1;
+      // chunk q-1's MMAs done: its data stage (that of chunk q+1) and its
+      // matrix stage (that of chunk q+2) are free
+      if (t == 0 && q >= 1 && !mlp_wait(done0 + 8 * (ds ^ 1), dpar(q - 1), MLP_WAIT_LIMIT)) s_fail = 1;
       tc_fence_before();
       __syncthreads();
       if (s_fail) break;
       tc_fence_after();
-      if (t == 0)
-        chb_bulk_load(smem_u32(Mhi(s ^ 1)), a.mat + (size_t)(q + 1) * CHB_CHUNK_BYTES, CHB_CHUNK_BYTES, full0 + 8 * (s ^ 1));
-      // chunk q+1's input (loaded an iteration ago) into the free stage, then
-      // the loads of chunk q+2 stay in flight until the next iteration
-      chb_store_input(xr, Dhi(s ^ 1), Dlo(s ^ 1));
+      issue_matrix(q + 2);
+      // chunk q+1's input (loaded an iteration ago) into the free data stage,
+      // then the loads of chunk q+2 stay in flight until the next iteration
+      chb_store_input(xr, Dhi(ds ^ 1), Dlo(ds ^ 1));
       if (q + 2 < nch) chb_load_input(a, in, c0, q + 2, xr);
     }
   }
-  // all MMAs of the tile (they complete in order): the last chunk's barrier
-  if (t == 0 && last >= 0 && !mlp_wait(done0 + 8 * (last & 1), par(last), MLP_WAIT_LIMIT)) s_fail = 1;
+  // all MMAs of the tile (they complete in order): the last chunk's barrier;
+  // matrix copies still in flight (only after a failed wait): their barriers
+  if (t == 0) {
+    if (last >= 0 && !mlp_wait(done0 + 8 * (last & 1), dpar(last), MLP_WAIT_LIMIT)) s_fail = 1;
+    for (int q = consumed; q < issued; ++q)
+      if (!mlp_wait(full0 + 8 * (q % CHB_MSTAGES), mpar(q), MLP_WAIT_LIMIT)) s_fail = 1;
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
