@@ -16,20 +16,25 @@
 //
 // One CTA (256 threads) owns 128 columns (the data is the A operand, M = 128,
 // columns as rows), the matrix is the B operand (N = 208 >= n output rows,
-// rows >= n zero), K = y in chunks of 16 (two MMA steps of 8).  The prepared
-// matrix chunks (canonical K-major TF32 tiles, hi and lo, built on the host)
-// arrive by one thread's bulk copies (cp.async.bulk, completing on an
-// mbarrier) into a three-stage ring, issued two chunks ahead, so their L2
-// latency is hidden behind two chunks of work; the input chunks are split
-// into hi/lo TF32 by all threads into a two-stage ring (the transpose to
-// K-major happens in the 16-byte shared-memory stores), loaded into
-// registers one chunk ahead.  One thread issues the 3xTF32 MMAs and commits
-// each chunk to an mbarrier; every wait is bounded, and on every exit the
-// copies and MMAs in flight are waited for (bounded) before TMEM is freed.
-// Accumulator: 208 TMEM columns (lane = data column, TMEM column = output
-// row); the two warp groups split the output rows in the epilogue, and a
-// warp's stores of one output row cover 32 consecutive columns.  110 KB of
-// shared memory and 256 TMEM columns: two CTAs per SM.
+// rows >= n zero), K = y in chunks of 16 (two MMA steps of 8).  The warps
+// specialise during the main loop:
+//   * thread 0 issues the 3xTF32 MMAs of chunk q as soon as its matrix and
+//     data stages are full, commits them to the stages' "empty" mbarriers,
+//     and keeps the prepared matrix chunks (canonical K-major TF32 tiles, hi
+//     and lo, built on the host) two chunks ahead in a three-stage ring by
+//     bulk copies (cp.async.bulk, completing on a "full" mbarrier);
+//   * warps 4-7 stage the input: global loads two chunks ahead in
+//     registers, the split into hi/lo TF32 and the transpose to K-major in
+//     16-byte shared-memory stores into a two-stage ring, then arrive on the
+//     stage's "full" mbarrier (after a proxy fence);
+// so the tensor pipe sees chunk after chunk without a CTA-wide barrier in
+// the loop.  Every wait is bounded; after the loop one commit covers every
+// MMA issued, and every exit waits (bounded) for it and for the copies in
+// flight before TMEM is freed.  Accumulator: 208 TMEM columns (lane = data
+// column, TMEM column = output row); in the epilogue the two warp groups
+// split the output rows, a warp's stores of one output row cover 32
+// consecutive columns.  110 KB of shared memory and 256 TMEM columns: two
+// CTAs per SM, whose epilogues and main loops overlap.
 #pragma once
 #include "sgs_mlp.cuh"
 
@@ -46,7 +51,7 @@ constexpr int CHB_MSTAGES = 3;                                // matrix ring
 constexpr int CHB_DSTAGE = 2 * CHB_B_BYTES;                   // data hi, lo
 constexpr int CHB_DATA0 = CHB_MSTAGES * CHB_CHUNK_BYTES;      // offset of the two data stages
 constexpr int CHB_BARS = CHB_DATA0 + 2 * CHB_DSTAGE;          // offset of the mbarriers
-constexpr int CHB_SMEM = CHB_BARS + 64;
+constexpr int CHB_SMEM = CHB_BARS + 128;
 constexpr int CHB_TMEM_COLS = 256;                            // 208 used
 // byte offset of (row r, k) in a canonical K-major TF32 tile with CHB_KC columns
 SB_HD __forceinline__ int chb_canon(int r, int k) { return (r >> 3) * CHB_SBO + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4; }
@@ -91,16 +96,18 @@ __device__ __forceinline__ void chb_bulk_load(unsigned dst, const void* src, uns
                : "memory");
 }
 
-// Input chunk q (rows q*KC .. +KC of columns c0 .. c0+127): each thread
-// loads CHB_ITEMS groups of four rows of one column into registers, and later
-// stores them split into hi/lo TF32 (one 16-byte store per group and part).
-constexpr int CHB_ITEMS = CHB_TILE * (CHB_KC / 4) / 256;
+// Input chunk q (rows q*KC .. +KC of columns c0 .. c0+127): each of the 128
+// producer threads (pt) loads CHB_ITEMS groups of four rows of one column
+// into registers, and later stores them split into hi/lo TF32 (one 16-byte
+// store per group and part).
+constexpr int CHB_PRODUCERS = 128;
+constexpr int CHB_ITEMS = CHB_TILE * (CHB_KC / 4) / CHB_PRODUCERS;
 
 __device__ __forceinline__ void chb_load_input(const ChebTCArgs& a, const float* __restrict__ in, int c0, int q,
-                                               float (&x)[CHB_ITEMS][4]) {
+                                               int pt, float (&x)[CHB_ITEMS][4]) {
 #pragma unroll
   for (int k = 0; k < CHB_ITEMS; ++k) {
-    const int it = threadIdx.x + 256 * k;
+    const int it = pt + CHB_PRODUCERS * k;
     const int r = it % CHB_TILE;
     const int g4 = it / CHB_TILE;
     const int col = c0 + r;
@@ -112,11 +119,11 @@ __device__ __forceinline__ void chb_load_input(const ChebTCArgs& a, const float*
   }
 }
 
-__device__ __forceinline__ void chb_store_input(const float (&x)[CHB_ITEMS][4], unsigned char* Bhi,
+__device__ __forceinline__ void chb_store_input(const float (&x)[CHB_ITEMS][4], int pt, unsigned char* Bhi,
                                                 unsigned char* Blo) {
 #pragma unroll
   for (int k = 0; k < CHB_ITEMS; ++k) {
-    const int it = threadIdx.x + 256 * k;
+    const int it = pt + CHB_PRODUCERS * k;
     const int r = it % CHB_TILE;
     const int g4 = it / CHB_TILE;
     float4 hi, lo;
@@ -135,20 +142,23 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   auto Mhi = [&](int m) { return sm + m * CHB_CHUNK_BYTES; };
   auto Dhi = [&](int d) { return sm + CHB_DATA0 + d * CHB_DSTAGE; };
   auto Dlo = [&](int d) { return sm + CHB_DATA0 + d * CHB_DSTAGE + CHB_B_BYTES; };
-  // full[3] (matrix chunk arrived), done[2] (MMAs of a chunk complete)
+  // mbarriers: mfull[3], mempty[3], dfull[2], dempty[2], acc
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + CHB_BARS);
-  unsigned* tslot = reinterpret_cast<unsigned*>(sm + CHB_BARS + 48);
+  unsigned* tslot = reinterpret_cast<unsigned*>(sm + CHB_BARS + 96);
   __shared__ int s_fail;
   const int t = threadIdx.x, warp = t >> 5;
   const int f = blockIdx.y;
   const int c0 = blockIdx.x * CHB_TILE;
   const float* __restrict__ in = a.in + (size_t)f * a.in_fs;
   float* __restrict__ out = a.out + (size_t)f * a.out_fs;
-  const unsigned full0 = smem_u32(&bars[0]), done0 = smem_u32(&bars[3]);
+  const unsigned mfull0 = smem_u32(&bars[0]), mempty0 = smem_u32(&bars[3]);
+  const unsigned dfull0 = smem_u32(&bars[6]), dempty0 = smem_u32(&bars[8]), accb = smem_u32(&bars[10]);
   if (t == 0) {
     s_fail = 0;
-    for (int i = 0; i < 5; ++i)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[i])), "r"(1) : "memory");
+    for (int i = 0; i < 11; ++i) {
+      const unsigned cnt = (i == 6 || i == 7) ? (unsigned)CHB_PRODUCERS : 1u;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[i])), "r"(cnt) : "memory");
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -161,39 +171,31 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tslot;
-  constexpr unsigned IDESC = chb_idesc(CHB_TILE, CHB_MROWS);
   const int nch = a.nchunks;
-  // k-th use of matrix stage q % 3 (chunk q = m + 3k) completes phase k
+  // the k-th use of a stage (chunk q = stage + k * stages) completes phase k
   auto mpar = [](int q) { return (unsigned)((q / CHB_MSTAGES) & 1); };
   auto dpar = [](int q) { return (unsigned)((q >> 1) & 1); };
-  int issued = 0;  // matrix chunks whose bulk copy thread 0 issued
-  auto issue_matrix = [&](int q) {
-    if (t == 0 && q < nch) {
+  int issued = 0, consumed = 0;  // thread 0: matrix copies issued / waited for
+  if (t == 0) {
+    constexpr unsigned IDESC = chb_idesc(CHB_TILE, CHB_MROWS);
+    auto issue_matrix = [&](int q) {
       chb_bulk_load(smem_u32(Mhi(q % CHB_MSTAGES)), a.mat + (size_t)q * CHB_CHUNK_BYTES, CHB_CHUNK_BYTES,
-                    full0 + 8 * (q % CHB_MSTAGES));
+                    mfull0 + 8 * (q % CHB_MSTAGES));
       issued = q + 1;
-    }
-  };
-  // matrix chunks 0 and 1 in flight, data chunk 0 staged, chunk 1 in registers
-  float xr[CHB_ITEMS][4];
-  issue_matrix(0);
-  issue_matrix(1);
-  chb_load_input(a, in, c0, 0, xr);
-  chb_store_input(xr, Dhi(0), Dlo(0));
-  if (nch > 1) chb_load_input(a, in, c0, 1, xr);
-  int last = -1;      // last committed chunk
-  int consumed = 0;   // matrix chunks thread 0 has waited for
-  for (int q = 0; q < nch; ++q) {
-    const int ms = q % CHB_MSTAGES, ds = q & 1;
-    if (t == 0) {
-      if (!mlp_wait(full0 + 8 * ms, mpar(q), MLP_WAIT_LIMIT)) s_fail = 1;
-      else consumed = q + 1;
-    }
-    async_proxy_fence();
-    tc_fence_before();
-    __syncthreads();
-    if (s_fail) break;
-    if (t == 0) {
+    };
+    issue_matrix(0);
+    if (nch > 1) issue_matrix(1);
+    for (int q = 0; q < nch; ++q) {
+      const int ms = q % CHB_MSTAGES, ds = q & 1;
+      if (!mlp_wait(mfull0 + 8 * ms, mpar(q), MLP_WAIT_LIMIT)) {
+        s_fail = 1;
+        break;
+      }
+      consumed = q + 1;
+      if (!mlp_wait(dfull0 + 8 * ds, dpar(q), MLP_WAIT_LIMIT)) {
+        s_fail = 1;
+        break;
+      }
       tc_fence_after();
       const unsigned mh = smem_u32(Mhi(ms)), ml = mh + CHB_A_BYTES;
       const unsigned xh = smem_u32(Dhi(ds)), xl = smem_u32(Dlo(ds));
@@ -205,35 +207,57 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
         chb_mma(tmem, ah, bl, IDESC, 1u);
         chb_mma(tmem, al, bh, IDESC, 1u);
       }
-      mlp_commit(done0 + 8 * ds);
+      mlp_commit(dempty0 + 8 * ds);
+      mlp_commit(mempty0 + 8 * ms);
+      if (q + 2 < nch) {
+        // matrix stage of chunk q+2 was last read by chunk q-1
+        if (q >= 1 && !mlp_wait(mempty0 + 8 * ((q - 1) % CHB_MSTAGES), mpar(q - 1), MLP_WAIT_LIMIT)) {
+          s_fail = 1;
+          break;
+        }
+        issue_matrix(q + 2);
+      }
     }
-    last = q;
-    if (q + 1 < nch) {
-      // chunk q-1's MMAs done: its data stage (that of chunk q+1) and its
-      // matrix stage (that of chunk q+2) are free
-      if (t == 0 && q >= 1 && !mlp_wait(done0 + 8 * (ds ^ 1), dpar(q - 1), MLP_WAIT_LIMIT)) s_fail = 1;
-      tc_fence_before();
-      __syncthreads();
-      if (s_fail) break;
-      tc_fence_after();
-      issue_matrix(q + 2);
-      // chunk q+1's input (loaded an iteration ago) into the free data stage,
-      // then the loads of chunk q+2 stay in flight until the next iteration
-      chb_store_input(xr, Dhi(ds ^ 1), Dlo(ds ^ 1));
-      if (q + 2 < nch) chb_load_input(a, in, c0, q + 2, xr);
+    // arrives when every MMA issued above has completed (also after a failure)
+    mlp_commit(accb);
+  } else if (warp >= 4) {
+    const int pt = t - 128;
+    float x0[CHB_ITEMS][4], x1[CHB_ITEMS][4];
+    chb_load_input(a, in, c0, 0, pt, x0);
+    if (nch > 1) chb_load_input(a, in, c0, 1, pt, x1);
+    auto stage = [&](int q, float (&x)[CHB_ITEMS][4]) -> bool {
+      const int ds = q & 1;
+      // data stage of chunk q was last read by chunk q-2
+      if (q >= 2 && !mlp_wait(dempty0 + 8 * ds, dpar(q - 2), MLP_WAIT_LIMIT)) return false;
+      chb_store_input(x, pt, Dhi(ds), Dlo(ds));
+      async_proxy_fence();
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(dfull0 + 8 * ds) : "memory");
+      if (q + 2 < nch) chb_load_input(a, in, c0, q + 2, pt, x);
+      return true;
+    };
+    for (int q = 0; q < nch; q += 2) {
+      if (!stage(q, x0)) {
+        s_fail = 1;
+        break;
+      }
+      if (q + 1 < nch && !stage(q + 1, x1)) {
+        s_fail = 1;
+        break;
+      }
     }
   }
-  // all MMAs of the tile (they complete in order): the last chunk's barrier;
-  // matrix copies still in flight (only after a failed wait): their barriers
-  if (t == 0) {
-    if (last >= 0 && !mlp_wait(done0 + 8 * (last & 1), dpar(last), MLP_WAIT_LIMIT)) s_fail = 1;
+  __syncthreads();
+  // the accumulator (every MMA complete), then the copies still in flight
+  // (only after a failed wait)
+  bool acc_ok = mlp_wait(accb, 0u, MLP_WAIT_LIMIT);
+  if (t == 0)
     for (int q = consumed; q < issued; ++q)
-      if (!mlp_wait(full0 + 8 * (q % CHB_MSTAGES), mpar(q), MLP_WAIT_LIMIT)) s_fail = 1;
-  }
+      if (!mlp_wait(mfull0 + 8 * (q % CHB_MSTAGES), mpar(q), MLP_WAIT_LIMIT)) acc_ok = false;
+  if (!acc_ok) s_fail = 1;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (!s_fail && last == nch - 1) {
+  if (!s_fail) {
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (data columns);
     // TMEM column k is output row k; the two warp groups split the rows
     constexpr int KG = CHB_MROWS / 16;
