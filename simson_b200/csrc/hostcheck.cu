@@ -220,16 +220,59 @@ extern "C" int sbh_cfft(int n, int cols, const double* in, double* out, int sign
   }
 }
 
-// The tensor-core Chebyshev matrix image decoded back to row-major hi and lo
-// parts (n x n each), for the CPU check of its layout and accuracy.
-extern "C" int sbh_chb_matrix(int n, int inverse, double scale, float* hi, float* lo) {
+// The tensor-core Chebyshev transform emulated on the host in FP64 from its
+// matrix image: the even/odd folding of the input, the two half-matrix
+// products with hi + lo decoded from the tile layout, and the unfolding --
+// the kernel's arithmetic without the TF32 split of the data.  in/out: n rows
+// of ncol values.  Returns the chunk count, or -1 if an image entry is not a
+// TF32 value.
+extern "C" int sbh_chb_apply(int n, int inverse, double scale, int ncol, const double* in, double* out) {
   std::vector<unsigned char> img;
   chb_build_matrix(n, inverse, scale, img);
-  for (int r = 0; r < n; ++r)
-    for (int c = 0; c < n; ++c) {
-      const unsigned char* base = img.data() + (size_t)(c / CHB_KC) * CHB_CHUNK_BYTES;
-      memcpy(&hi[(size_t)r * n + c], base + chb_canon(r, c % CHB_KC), 4);
-      memcpy(&lo[(size_t)r * n + c], base + CHB_A_BYTES + chb_canon(r, c % CHB_KC), 4);
+  const int N = n - 1, H = N / 2, ne = chb_even_chunks(n), no = chb_odd_chunks(n);
+  const int KE = ne * CHB_KC, KO = no * CHB_KC;
+  std::vector<double> Me((size_t)CHB_NMAX * KE, 0.0), Mo((size_t)CHB_NMAX * (KO > 0 ? KO : 1), 0.0);
+  for (int q = 0; q < ne + no; ++q) {
+    const bool odd = chb_is_odd(q, no);
+    const int pi = chb_part_index(q);
+    const unsigned char* base = img.data() + (size_t)q * CHB_CHUNK_BYTES;
+    for (int r = 0; r < CHB_NMAX; ++r)
+      for (int kk = 0; kk < CHB_KC; ++kk) {
+        float hi, lo;
+        memcpy(&hi, base + chb_canon(r, kk), 4);
+        memcpy(&lo, base + CHB_A_BYTES + chb_canon(r, kk), 4);
+        unsigned uh, ul;
+        memcpy(&uh, &hi, 4);
+        memcpy(&ul, &lo, 4);
+        if ((uh & 0x1FFFu) || (ul & 0x1FFFu)) return -1;
+        const int c = pi * CHB_KC + kk;
+        (odd ? Mo[(size_t)r * KO + c] : Me[(size_t)r * KE + c]) = (double)hi + (double)lo;
+      }
+  }
+  std::vector<double> ev(KE), od(KO > 0 ? KO : 1), E(CHB_NMAX), O(CHB_NMAX);
+  for (int col = 0; col < ncol; ++col) {
+    auto x = [&](int row) { return in[(size_t)row * ncol + col]; };
+    for (int m = 0; m < KE; ++m)
+      ev[m] = inverse ? (m <= H ? x(2 * m) : 0.0) : (m < H ? x(m) + x(N - m) : (m == H ? x(H) : 0.0));
+    for (int m = 0; m < KO; ++m) od[m] = m < H ? (inverse ? x(2 * m + 1) : x(m) - x(N - m)) : 0.0;
+    for (int r = 0; r < CHB_NMAX; ++r) {
+      double se = 0.0, so = 0.0;
+      for (int c = 0; c < KE; ++c) se += Me[(size_t)r * KE + c] * ev[c];
+      for (int c = 0; c < KO; ++c) so += Mo[(size_t)r * KO + c] * od[c];
+      E[r] = se;
+      O[r] = so;
     }
-  return (int)(img.size() / CHB_CHUNK_BYTES);
+    auto y = [&](int row) -> double& { return out[(size_t)row * ncol + col]; };
+    if (!inverse) {
+      for (int m = 0; m <= H; ++m) y(2 * m) = E[m];
+      for (int m = 0; m < H; ++m) y(2 * m + 1) = O[m];
+    } else {
+      for (int j = 0; j < H; ++j) {
+        y(j) = E[j] + O[j];
+        y(N - j) = E[j] - O[j];
+      }
+      y(H) = E[H];
+    }
+  }
+  return ne + no;
 }

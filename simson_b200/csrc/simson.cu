@@ -306,9 +306,9 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   if (c->mixed && (cudaMalloc(&c->stf, 5 * fld * sizeof(float2)) != cudaSuccess ||
                    cudaMalloc(&c->meanp, 4 * (size_t)g.nyp * sizeof(double)) != cudaSuccess))
     return fail(SGPU_E_CUDA);
-  if (c->mixed && g.nyp <= CHB_MROWS) {
+  if (c->mixed && g.nyp <= CHB_MAX_NY) {
     // the step's two Chebyshev transforms as tensor-core GEMMs (up to
-    // CHB_MROWS points in y; larger grids keep the FFT transforms)
+    // CHB_MAX_NY points in y; larger grids keep the FFT transforms)
     std::vector<unsigned char> mf, mi;
     chb_build_matrix(g.nyp, 0, 1.0 / ((double)g.nxp * (double)g.nzp), mf);
     chb_build_matrix(g.nyp, 1, 1.0, mi);
@@ -465,7 +465,12 @@ static void launch_cheb_tc(sgpu_ctx* c, const float2* in, size_t in_fs, float2* 
   A.out_fs = 2 * out_fs;
   A.ncol = 2 * g.NP;
   A.n = g.nyp;
-  A.nchunks = (g.nyp + CHB_KC - 1) / CHB_KC;
+  A.inverse = (mat == c->chb_inv) ? 1 : 0;
+  A.ne = chb_even_chunks(g.nyp);
+  A.no = chb_odd_chunks(g.nyp);
+  const int H = (g.nyp - 1) / 2;
+  A.nre = (H + 1 + 15) / 16 * 16;
+  A.nro = (H + 15) / 16 * 16;
   A.mat = mat;
   A.skip_oddball = skip_oddball;
   A.nx2 = g.nx2;

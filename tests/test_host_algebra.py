@@ -182,15 +182,15 @@ def test_fixed_length_fft(n, prec):
                 assert np.array_equal(out, out4)
 
 
-@pytest.mark.parametrize("n", [17, 65, 193])
+@pytest.mark.parametrize("n", [17, 33, 65, 97, 129, 193, 223])
 def test_tensor_core_chebyshev_matrix(n):
-    """The 3xTF32 matrices of the mixed path's tensor-core Chebyshev
-    transforms: decoded from their tile layout, hi + lo is the exact DCT-I
-    matrix to ~2^-22, hi and lo are TF32 values (13 low bits zero), and
-    forward then inverse is the identity."""
+    """The mixed path's tensor-core Chebyshev transforms, emulated in FP64 from
+    their matrix image (even/odd folding, the two half matrices decoded from
+    the tile layout as hi + lo, unfolding): every image entry is a TF32 value,
+    forward and inverse equal the dense DCT-I of the reference's conventions
+    to ~2^-21, and inverse after forward is the identity."""
     host = ctypes.CDLL(sbuild.build_hostcheck())
-    fp = ctypes.POINTER(ctypes.c_float)
-    host.sbh_chb_matrix.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, fp, fp]
+    host.sbh_chb_apply.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp, dp]
     N = n - 1
     j = np.arange(n)
     cosm = np.cos(np.pi * np.outer(j, j) / N)
@@ -198,14 +198,17 @@ def test_tensor_core_chebyshev_matrix(n):
     cb = np.where((j == 0) | (j == N), 2.0, 1.0)
     scale = 1.0 / 3.0
     exact = {0: scale * cosm * w[None, :] / (N * cb[:, None]), 1: cosm}
-    mats = {}
-    for inv in (0, 1):
-        hi = np.zeros((n, n), np.float32)
-        lo = np.zeros((n, n), np.float32)
-        host.sbh_chb_matrix(n, inv, scale if inv == 0 else 1.0, hi.ctypes.data_as(fp), lo.ctypes.data_as(fp))
-        for part in (hi, lo):
-            assert np.all(part.view(np.uint32) & 0x1FFF == 0)
-        m = hi.astype(np.float64) + lo.astype(np.float64)
-        assert np.abs(m - exact[inv]).max() <= 2.0 ** -21 * np.abs(exact[inv]).max()
-        mats[inv] = m
-    np.testing.assert_allclose(mats[1] @ mats[0], scale * np.eye(n), atol=1e-5 * scale)
+    ncol = 7
+    rng = np.random.default_rng(n)
+    u = rng.standard_normal((n, ncol))
+    res = {}
+    for inv, s in ((0, scale), (1, 1.0)):
+        out = np.zeros((n, ncol))
+        assert host.sbh_chb_apply(n, inv, s, ncol, P(np.ascontiguousarray(u)), P(out)) > 0
+        ref = exact[inv] @ u
+        assert np.abs(out - ref).max() <= 2.0 ** -20 * np.abs(ref).max()
+        res[inv] = out
+    a = res[0]
+    back = np.zeros((n, ncol))
+    host.sbh_chb_apply(n, 1, 1.0, ncol, P(np.ascontiguousarray(a)), P(back))
+    np.testing.assert_allclose(back, scale * u, atol=1e-5 * scale * np.abs(u).max())
