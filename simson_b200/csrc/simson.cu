@@ -446,8 +446,23 @@ static void launch_cheb_t(sgpu_ctx* c, const typename C2<SI>::type* in, size_t i
   const Dims& g = c->g;
   dim3 grid((g.NP + PB - 1) / PB, nfields);
   const size_t sm = smem_fft(2 * (g.nyp - 1), PB, sizeof(typename C2<T>::type));
-  k_cheb<T, PB, SI, SO><<<grid, sgpu_ctx::fft_threads, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse, scale,
-                                                                        c->twy.plan, tw, skip_oddball);
+  // transform lengths 2(ny-1) of the production and test grids take the
+  // compile-time plan
+  switch (2 * (g.nyp - 1)) {
+#define SB_CHEB_CASE(L)                                                                                      \
+  case L: {                                                                                                  \
+    constexpr int NT = fixed_threads(L, PB);                                                                 \
+    cudaFuncSetAttribute(k_cheb<T, PB, SI, SO, L, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+    k_cheb<T, PB, SI, SO, L, NT><<<grid, NT, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse, scale,      \
+                                                              c->twy.plan, tw, skip_oddball);               \
+    break;                                                                                                   \
+  }
+    SB_CHEB_CASE(128) SB_CHEB_CASE(192) SB_CHEB_CASE(256) SB_CHEB_CASE(384)
+#undef SB_CHEB_CASE
+    default:
+      k_cheb<T, PB, SI, SO><<<grid, sgpu_ctx::fft_threads, sm, c->stream>>>(in, in_fs, out, out_fs, g, inverse,
+                                                                            scale, c->twy.plan, tw, skip_oddball);
+  }
   c->launches++;
 }
 

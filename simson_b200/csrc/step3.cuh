@@ -336,24 +336,28 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
 // ---------------------------------------------------------------------------
 // Chebyshev transforms over pencils
 // ---------------------------------------------------------------------------
-template <class T, int PB, class SI, class SO>
-__global__ void k_cheb(const typename C2<SI>::type* __restrict__ in, size_t in_fs,
-                       typename C2<SO>::type* __restrict__ out, size_t out_fs, Dims g, int inverse, double scale,
-                       FFTPlan plan, const typename C2<T>::type* __restrict__ tw, int skip_oddball) {
+// N > 0: the transform length 2(ny-1) is N, with the compile-time plan and
+// NT threads per CTA; its first pass reads the columns (even extension
+// folded into the index) and its last pass writes the n kept coefficients.
+template <class T, int PB, class SI, class SO, int N = 0, int NT = 0>
+__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+    k_cheb(const typename C2<SI>::type* __restrict__ in, size_t in_fs, typename C2<SO>::type* __restrict__ out,
+           size_t out_fs, Dims g, int inverse, double scale, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
+           int skip_oddball) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = g.nyp;
-  const int N = n - 1;
-  const int L = 2 * N;
+  const int Ny = n - 1;
+  const int L = 2 * Ny;
   V* b0 = reinterpret_cast<V*>(smem_raw);
   V* b1 = b0 + (size_t)L * PB;
   const int f = blockIdx.y;
   const int p0 = blockIdx.x * PB;
   const typename C2<SI>::type* src = in + f * in_fs;
   typename C2<SO>::type* dst = out + f * out_fs;
-  for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
-    const int j = t / PB;
-    const int b = t - j * PB;
+  // row j (0..Ny) of pencil p0 + b, with the inverse transform's 1/2 on the
+  // interior rows
+  auto load = [&](int j, int b) -> V {
     const int p = p0 + b;
     double2 v = double2{0.0, 0.0};
     if (p < g.NP) {
@@ -361,26 +365,41 @@ __global__ void k_cheb(const typename C2<SI>::type* __restrict__ in, size_t in_f
       v = double2{(double)q.x, (double)q.y};
     }
     if (inverse) {
-      const double cb = (j == 0 || j == N) ? 1.0 : 0.5;
+      const double cb = (j == 0 || j == Ny) ? 1.0 : 0.5;
       v.x *= cb;
       v.y *= cb;
     }
-    const V w = V{(T)v.x, (T)v.y};
-    b0[j * PB + b] = w;
-    if (j >= 1 && j <= N - 1) b0[(L - j) * PB + b] = w;
-  }
-  __syncthreads();
-  V* res = fft_columns<T, PB>(b0, b1, plan, tw, -1);
-  for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
-    const int k = t / PB;
-    const int b = t - k * PB;
+    return V{(T)v.x, (T)v.y};
+  };
+  // coefficient k (0..Ny) of pencil p0 + b
+  auto store = [&](int k, int b, V e) {
     const int p = p0 + b;
-    if (p >= g.NP) continue;
-    if (skip_oddball && (p / g.nx2) == g.zodd) continue;
-    const V e = res[k * PB + b];
+    if (p >= g.NP) return;
+    if (skip_oddball && (p / g.nx2) == g.zodd) return;
     double fac = scale;
-    if (!inverse) fac = scale / ((double)N * ((k == 0 || k == N) ? 2.0 : 1.0));
+    if (!inverse) fac = scale / ((double)Ny * ((k == 0 || k == Ny) ? 2.0 : 1.0));
     dst[(size_t)k * g.NP + p] = typename C2<SO>::type{(SO)((double)e.x * fac), (SO)((double)e.y * fac)};
+  };
+  if constexpr (N > 0) {
+    cfft_io<T, PB, N, -1, NT>([&](int m, int b) { return load(m <= Ny ? m : L - m, b); },
+                              [&](int k, int b, V e) {
+                                if (k <= Ny) store(k, b, e);
+                              },
+                              b0, b1, tw, threadIdx.x);
+  } else {
+    for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
+      const int j = t / PB;
+      const int b = t - j * PB;
+      const V w = load(j, b);
+      b0[j * PB + b] = w;
+      if (j >= 1 && j <= Ny - 1) b0[(L - j) * PB + b] = w;
+    }
+    __syncthreads();
+    V* res = fft_columns<T, PB>(b0, b1, plan, tw, -1);
+    for (int t = threadIdx.x; t < n * PB; t += blockDim.x) {
+      const int k = t / PB;
+      store(k, t - k * PB, res[k * PB + (t - k * PB)]);
+    }
   }
 }
 
