@@ -327,8 +327,13 @@ def main():
     dom = max((k for k in prof if k not in ("other",) and prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms = prof[dom][0] / prof[dom][1]
     dom_bytes = kernel_bytes(dom, w, head)
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    # from ncu captures of this build at this workload, summarised in
+    # profiles/: the pencil kernel captured at 384x193x384 (one pass), the x
+    # pass at 384x33x384 scaled by ny (its traffic grows with the planes)
+    measured_traffic = {("mixed", "pencil"): 2.64e9 + 2.53e9, ("mixed", "xpass"): (175.30e6 + 60.77e6) * 193 / 33}
     roof = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
-            "traffic": None, "launch_ms": dom_ms}
+            "traffic": measured_traffic.get((head, dom)), "launch_ms": dom_ms}
     if dom_bytes:
         ach = dom_bytes / (dom_ms / 1000.0) / 1e9
         roof.update(achieved=ach, frac=ach / hbm, algorithmic_bytes=dom_bytes)

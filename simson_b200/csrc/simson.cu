@@ -283,8 +283,8 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   if ((rc = make_tw(c->twz, g.nzp)) || (rc = make_tw(c->twx, g.nxp)) || (rc = make_tw(c->twy, 2 * (g.nyp - 1))))
     return fail(rc);
   const size_t fld = (size_t)g.nyp * g.NP;
-  c->ncz = 23;
-  c->nrz = 7;
+  c->ncz = 21;  // complex scratch fields czf(c, 0..20)
+  c->nrz = 2;
   if (cudaMalloc(&c->st, 7 * fld * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&c->puw, 2 * g.ny * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->scal, 4 * sizeof(double)) != cudaSuccess ||
@@ -731,12 +731,10 @@ static int enqueue_linear(sgpu_ctx* c) {
   PencilBufs B;
   B.H1 = czf(c, 0); B.H2 = czf(c, 1); B.H3 = czf(c, 2);
   B.PV = slot(c, 5); B.PW = slot(c, 6);
-  B.G = czf(c, 3); B.DG = czf(c, 4); B.HV = czf(c, 5); B.HOM = czf(c, 6); B.FV = czf(c, 7); B.FW = czf(c, 8);
-  B.PHI = czf(c, 9); B.OM = czf(c, 10); B.V = czf(c, 11); B.DV = czf(c, 12); B.DOM = czf(c, 13);
-  B.T1 = czf(c, 14); B.T2 = czf(c, 15);
+  B.HV = czf(c, 5); B.HOM = czf(c, 6);
+  B.PHI = czf(c, 9); B.OM = czf(c, 10); B.V = czf(c, 11); B.DV = czf(c, 12);
   B.OU = czf(c, 16); B.OV = czf(c, 17); B.OW = czf(c, 18); B.OX = czf(c, 19); B.OZ = czf(c, 20);
-  B.PHIH = rzf(c, 0); B.VH = rzf(c, 1); B.DVH = rzf(c, 2); B.CP = rzf(c, 3); B.WT = rzf(c, 4);
-  B.CPL = rzf(c, 5); B.WTL = rzf(c, 6);
+  B.PHIH = rzf(c, 0); B.DVH = rzf(c, 1);
   // kx = kz = 0 (mean flow, cflux) on the side stream, concurrent with the pencils
   MeanArgs M;
   M.H1 = B.H1; M.H3 = B.H3; M.puw = c->puw; M.scal = c->scal; M.scr = c->mscr;

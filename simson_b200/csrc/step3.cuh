@@ -409,10 +409,10 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
 struct PencilBufs {
   double2 *H1, *H2, *H3;          // Chebyshev nonlinear term (normalised)
   double2 *PV, *PW;               // state slots 6,7 (partial RHS, Chebyshev), updated in place
-  double2 *G, *DG, *HV, *HOM, *FV, *FW, *PHI, *OM, *V, *DV, *DOM, *T1, *T2;
+  double2 *HV, *HOM;              // forcing h_v, h_omega (storage FC), read by the last sweep
+  double2 *PHI, *OM, *V, *DV;     // solutions phi, omega_y (storage SC), v; dv (FP64 path)
   double2 *OU, *OV, *OW, *OX, *OZ;  // outputs (Chebyshev)
-  double *PHIH, *VH, *DVH, *CP, *WT;
-  double *CPL, *WTL;  // coefficients of the lambda solve (its own arrays: their type may differ)
+  double *PHIH, *DVH;             // k_pencil_hom: phi_h, and D v_h for the FP64 path's sums
 };
 
 struct RKc {
