@@ -23,17 +23,17 @@
 // with Fe = s w_j cos(2 pi j m / N) / (N cbar_{2m}), Fo = s w_j cos(pi j (2m+1) / N) / N,
 // Ie = cos(2 pi j m / N), Io = cos(pi j (2m+1) / N).
 //
-// One CTA (256 threads) owns 128 columns (the data is the A operand, M = 128,
+// One CTA (288 threads: eight producer warps, one MMA warp) owns 128 columns (the data is the A operand, M = 128,
 // columns as rows); the matrices are the B operands (N = H+1 and H rounded up
 // to 16, at most 112).  K is cut into chunks of 16, taken alternately from
 // the even and the odd GEMM (e0 o0 e1 o1 ...), accumulated into TMEM
 // columns 0.. (even) and 128.. (odd).  The warps specialise in the main loop:
-//   * thread 0 issues the 3xTF32 MMAs of chunk q as soon as its matrix and
+//   * one thread (warp 8) issues the 3xTF32 MMAs of chunk q as soon as its matrix and
 //     data stages are full, commits them to the stages' "empty" mbarriers,
 //     and keeps the prepared matrix chunks (canonical K-major TF32 tiles, hi
 //     and lo, built on the host) two chunks ahead in a three-stage ring by
 //     bulk copies (cp.async.bulk, completing on a "full" mbarrier);
-//   * warps 4-7 stage the input: for each pair of chunks the rows j and
+//   * warps 0-7 stage the input: for each pair of chunks the rows j and
 //     N-j (forward) or 2m and 2m+1 (inverse) are loaded once, a pair ahead in
 //     registers, folded, split into hi/lo TF32 and transposed to K-major in
 //     16-byte shared-memory stores into a two-stage ring (even chunk in
@@ -125,7 +125,8 @@ __device__ __forceinline__ void chb_bulk_load(unsigned dst, const void* src, uns
 // needs -- u_j and u_{N-j} (forward) or a_{2m} and a_{2m+1} (inverse) -- into
 // registers, and later stores the even and the odd tile split into hi/lo
 // TF32 (one 16-byte store per group, part and tile).
-constexpr int CHB_PRODUCERS = 128;
+constexpr int CHB_PRODUCERS = 256;                 // warps 0-7 stage the data
+constexpr int CHB_THREADS = CHB_PRODUCERS + 32;     // warp 8: MMA issue and matrix copies
 constexpr int CHB_ITEMS = CHB_TILE * (CHB_KC / 4) / CHB_PRODUCERS;
 
 struct ChbPair {
@@ -188,7 +189,7 @@ __device__ __forceinline__ void chb_store_tile(const ChebTCArgs& a, const ChbPai
   }
 }
 
-__global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
+__global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   // matrix stage m (hi | lo) at m * CHB_CHUNK_BYTES; data stage d (hi | lo):
   // d = 0 holds the even chunks, d = 1 the odd ones
@@ -228,8 +229,9 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   // the k-th use of a stage (chunk q = stage + k * stages) completes phase k
   auto mpar = [](int q) { return (unsigned)((q / CHB_MSTAGES) & 1); };
   auto dpar = [](int q) { return (unsigned)((q >> 1) & 1); };
-  int issued = 0, consumed = 0;  // thread 0: matrix copies issued / waited for
-  if (t == 0) {
+  int issued = 0, consumed = 0;  // MMA thread: matrix copies issued / waited for
+  const bool mma_thread = t == CHB_PRODUCERS;
+  if (mma_thread) {
     const unsigned idesc_e = chb_idesc(CHB_TILE, a.nre), idesc_o = chb_idesc(CHB_TILE, a.nro);
     auto issue_matrix = [&](int q) {
       chb_bulk_load(smem_u32(Mhi(q % CHB_MSTAGES)), a.mat + (size_t)q * CHB_CHUNK_BYTES, CHB_CHUNK_BYTES,
@@ -277,8 +279,8 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
     }
     // arrives when every MMA issued above has completed (also after a failure)
     mlp_commit(accb);
-  } else if (warp >= 4) {
-    const int pt = t - 128;
+  } else if (t < CHB_PRODUCERS) {
+    const int pt = t;
     ChbPair pa, pb;
     chb_load_pair(a, in, c0, 0, pt, pa);
     if (ne > 1) chb_load_pair(a, in, c0, 1, pt, pb);
@@ -311,14 +313,14 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
   // the accumulators (every MMA complete), then the copies still in flight
   // (only after a failed wait)
   bool acc_ok = mlp_wait(accb, 0u, MLP_WAIT_LIMIT);
-  if (t == 0)
+  if (mma_thread)
     for (int q = consumed; q < issued; ++q)
       if (!mlp_wait(mfull0 + 8 * (q % CHB_MSTAGES), mpar(q), MLP_WAIT_LIMIT)) acc_ok = false;
   if (!acc_ok) s_fail = 1;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (!s_fail) {
+  if (!s_fail && warp < 8) {
     // warp w reads TMEM lanes 32 (w % 4) .. +31 (data columns)
     const int N = a.n - 1, H = N / 2;
     const int grp = warp >> 2;
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(256, 2) k_cheb_tc(ChebTCArgs a) {
         }
       }
     }
-  } else if (t == 0) {
+  } else if (s_fail && t == 0) {
     atomicExch(a.err, 1);
   }
   tc_fence_before();

@@ -492,7 +492,7 @@ static void launch_cheb_tc(sgpu_ctx* c, const float2* in, size_t in_fs, float2* 
   A.zodd = g.zodd;
   A.err = c->chb_err;
   dim3 grid((A.ncol + CHB_TILE - 1) / CHB_TILE, nfields);
-  k_cheb_tc<<<grid, 256, CHB_SMEM, c->stream>>>(A);
+  k_cheb_tc<<<grid, CHB_THREADS, CHB_SMEM, c->stream>>>(A);
   c->launches++;
 }
 
