@@ -156,6 +156,29 @@ int sgpu_sgs_mlp_eval(sgpu_ctx* ctx, const sgpu_sgs_mlp* p, const float* x, floa
  * Synchronises the library's stream. */
 int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
 
+/* Multi-GPU runs (one context per GPU, the reference's MPI decomposition of
+ * bla/par.f:102 and bla/getpxz.f / putpxz.f mapped to whole-state contexts):
+ * restrict this context to a shard -- step 2 (sgpu_nonlin) on the xz-planes
+ * ylo <= y < yhi, step 3 (sgpu_linear) on the kz planes zlo <= iz < zhi (iz
+ * the stored kz index, kx all).  (0, ny, 0, nz) is the whole domain.  Before
+ * step 2 each shard needs slots 0-4 of its planes from every shard's kz
+ * planes, after it each shard needs slots 0-2 (H) of its kz planes from every
+ * shard's planes; the host moves these blocks (sgpu_copy_block plus its
+ * transport, e.g. an NCCL all-to-all).  sgpu_prhs still works on the whole
+ * uploaded state; LES and sgpu_amplitudes need the whole domain
+ * (SGPU_E_PARAM / SGPU_E_STATE on a shard).  Replaces the plane transposes of
+ * bla/getpxz.f:127-149 and bla/putpxz.f:69-93. */
+int sgpu_set_shard(sgpu_ctx* ctx, int ylo, int yhi, int zlo, int zhi);
+
+/* Copy state slots slot0 .. slot0+nslots-1 of the planes ylo..yhi-1 and kz
+ * planes zlo..zhi-1 between the state and the device buffer buf (to_state =
+ * 0: state -> buf, 1: buf -> state), packed as [slot][y][kz][kx] in the
+ * state's storage (complex FP32 for slots 0-4 under SGPU_MIXED, complex FP64
+ * otherwise); *bytes receives the block size (buf == NULL only reports it).
+ * Synchronises. */
+int sgpu_copy_block(sgpu_ctx* ctx, int slot0, int nslots, int ylo, int yhi, int zlo, int zhi, void* buf,
+                    int to_state, size_t* bytes);
+
 /* Stream-ordered timing on the library's stream: record event slot (0..15),
  * elapsed milliseconds between two recorded slots (synchronises on b). */
 int sgpu_event_record(sgpu_ctx* ctx, int slot);

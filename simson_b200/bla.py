@@ -92,6 +92,9 @@ def load_library(build: bool = True):
     fp = ctypes.POINTER(ctypes.c_float)
     lib.sgpu_set_sgs_mlp.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp)]
     lib.sgpu_sgs_mlp_eval.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp), fp, fp, ctypes.c_longlong]
+    lib.sgpu_set_shard.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.sgpu_copy_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -163,6 +166,23 @@ class Channel:
         return p
 
     # --- the reference's call sequence ----------------------------------
+    def set_shard(self, ylo, yhi, zlo, zhi):
+        """Compute only a shard of the domain: step 2 on the xz-planes
+        ylo <= y < yhi, step 3 on the stored kz planes zlo <= iz < zhi
+        (bla/par.f:102 z-slabs; simson_b200.shard moves the blocks)."""
+        self._check(self.lib.sgpu_set_shard(self._ctx, ylo, yhi, zlo, zhi), "set_shard")
+
+    def copy_block(self, slot0, nslots, ylo, yhi, zlo, zhi, buf_ptr=None, to_state=False):
+        """Pack (to_state=False) or unpack a block of state slots between the
+        state and the device buffer at buf_ptr ([slot][y][kz][kx], the
+        state's storage); returns its size in bytes (buf_ptr None: size
+        only)."""
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.sgpu_copy_block(self._ctx, slot0, nslots, ylo, yhi, zlo, zhi,
+                                             ctypes.c_void_p(buf_ptr) if buf_ptr else None, int(to_state),
+                                             ctypes.byref(n)), "copy_block")
+        return n.value
+
     def prhs(self):
         self._check(self.lib.sgpu_prhs(self._ctx), "prhs")
 

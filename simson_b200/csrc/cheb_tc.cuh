@@ -98,11 +98,13 @@ __device__ __forceinline__ float to_tf32(float x) {
 }
 
 struct ChebTCArgs {
-  const float* in;               // field f, row j, column c at in[f * in_fs + j * ncol + c]
+  const float* in;               // field f, row j, column c at in[f * in_fs + j * ld + c]
   size_t in_fs;
   float* out;
   size_t out_fs;
-  int ncol;                      // 2 NP
+  int ncol;                      // columns transformed: 2 (p1 - p0), from pencil p0 on
+  int ld;                        // row stride (2 NP)
+  int p0;                        // first pencil (the columns start at 2 p0 of the full field)
   int n;                         // ny = N + 1, N = 2H
   int inverse;                   // 0: physical -> Chebyshev, 1: Chebyshev -> physical
   int ne, no;                    // K chunks of the even and the odd GEMM
@@ -153,8 +155,8 @@ __device__ __forceinline__ void chb_load_pair(const ChebTCArgs& a, const float* 
       } else {
         r0 = m; r1 = N - m; v0 = m <= H; v1 = m < H;
       }
-      p.x[k][s] = (cv && v0) ? in[(size_t)r0 * a.ncol + col] : 0.f;
-      p.y[k][s] = (cv && v1) ? in[(size_t)r1 * a.ncol + col] : 0.f;
+      p.x[k][s] = (cv && v0) ? in[(size_t)r0 * a.ld + col] : 0.f;
+      p.y[k][s] = (cv && v1) ? in[(size_t)r1 * a.ld + col] : 0.f;
     }
   }
 }
@@ -325,7 +327,7 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
     const int N = a.n - 1, H = N / 2;
     const int grp = warp >> 2;
     const int col = c0 + (warp & 3) * 32 + (t & 31);
-    const bool keep = col < a.ncol && !(a.skip_oddball && (col >> 1) / a.nx2 == a.zodd);
+    const bool keep = col < a.ncol && !(a.skip_oddball && (a.p0 + (col >> 1)) / a.nx2 == a.zodd);
     const unsigned taddr = tmem + ((unsigned)((warp & 3) * 32) << 16);
     if (!a.inverse) {
       // group 0: even rows k = 2m from TMEM columns m; group 1: odd rows
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int m = 16 * kc + i;
-            if (m < nm) out[(size_t)(2 * m + grp) * a.ncol + col] = v[i];
+            if (m < nm) out[(size_t)(2 * m + grp) * a.ld + col] = v[i];
           }
         }
       }
@@ -361,10 +363,10 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
             const int j = 16 * kc + i;
             if (j < H) {
               const float ov = has_o ? o[i] : 0.f;
-              out[(size_t)j * a.ncol + col] = e[i] + ov;
-              out[(size_t)(N - j) * a.ncol + col] = e[i] - ov;
+              out[(size_t)j * a.ld + col] = e[i] + ov;
+              out[(size_t)(N - j) * a.ld + col] = e[i] - ov;
             } else if (j == H) {
-              out[(size_t)j * a.ncol + col] = e[i];
+              out[(size_t)j * a.ld + col] = e[i];
             }
           }
         }

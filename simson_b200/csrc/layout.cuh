@@ -22,6 +22,11 @@ struct Dims {
   int nxp, nzp;     // 3/2-rule dealiasing grid
   int NP;           // pencils per field, nz*nx2
   int zodd;         // oddball kz index nz/2 (skipped by step 3)
+  // the part of the domain this context computes (a shard of a multi-GPU
+  // run; the whole domain otherwise): step 2 on the xz-planes y0 <= y < y1,
+  // step 3 on the pencils p0 <= p < p1 (a slab of kz planes)
+  int y0, y1;
+  int p0, p1;
 };
 
 }  // namespace sb

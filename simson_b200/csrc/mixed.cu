@@ -28,12 +28,12 @@ void mixed_zfwd(cudaStream_t s, dim3 grid, size_t smem, const float2* xb, float2
 
 void mixed_pencil_hom(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
                       double re, double anbn, double* vh, double* hs, double* cf) {
-  k_pencil_hom<double, float><<<(g.NP + 127) / 128, 128, 0, s>>>(B, g, alfa, beta, re, anbn, vh, hs, cf);
+  k_pencil_hom<double, float><<<(g.p1 - g.p0 + 127) / 128, 128, 0, s>>>(B, g, alfa, beta, re, anbn, vh, hs, cf);
 }
 
 void mixed_pencil(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
                   double re, RKc rk, const double* vh, const double* hs, double* cf) {
-  k_pencil<float2, double, float><<<(g.NP + 127) / 128, 128, 0, s>>>(B, g, alfa, beta, re, rk, vh, hs, cf);
+  k_pencil<float2, double, float><<<(g.p1 - g.p0 + 127) / 128, 128, 0, s>>>(B, g, alfa, beta, re, rk, vh, hs, cf);
 }
 
 void mixed_mean(cudaStream_t s, const MeanArgs& M, const Dims& g, double re, RKc rk) {

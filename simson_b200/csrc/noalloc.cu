@@ -82,6 +82,7 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   g.nx2 = P.nx / 2; g.nyp = P.ny;
   g.nxp = P.nx + P.nx / 2; g.nzp = P.nz + P.nz / 2;
   g.NP = P.nz * g.nx2; g.zodd = P.nz / 2;
+  g.y0 = 0; g.y1 = g.nyp; g.p0 = 0; g.p1 = g.NP;  // the whole domain
   const size_t fine = (size_t)g.nyp * g.nzp * g.nx2 * sizeof(double2);
   const size_t need = 9 * fine;
   if (need > SGPU_NOALLOC_SCRATCH_BYTES || g.nzp > SGPU_NOALLOC_MAX_FFT || g.nxp > SGPU_NOALLOC_MAX_FFT ||

@@ -264,6 +264,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   g.nx2 = P.nx / 2; g.nyp = P.ny;
   g.nxp = P.nx + P.nx / 2; g.nzp = P.nz + P.nz / 2;
   g.NP = P.nz * g.nx2; g.zodd = P.nz / 2;
+  g.y0 = 0; g.y1 = g.nyp; g.p0 = 0; g.p1 = g.NP;  // the whole domain
   int rc = SGPU_OK;
   auto fail = [&](int r) { sgpu_finalize(c); return r; };
   if (cudaSetDevice(P.device) != cudaSuccess) return fail(SGPU_E_CUDA);
@@ -444,7 +445,7 @@ static void launch_cheb_t(sgpu_ctx* c, const typename C2<SI>::type* in, size_t i
                           size_t out_fs, int nfields, int inverse, double scale, int skip_oddball,
                           const typename C2<T>::type* tw) {
   const Dims& g = c->g;
-  dim3 grid((g.NP + PB - 1) / PB, nfields);
+  dim3 grid((g.p1 - g.p0 + PB - 1) / PB, nfields);
   const size_t sm = smem_fft(2 * (g.nyp - 1), PB, sizeof(typename C2<T>::type));
   // transform lengths 2(ny-1) of the production and test grids take the
   // compile-time plan
@@ -474,11 +475,14 @@ static void launch_cheb_tc(sgpu_ctx* c, const float2* in, size_t in_fs, float2* 
                            const unsigned char* mat, int skip_oddball) {
   const Dims& g = c->g;
   ChebTCArgs A{};
-  A.in = reinterpret_cast<const float*>(in);
+  // this context's pencils p0 <= p < p1 (columns 2 p0 .. 2 p1 of the full fields)
+  A.in = reinterpret_cast<const float*>(in) + 2 * (size_t)g.p0;
   A.in_fs = 2 * in_fs;
-  A.out = reinterpret_cast<float*>(out);
+  A.out = reinterpret_cast<float*>(out) + 2 * (size_t)g.p0;
   A.out_fs = 2 * out_fs;
-  A.ncol = 2 * g.NP;
+  A.ncol = 2 * (g.p1 - g.p0);
+  A.ld = 2 * g.NP;
+  A.p0 = g.p0;
   A.n = g.nyp;
   A.inverse = (mat == c->chb_inv) ? 1 : 0;
   A.ne = chb_even_chunks(g.nyp);
@@ -532,9 +536,68 @@ static void cheb_to_phys(sgpu_ctx* c, const double2* in, int slot0, int nfields,
 
 static void les_filter_velocity(sgpu_ctx* c, int skip_oddball);
 
+static bool sharded(const sgpu_ctx* c) {
+  const Dims& g = c->g;
+  return g.y0 != 0 || g.y1 != g.nyp || g.p0 != 0 || g.p1 != g.NP;
+}
+
+// the whole domain for the duration of a call (sgpu_prhs works on every
+// pencil in every context: its inputs are the whole uploaded state)
+struct WholeDomain {
+  sgpu_ctx* c;
+  Dims keep;
+  explicit WholeDomain(sgpu_ctx* ctx) : c(ctx), keep(ctx->g) {
+    c->g.y0 = 0; c->g.y1 = c->g.nyp; c->g.p0 = 0; c->g.p1 = c->g.NP;
+  }
+  ~WholeDomain() { c->g = keep; }
+};
+
+extern "C" int sgpu_set_shard(sgpu_ctx* c, int ylo, int yhi, int zlo, int zhi) {
+  if (!c) return SGPU_E_PARAM;
+  const Dims& g = c->g;
+  if (ylo < 0 || yhi > g.nyp || ylo >= yhi || zlo < 0 || zhi > g.nz || zlo >= zhi) return SGPU_E_PARAM;
+  const bool whole = ylo == 0 && yhi == g.nyp && zlo == 0 && zhi == g.nz;
+  if (!whole && c->iles != 0) return SGPU_E_PARAM;  // LES needs the whole domain
+  c->g.y0 = ylo; c->g.y1 = yhi;
+  c->g.p0 = zlo * g.nx2; c->g.p1 = zhi * g.nx2;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int yhi, int zlo, int zhi, void* buf,
+                               int to_state, size_t* bytes) {
+  if (!c || !bytes) return SGPU_E_PARAM;
+  const Dims& g = c->g;
+  if (slot0 < 0 || nslots < 1 || slot0 + nslots > 7 || ylo < 0 || yhi > g.nyp || ylo >= yhi || zlo < 0 ||
+      zhi > g.nz || zlo >= zhi)
+    return SGPU_E_PARAM;
+  const size_t fld = (size_t)g.nyp * g.NP;
+  size_t off = 0;
+  for (int s = slot0; s < slot0 + nslots; ++s) {
+    // complex FP32 under SGPU_MIXED for slots 0-4, complex FP64 otherwise
+    const bool f32 = c->mixed && s < 5;
+    const size_t es = f32 ? sizeof(float2) : sizeof(double2);
+    char* base = f32 ? reinterpret_cast<char*>(c->stf + s * fld) : reinterpret_cast<char*>(c->st + s * fld);
+    char* src = base + ((size_t)ylo * g.NP + (size_t)zlo * g.nx2) * es;
+    const size_t width = (size_t)(zhi - zlo) * g.nx2 * es, pitch = (size_t)g.NP * es;
+    const size_t height = (size_t)(yhi - ylo);
+    if (buf) {
+      char* b = static_cast<char*>(buf) + off;
+      if (to_state)
+        CK(cudaMemcpy2DAsync(src, pitch, b, width, width, height, cudaMemcpyDeviceToDevice, c->stream));
+      else
+        CK(cudaMemcpy2DAsync(b, width, src, pitch, width, height, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    off += width * height;
+  }
+  *bytes = off;
+  if (buf) CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
 extern "C" int sgpu_prhs(sgpu_ctx* c) {
   if (!c) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
+  WholeDomain whole(c);
   const Dims& g = c->g;
   const size_t fld = (size_t)g.nyp * g.NP;
   // first-stage RK factors (bla/bla.f:1466-1478) and cflux px (:1622-1633)
@@ -661,7 +724,8 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     k_cfl_reset<<<1, 1, 0, c->stream>>>(c->cfl_bits);
     c->launches++;
   }
-  dim3 gz((g.nx2 + c->kb - 1) / c->kb, g.nyp);
+  const int nyl = g.y1 - g.y0;  // this context's xz-planes
+  dim3 gz((g.nx2 + c->kb - 1) / c->kb, nyl);
   const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
@@ -673,8 +737,8 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     // FP32 transforms and products on the FP32 velocity/vorticity fields
     float2* zbf = reinterpret_cast<float2*>(c->zb);
     float2* xbf = reinterpret_cast<float2*>(c->xb);
-    dim3 gzf((g.nx2 + sgpu_ctx::kbf - 1) / sgpu_ctx::kbf, g.nyp);
-    dim3 gxf((g.nzp + sgpu_ctx::rbf - 1) / sgpu_ctx::rbf, g.nyp);
+    dim3 gzf((g.nx2 + sgpu_ctx::kbf - 1) / sgpu_ctx::kbf, nyl);
+    dim3 gxf((g.nzp + sgpu_ctx::rbf - 1) / sgpu_ctx::rbf, nyl);
     // the FFTs carry only the perturbations; the mean profiles enter the
     // products analytically and their mean-mean product in FP64
     prof_mark(c, K_ZINV);
@@ -689,7 +753,7 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     prof_mark(c, K_ZINV);
     launch_zinv<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa,
                                               c->beta, 0);
-    dim3 gx((g.nzp + c->rb - 1) / c->rb, g.nyp);
+    dim3 gx((g.nzp + c->rb - 1) / c->rb, nyl);
     prof_mark(c, K_XPASS);
     launch_xpass<double, sgpu_ctx::rb, sgpu_ctx::xpass64_threads>(gx, s_x, c->stream, c->zb, c->xb, g, c->twx.plan,
                                                                   c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
@@ -740,7 +804,10 @@ static int enqueue_linear(sgpu_ctx* c) {
   M.H1 = B.H1; M.H3 = B.H3; M.puw = c->puw; M.scal = c->scal; M.scr = c->mscr;
   M.OU = B.OU; M.OV = B.OV; M.OW = B.OW; M.OX = B.OX; M.OZ = B.OZ; M.PV = B.PV; M.PW = B.PW;
   M.cflux = P.cflux;
-  if (c->prof) {
+  // the mean flow belongs to the context that owns pencil 0 (kz = 0)
+  const bool own_mean = g.p0 == 0;
+  if (!own_mean) {
+  } else if (c->prof) {
     prof_mark(c, K_MEAN);
     if (c->mixed)
       mixed_mean(c->stream, M, g, P.re, rk);
@@ -771,7 +838,7 @@ static int enqueue_linear(sgpu_ctx* c) {
       mixed_pencil_hom(c->stream, B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld,
                        c->hom_s + hs * 2 * (size_t)g.NP, c->hom_cf + hs * 4 * fld);
     else
-      k_pencil_hom<double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(
+      k_pencil_hom<double, double><<<(g.p1 - g.p0 + 127) / 128, 128, 0, c->stream>>>(
           B, g, c->alfa, c->beta, P.re, anbn, c->hom_vh + hs * fld, c->hom_s + hs * 2 * (size_t)g.NP,
           c->hom_cf + hs * 4 * fld);
     c->launches++;
@@ -783,9 +850,9 @@ static int enqueue_linear(sgpu_ctx* c) {
   if (c->mixed)
     mixed_pencil(c->stream, B, g, c->alfa, c->beta, P.re, rk, vhc, hsc, cfc);
   else
-    k_pencil<double2, double, double><<<(g.NP + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
+    k_pencil<double2, double, double><<<(g.p1 - g.p0 + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
                                                                                  vhc, hsc, cfc);
-  if (!c->prof) cudaStreamWaitEvent(c->stream, c->join, 0);
+  if (!c->prof && own_mean) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
   cheb_to_phys(c, B.OU, 0, 5, 1, /*fp32_input=*/c->mixed);
@@ -923,6 +990,7 @@ extern "C" int sgpu_profile_read(sgpu_ctx* c, double* ms, int* count, int n) {
 // device; the y-integrals of the row run here with the Clenshaw-Curtis weights
 // of bla/preprbl.f:78-87 and gridy = 1 + eta (:56-58).
 extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
+  if (c && sharded(c)) return SGPU_E_STATE;  // statistics read the whole state
   if (!c || !amp) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
   const Dims& g = c->g;
@@ -1036,6 +1104,7 @@ static int sgs_setup(sgpu_ctx* c) {
 // ADM-RT large-eddy model (bla/rparamles.f, bla/bla.f:1489-1518, 2212-2231):
 // filter tables on the host (les_filter.h), gu and the tables on the device.
 extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
+  if (c && sharded(c) && p && p->iles != 0) return SGPU_E_PARAM;  // LES needs the whole domain
   if (!c || !p) return SGPU_E_PARAM;
   if (p->iles == 0) {
     c->iles = 0;

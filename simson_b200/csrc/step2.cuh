@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) 
   const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* b0 = reinterpret_cast<V*>(smem_raw);
   V* b1 = b0 + (size_t)nzp * KB;
-  const int y = blockIdx.y;
+  const int y = g.y0 + blockIdx.y;
   const int kx0 = blockIdx.x * KB;
   const int nzh = g.nz / 2;
   const size_t slot = (size_t)g.nyp * g.NP;
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* bA = reinterpret_cast<V*>(smem_raw);
   V* bB = bA + (size_t)n * B;
-  const int y = blockIdx.y;
+  const int y = g.y0 + blockIdx.y;
   const int m0 = blockIdx.x * RB;
   // Hermitian completion of two half spectra into one complex spectrum:
   // element k of column c = 3 r + q (row m0 + r, fields 2q and 2q+1)
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   const int nthr = NT > 0 ? NT : (int)blockDim.x;
   V* b0 = reinterpret_cast<V*>(smem_raw);
   V* b1 = b0 + (size_t)nzp * KB;
-  const int y = blockIdx.y;
+  const int y = g.y0 + blockIdx.y;
   const int kx0 = blockIdx.x * KB;
   const int nzh = g.nz / 2;
   const size_t fs = (size_t)g.nyp * nzp * g.nx2;

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   V* b0 = reinterpret_cast<V*>(smem_raw);
   V* b1 = b0 + (size_t)L * PB;
   const int f = blockIdx.y;
-  const int p0 = blockIdx.x * PB;
+  const int p0 = g.p0 + blockIdx.x * PB;
   const typename C2<SI>::type* src = in + f * in_fs;
   typename C2<SO>::type* dst = out + f * out_fs;
   // row j (0..Ny) of pencil p0 + b, with the inverse transform's 1/2 on the
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   auto load = [&](int j, int b) -> V {
     const int p = p0 + b;
     double2 v = double2{0.0, 0.0};
-    if (p < g.NP) {
+    if (p < g.p1) {
       const auto q = src[(size_t)j * g.NP + p];
       v = double2{(double)q.x, (double)q.y};
     }
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
   // coefficient k (0..Ny) of pencil p0 + b
   auto store = [&](int k, int b, V e) {
     const int p = p0 + b;
-    if (p >= g.NP) return;
+    if (p >= g.p1) return;
     if (skip_oddball && (p / g.nx2) == g.zodd) return;
     double fac = scale;
     if (!inverse) fac = scale / ((double)Ny * ((k == 0 || k == Ny) ? 2.0 : 1.0));
@@ -438,8 +438,8 @@ __global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const 
                                                     const double* __restrict__ beta, double re, double anbn,
                                                     double* __restrict__ VHc, double* __restrict__ HS,
                                                     double* __restrict__ CF) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.NP) return;
+  const int p = g.p0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.p1) return;
   const int kx = p % g.nx2;
   const int iz = p / g.nx2;
   if (iz == g.zodd || p == 0) return;
@@ -491,8 +491,8 @@ __global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const d
                                                 double* __restrict__ CF) {
   typedef typename C2<SC>::type SC2;
   typedef typename C2<FC>::type FC2;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.NP) return;
+  const int p = g.p0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.p1) return;
   const int kx = p % g.nx2;
   const int iz = p / g.nx2;
   if (iz == g.zodd || p == 0) return;
