@@ -229,6 +229,40 @@ def les_arm(steps, warmup):
             "variants": out}
 
 
+def shard_arm(args, rank, world, precision):
+    """One channel of the workload split over the ranks (simson_b200.shard):
+    every rank uploads the same field and runs prhs, then each substep moves
+    the two block all-to-alls over NCCL around its step-2 planes and step-3
+    kz planes.  Timed with CUDA events on each rank's stream, max over ranks."""
+    from simson_b200.bla import Channel, FP64, MIXED
+    from simson_b200.fields import channel_field
+    from simson_b200.shard import ShardedChannel
+
+    w = WORKLOAD
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"],
+                 precision=MIXED if precision == "mixed" else FP64, device=dev)
+    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"])
+    ch.set_velocity(u, v, wv)
+    ch.prhs()
+    sc = ShardedChannel(ch, rank, world, f"cuda:{dev}")
+    sc.step(args.warmup)
+    ch.sync()
+    dist_barrier(world)
+    clk = ClockSampler(dev)
+    clk.start()
+    l0 = ch.launches()
+    b0 = sc.bytes_moved
+    ch.record(0)
+    sc.step(args.steps)
+    ch.record(1)
+    ms = dist_max(ch.elapsed_ms(0, 1), world)
+    clocks = clk.stop()
+    out = dict(ms=ms, bytes=sc.bytes_moved - b0, launches=ch.launches() - l0, clocks=clocks)
+    ch.close()
+    return out
+
+
 def dist_barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -277,6 +311,9 @@ def main():
                     help="both: time FP64 and mixed; value is the mixed-precision step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration timings")
+    ap.add_argument("--shard", action="store_true",
+                    help="one channel split over the ranks (z-slab shards, NCCL all-to-alls; strong scaling) "
+                         "instead of one replica per rank")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -307,6 +344,23 @@ def main():
                 "cpu_baseline": r, "e2e": {"value": r["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return
+    if args.shard:
+        prec = "mixed" if args.precision in ("both", "mixed") else "fp64"
+        r = shard_arm(args, rank, world, prec)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        if rank == 0:
+            config["parallelism"] = f"z-slab shards x{world} (step 2 on ny/{world} planes, step 3 on nz/{world} kz planes)"
+            config["precision"] = prec
+            print(json.dumps({
+                "metric": METRIC, "value": args.steps / (r["ms"] / 1000.0), "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic", "config": config,
+                "exchange_bytes_per_step_per_rank": r["bytes"] / max(args.steps, 1), "clocks": r["clocks"],
+                "gpu_launches": r["launches"]}))
         return
     runs = {}
     for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):

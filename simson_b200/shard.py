@@ -76,7 +76,8 @@ def exchange(state, ranges, rank, block, alltoall, alloc):
         if send_sizes[s]:
             state.copy_block(*block(ranges, rank, s), buf_ptr=sp + off, to_state=False)
         off += send_sizes[s]
-    alltoall(send, send_sizes, recv, recv_sizes)
+    if nr > 1:
+        alltoall(send, send_sizes, recv, recv_sizes)
     off = 0
     for s in range(nr):
         if recv_sizes[s]:
@@ -100,6 +101,10 @@ def torch_alltoall(group=None):
     def alltoall(send, send_sizes, recv, recv_sizes):
         dist.all_to_all_single(recv[:sum(recv_sizes)], send[:sum(send_sizes)], output_split_sizes=recv_sizes,
                                input_split_sizes=send_sizes, group=group)
+        if recv.is_cuda:
+            # the library unpacks on its own stream: the transfer must be complete
+            import torch
+            torch.cuda.current_stream(recv.device).synchronize()
     return alltoall
 
 
