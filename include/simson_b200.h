@@ -166,7 +166,8 @@ int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
  * shard's planes; the host moves these blocks (sgpu_copy_block plus its
  * transport, e.g. an NCCL all-to-all).  sgpu_prhs still works on the whole
  * uploaded state; LES and sgpu_amplitudes need the whole domain
- * (SGPU_E_PARAM / SGPU_E_STATE on a shard).  Replaces the plane transposes of
+ * (SGPU_E_PARAM / SGPU_E_STATE on a shard), and so does sgpu_step_rk (the
+ * exchanges sit between its two steps).  Replaces the plane transposes of
  * bla/getpxz.f:127-149 and bla/putpxz.f:69-93. */
 int sgpu_set_shard(sgpu_ctx* ctx, int ylo, int yhi, int zlo, int zhi);
 

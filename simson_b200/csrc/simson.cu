@@ -897,6 +897,8 @@ extern "C" int sgpu_linear(sgpu_ctx* c) {
 extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
   if (!c || nsub < 0) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
+  // a shard needs the block exchanges between its two steps (host-driven)
+  if (sharded(c)) return SGPU_E_STATE;
   for (int s = 0; s < nsub; ++s) {
     // the CFL word is read back lazily (sgpu_get_scalars): no host sync per substep
     int r = enqueue_nonlin(c);
