@@ -12,12 +12,15 @@ needed between steps.
 Arms:
   own (default)   the CUDA step through the C ABI, state resident in HBM;
                   ``e2e`` repeats it through the same ABI with the whole state
-                  uploaded from pinned host memory and downloaded every step.
+                  uploaded from pinned host memory and downloaded every step
+                  (sgpu_offload_steps: the copies of consecutive steps overlap
+                  per slot, PCIe being full duplex).
   --impl reference  the reference's own CPU implementation of the step (the
                   translated Fortran, oracle/_ref) on all host cores, OpenMP.
 
-Multi-GPU: the step runs as independent replicas, one per rank (weak scaling);
-the path is not sharded across GPUs in this build.
+Multi-GPU: by default the step runs as independent replicas, one per rank
+(weak scaling); --shard splits one channel over the ranks (z-slab shards with
+two NCCL block all-to-alls per substep, simson_b200/shard.py; strong scaling).
 """
 from __future__ import annotations
 
@@ -173,11 +176,12 @@ def own_arm(args, rank, world, precision):
     ch.download_raw(hr.ptr, hi.ptr, nslots)
     e2e_steps = max(2, min(args.steps, 10))
     ch.sync()
+    # every step uploads the 7 slots from the pinned host arrays and downloads
+    # the result into them (sgpu_offload_steps; the copies of consecutive
+    # steps overlap per slot)
+    ch.offload_steps(hr.ptr, hi.ptr, 1)  # warm-up: streams and events
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ch.upload_raw(hr.ptr, hi.ptr, nslots)
-        ch.step(1)
-        ch.download_raw(hr.ptr, hi.ptr, nslots)
+    ch.offload_steps(hr.ptr, hi.ptr, e2e_steps)
     e2e_s = time.perf_counter() - t0
     e2e_s = dist_max(e2e_s * 1000.0, world) / 1000.0
     nbytes = int(np.prod(shape)) * 8 * 2

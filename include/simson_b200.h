@@ -156,6 +156,16 @@ int sgpu_sgs_mlp_eval(sgpu_ctx* ctx, const sgpu_sgs_mlp* p, const float* x, floa
  * Synchronises the library's stream. */
 int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
 
+/* The driver keeps the state: advance it by nsteps RK3 steps, each step
+ * uploading all 7 slots from ur, ui (reference layout, as sgpu_upload_state;
+ * pinned host memory for full speed) and downloading the result into them
+ * (as sgpu_download_state), so the host arrays are current after every step.
+ * The copies of consecutive steps are pipelined per slot: the upload of slot
+ * k for step n+1 waits only for slot k of step n to be back on the host and
+ * overlaps the download of the other slots (PCIe is full duplex).  Returns
+ * after the last download.  Not on a shard. */
+int sgpu_offload_steps(sgpu_ctx* ctx, double* ur, double* ui, int nsteps);
+
 /* Multi-GPU runs (one context per GPU, the reference's MPI decomposition of
  * bla/par.f:102 and bla/getpxz.f / putpxz.f mapped to whole-state contexts):
  * restrict this context to a shard -- step 2 (sgpu_nonlin) on the xz-planes

@@ -92,6 +92,7 @@ def load_library(build: bool = True):
     fp = ctypes.POINTER(ctypes.c_float)
     lib.sgpu_set_sgs_mlp.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp)]
     lib.sgpu_sgs_mlp_eval.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp), fp, fp, ctypes.c_longlong]
+    lib.sgpu_offload_steps.argtypes = [vp, dp, dp, ctypes.c_int]
     lib.sgpu_set_shard.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.sgpu_copy_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
@@ -164,6 +165,14 @@ class Channel:
         p = np.empty((2, self.ny))
         self._check(self.lib.sgpu_download_puw(self._ctx, _dp(p)), "puw")
         return p
+
+    def offload_steps(self, re_ptr, im_ptr, n):
+        """n RK3 steps with the state round-tripped through the host arrays
+        (all 7 slots, reference layout, pinned) every step, the copies of
+        consecutive steps pipelined per slot (sgpu_offload_steps)."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.sgpu_offload_steps(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), n),
+                    "offload_steps")
 
     # --- the reference's call sequence ----------------------------------
     def set_shard(self, ylo, yhi, zlo, zhi):

@@ -46,6 +46,9 @@ struct sgpu_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;      // mean-flow solve, overlapped with the pencils
   cudaEvent_t fork = nullptr, join = nullptr;
+  // sgpu_offload_steps: copy streams and per-slot events (created on first use)
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t up_done[7] = {}, out_ready[7] = {}, down_done[7] = {};
   cudaEvent_t ev[16] = {};
   // resident state
   double2* st = nullptr;     // [7][nyp][NP]; SGPU_MIXED keeps only slots 5-6 (p_v, p_omega) here
@@ -162,8 +165,9 @@ static int make_tw(Tw& t, int n) {
 // ---------------------------------------------------------------------------
 // layout conversion between the reference's split arrays and the device state
 // ---------------------------------------------------------------------------
+// s0: state slot of the first reference slot (re, im point at that slot)
 __global__ void k_from_ref(const double* __restrict__ re, const double* __restrict__ im, double2* __restrict__ st,
-                           Dims g, int nslots) {
+                           Dims g, int nslots, int s0 = 0) {
   const size_t tot = (size_t)nslots * g.nyp * g.NP;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
     // i indexes the reference layout x + nx2*(y + nyp*(z + nz*s))
@@ -171,20 +175,20 @@ __global__ void k_from_ref(const double* __restrict__ re, const double* __restri
     const int x = r % g.nx2; r /= g.nx2;
     const int y = r % g.nyp; r /= g.nyp;
     const int z = r % g.nz; r /= g.nz;
-    const int s = (int)r;
+    const int s = s0 + (int)r;
     st[((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x] = double2{re[i], im[i]};
   }
 }
 
 __global__ void k_to_ref(const double2* __restrict__ st, double* __restrict__ re, double* __restrict__ im, Dims g,
-                         int nslots) {
+                         int nslots, int s0 = 0) {
   const size_t tot = (size_t)nslots * g.nyp * g.NP;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
     size_t r = i;
     const int x = r % g.nx2; r /= g.nx2;
     const int y = r % g.nyp; r /= g.nyp;
     const int z = r % g.nz; r /= g.nz;
-    const int s = (int)r;
+    const int s = s0 + (int)r;
     const double2 v = st[((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x];
     re[i] = v.x;
     im[i] = v.y;
@@ -193,14 +197,15 @@ __global__ void k_to_ref(const double2* __restrict__ st, double* __restrict__ re
 
 // SGPU_MIXED: slots 0-4 live in FP32 (stf), slots 5-6 in FP64 (st)
 __global__ void k_from_ref_mixed(const double* __restrict__ re, const double* __restrict__ im,
-                                 double2* __restrict__ st, float2* __restrict__ stf, Dims g, int nslots) {
+                                 double2* __restrict__ st, float2* __restrict__ stf, Dims g, int nslots,
+                                 int s0 = 0) {
   const size_t tot = (size_t)nslots * g.nyp * g.NP;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
     size_t r = i;
     const int x = r % g.nx2; r /= g.nx2;
     const int y = r % g.nyp; r /= g.nyp;
     const int z = r % g.nz; r /= g.nz;
-    const int s = (int)r;
+    const int s = s0 + (int)r;
     const size_t o = ((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x;
     // every slot also lands in FP64: sgpu_prhs differentiates u, v, w up to
     // four times in y, which FP32 rounding would not survive
@@ -210,14 +215,14 @@ __global__ void k_from_ref_mixed(const double* __restrict__ re, const double* __
 }
 
 __global__ void k_to_ref_mixed(const double2* __restrict__ st, const float2* __restrict__ stf,
-                               double* __restrict__ re, double* __restrict__ im, Dims g, int nslots) {
+                               double* __restrict__ re, double* __restrict__ im, Dims g, int nslots, int s0 = 0) {
   const size_t tot = (size_t)nslots * g.nyp * g.NP;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
     size_t r = i;
     const int x = r % g.nx2; r /= g.nx2;
     const int y = r % g.nyp; r /= g.nyp;
     const int z = r % g.nz; r /= g.nz;
-    const int s = (int)r;
+    const int s = s0 + (int)r;
     const size_t o = ((size_t)s * g.nyp + y) * g.NP + (size_t)z * g.nx2 + x;
     if (s < 5) {
       const float2 v = stf[o];
@@ -385,6 +390,13 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   for (auto& e : c->pev) cudaEventDestroy(e);
   if (c->fork) cudaEventDestroy(c->fork);
   if (c->join) cudaEventDestroy(c->join);
+  for (int k = 0; k < 7; ++k) {
+    if (c->up_done[k]) cudaEventDestroy(c->up_done[k]);
+    if (c->out_ready[k]) cudaEventDestroy(c->out_ready[k]);
+    if (c->down_done[k]) cudaEventDestroy(c->down_done[k]);
+  }
+  if (c->h2d) cudaStreamDestroy(c->h2d);
+  if (c->d2h) cudaStreamDestroy(c->d2h);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -906,6 +918,60 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
     r = enqueue_linear(c);
     if (r) return r;
   }
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
+  if (!c || !ur || !ui || nsteps < 0) return SGPU_E_PARAM;
+  if (sharded(c)) return SGPU_E_STATE;
+  const Dims& g = c->g;
+  const size_t n1 = (size_t)g.nyp * g.NP;  // one slot of the reference layout
+  if (!c->h2d) {
+    CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    for (int k = 0; k < 7; ++k) {
+      CK(cudaEventCreateWithFlags(&c->up_done[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->out_ready[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->down_done[k], cudaEventDisableTiming));
+    }
+  }
+  double* sre = c->stage;           // staging of the reference layout, slot k at k * n1
+  double* sim = c->stage + 7 * n1;
+  for (int step = 0; step < nsteps; ++step) {
+    // in: slot k of this step waits only for slot k of the previous step to
+    // be back on the host, so it overlaps the download of the other slots
+    for (int k = 0; k < 7; ++k) {
+      if (step > 0) CK(cudaStreamWaitEvent(c->h2d, c->down_done[k], 0));
+      CK(cudaMemcpyAsync(sre + k * n1, ur + k * n1, n1 * sizeof(double), cudaMemcpyHostToDevice, c->h2d));
+      CK(cudaMemcpyAsync(sim + k * n1, ui + k * n1, n1 * sizeof(double), cudaMemcpyHostToDevice, c->h2d));
+      CK(cudaEventRecord(c->up_done[k], c->h2d));
+      CK(cudaStreamWaitEvent(c->stream, c->up_done[k], 0));
+      if (c->mixed)
+        k_from_ref_mixed<<<592, 256, 0, c->stream>>>(sre + k * n1, sim + k * n1, c->st, c->stf, g, 1, k);
+      else
+        k_from_ref<<<592, 256, 0, c->stream>>>(sre + k * n1, sim + k * n1, c->st, g, 1, k);
+      c->launches++;
+    }
+    c->have_state = true;
+    int r = sgpu_step_rk(c, 3);
+    if (r) return r;
+    // out: slot by slot, each copy as soon as its conversion is done
+    for (int k = 0; k < 7; ++k) {
+      if (c->mixed)
+        k_to_ref_mixed<<<592, 256, 0, c->stream>>>(c->st, c->stf, sre + k * n1, sim + k * n1, g, 1, k);
+      else
+        k_to_ref<<<592, 256, 0, c->stream>>>(c->st, sre + k * n1, sim + k * n1, g, 1, k);
+      c->launches++;
+      CK(cudaEventRecord(c->out_ready[k], c->stream));
+      CK(cudaStreamWaitEvent(c->d2h, c->out_ready[k], 0));
+      CK(cudaMemcpyAsync(ur + k * n1, sre + k * n1, n1 * sizeof(double), cudaMemcpyDeviceToHost, c->d2h));
+      CK(cudaMemcpyAsync(ui + k * n1, sim + k * n1, n1 * sizeof(double), cudaMemcpyDeviceToHost, c->d2h));
+      CK(cudaEventRecord(c->down_done[k], c->d2h));
+    }
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->d2h));
+  CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
 }
 
