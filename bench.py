@@ -168,6 +168,15 @@ def own_arm(args, rank, world, precision):
     ch.step(2)
     prof = ch.profile_read()
     ch.profile(False)
+    # one xy-statistics sample (boxxys on every plane), outside the timed
+    # steps: the first call sets up its buffers
+    ch.xys_sample()
+    ch.sync()
+    ch.record(0)
+    for _ in range(3):
+        ch.xys_sample()
+    ch.record(1)
+    xys_ms = ch.elapsed_ms(0, 1) / 3
     # end-to-end through the public API with host buffers
     nslots = 7
     shape = (nslots, w["nz"], w["ny"], w["nx"] // 2)
@@ -190,7 +199,7 @@ def own_arm(args, rank, world, precision):
     finite = bool(np.isfinite(sc["px"]))
     ch.close()
     return dict(ms=ms, launches=launches, clocks=clocks, prof=prof, e2e_s=e2e_s, e2e_steps=e2e_steps,
-                e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw)
+                e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw, xys_ms=xys_ms)
 
 
 LES_WORKLOAD = dict(nx=64, ny=97, nz=64, re=4200.0, xl=2 * np.pi, zl=np.pi, dt=0.005, rms=0.1, seed=4)
@@ -417,6 +426,7 @@ def main():
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
         "finite": res["finite"],
+        "xys_sample_ms": res["xys_ms"],
     }
     if "fp64" in runs and "mixed" in runs:
         r64 = runs["fp64"]

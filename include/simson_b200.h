@@ -156,6 +156,26 @@ int sgpu_sgs_mlp_eval(sgpu_ctx* ctx, const sgpu_sgs_mlp* p, const float* x, floa
  * Synchronises the library's stream. */
 int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
 
+/* xy statistics (bla/boxxys.f, taken by bla/bla.f:2069-2107 at the start of a
+ * step when mod(it-1-nst, ixys) = 0 and t >= txys; the caller decides when):
+ * one sample of the current state with weight dtn is added to the running
+ * sums xys and sumw (sumw += dtn), on the library's stream.  Entries computed
+ * (1-based, the reference's numbering): 1-15 means and second moments of
+ * u_i, omega_i and uv, uw, vw; 25-30 the dissipation tensor du_i/dx_k
+ * du_j/dx_k; 43-44 running min / max over z of u - <u>_z; 45-51 S_ij S_ij
+ * and S_ij; 63-72 third moments; 75-77 u_i^4.  The pressure, LES and MHD
+ * entries stay zero (the reference built with pressure = 0, no LES or MHD
+ * statistics).  nx <= 512.  Not on a shard. */
+int sgpu_xys_sample(sgpu_ctx* ctx, double dtn);
+
+/* The running sums: xys[96*ny*nx] in the layout of the reference's
+ * xys(nx, ny, 96) (x fastest), *sumw the accumulated weight (either may be
+ * read before any sample: zeros).  Synchronises the library's stream. */
+int sgpu_xys_get(sgpu_ctx* ctx, double* xys, double* sumw);
+
+/* Zero the running sums (a new averaging period, bla/bla.f:1573). */
+int sgpu_xys_reset(sgpu_ctx* ctx);
+
 /* The driver keeps the state: advance it by nsteps RK3 steps, each step
  * uploading all 7 slots from ur, ui (reference layout, as sgpu_upload_state;
  * pinned host memory for full speed) and downloading the result into them

@@ -22,6 +22,7 @@ Translated units (reference file: what it contributes):
                  solvbc.f                                                  (step 3)
   bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
   bla/boxamp.f                                                             (plane statistics)
+  bla/boxxys.f xzsh.f + bla.f 2069-2107                                    (xy statistics)
   bla/init_filter.f lpf_y.f hpf_y.f bandsolver.f + bla.f 1489-1545         (ADM-RT LES filters)
   bla/les.f sgs_stress.f filter_cutoff.f + bla.f 1945-2020                 (eddy-viscosity LES)
 For grids up to SMAG_MAX_POINTS the driver's compile-time switch iiles_smag
@@ -52,7 +53,7 @@ UNIT_FILES = [
     "linearbl.f", "getxy.f", "putxy.f", "setmacrhs.f", "trid.f", "dcheb.f", "evald.f",
     "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
     "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
-    "les.f", "sgs_stress.f", "filter_cutoff.f",
+    "les.f", "sgs_stress.f", "filter_cutoff.f", "boxxys.f", "xzsh.f",
 ]
 
 MAIN_RANGES = [
@@ -65,6 +66,7 @@ MAIN_RANGES = [
     ("bla_substep_time", 1796, 1797),
     ("bla_les", 1945, 2020),
     ("bla_boxshift", 1819, 1826),
+    ("bla_xys", 2069, 2107),
     ("bla_nonlin", 2251, 2288),
     ("bla_cfl", 2349, 2351),
     ("bla_rkweights", 2384, 2397),

@@ -142,6 +142,31 @@ void sref_grid(double *eta, double *wint) {
 void sref_set_iamp(int iamp) { v_iamp = iamp > 0 ? iamp : -1000000; }
 void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(double)); }
 
+/* xy statistics: the sampling block of bla/bla.f:2069-2107 (boxxys on every
+ * xz-plane with weight dtn, then sumw(istat) += dtn) run on the current
+ * state, as bla.f does at the start of a step that takes statistics.  With
+ * reset != 0 xys and sumw are zeroed first (bla.f:1573 and the zeroed
+ * allocation).  out receives xys(1:nx, 1:nyp, 1:nxys) of istat = 1 (x
+ * fastest; the array's y extent is nyp/nproc+1), sumw_out sumw(1). */
+void sref_xys(double dtn, int reset, double *out, double *sumw_out) {
+  const long ly = (long)v_nyp / v_nproc + 1;
+  if (reset) {
+    memset(v_xys, 0, (size_t)v_nx * ly * v_nxys * v_mxys * sizeof(double));
+    v_sumw[0] = 0.0;
+  }
+  const double dtn_saved = v_dtn;
+  v_dtn = dtn;
+  v_xysp = 1.0; /* istat = mod(int(t/xysp), mxys) + 1 = 1 */
+  v_do_stat = 1;
+  bla_xys();
+  v_do_stat = 0;
+  v_dtn = dtn_saved;
+  for (long s = 0; s < v_nxys; ++s)
+    for (long y = 0; y < v_nyp; ++y)
+      memcpy(out + (s * v_nyp + y) * v_nx, v_xys + (s * ly + y) * v_nx, (size_t)v_nx * sizeof(double));
+  *sumw_out = v_sumw[0];
+}
+
 /* LES as rparamles.f would leave it for an sgs.i with iles, cutoff_inv, iord,
  * chi, cs, ineg (bla/rparamles.f:31-60), ihighorder as given (the reference
  * default is 2), then the filter set-up of bla/bla.f:1489-1545 and

@@ -42,6 +42,7 @@ def _lib(nx, ny, nz, build=True, fma=False):
     lib.sref_get_filter.argtypes = [dp] * 6
     lib.sref_get_gu.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_amp.argtypes = [dp]
+    lib.sref_xys.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp]
     return lib
 
 
@@ -148,6 +149,16 @@ class RefSim:
         a = np.empty((20, self.nyp))
         self.lib.sref_get_amp(_dp(a))
         return a
+
+    def xys(self, dtn, reset=False, nxys=96):
+        """One statistics sample (bla/bla.f:2069-2107: boxxys on every plane
+        with weight dtn) of the current state, added to the running sums
+        (zeroed first with reset).  Returns (xys, sumw): xys[s-1, y, x] =
+        xys(x+1, y+1, s) of the reference, shape (nxys, nyp, nx)."""
+        out = np.empty((nxys, self.nyp, self.nx))
+        sw = np.zeros(1)
+        self.lib.sref_xys(float(dtn), 1 if reset else 0, _dp(out), _dp(sw))
+        return out, float(sw[0])
 
     def state(self):
         return [self.get_slot(k) for k in range(1, 8)]

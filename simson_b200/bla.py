@@ -86,6 +86,9 @@ def load_library(build: bool = True):
     lib.sgpu_host_alloc.argtypes = [ctypes.c_ulonglong, ctypes.POINTER(vp)]
     lib.sgpu_host_free.argtypes = [vp]
     lib.sgpu_amplitudes.argtypes = [vp, dp, dp]
+    lib.sgpu_xys_sample.argtypes = [vp, ctypes.c_double]
+    lib.sgpu_xys_get.argtypes = [vp, dp, dp]
+    lib.sgpu_xys_reset.argtypes = [vp]
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
@@ -116,6 +119,7 @@ class Channel:
                  rot=0.0, icfl=3, precision=FP64, device=0):
         self.lib = load_library()
         self.nx, self.ny, self.nz = nx, ny, nz
+        self.dt = dt
         self.shape = (nz, ny, nx // 2)
         if px is None:
             px = -2.0 / re  # bla/bla.f:1630 first guess under cflux
@@ -300,6 +304,25 @@ class Channel:
         row = np.zeros(19)
         self._check(self.lib.sgpu_amplitudes(self._ctx, _dp(amp), _dp(row)), "amplitudes")
         return amp, dict(zip(self.AMP_ROW, row))
+
+    NXYS = 96
+
+    def xys_sample(self, dtn=None):
+        """Add one xy-statistics sample of the current state with weight dtn
+        (default the time step) to the running sums (bla/boxxys.f as
+        bla/bla.f:2069-2107 takes it)."""
+        self._check(self.lib.sgpu_xys_sample(self._ctx, float(self.dt if dtn is None else dtn)), "xys_sample")
+
+    def xys(self):
+        """The running xy statistics: (xys, sumw) with xys[s-1, y, x] =
+        xys(x+1, y+1, s) of the reference, shape (96, ny, nx)."""
+        out = np.empty((self.NXYS, self.ny, self.nx))
+        sw = np.zeros(1)
+        self._check(self.lib.sgpu_xys_get(self._ctx, _dp(out), _dp(sw)), "xys_get")
+        return out, float(sw[0])
+
+    def xys_reset(self):
+        self._check(self.lib.sgpu_xys_reset(self._ctx), "xys_reset")
 
     KERNELS = ("zinv", "xpass", "zfwd", "cheb_fwd", "pencil", "mean", "cheb_inv", "other")
 

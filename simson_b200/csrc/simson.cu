@@ -20,6 +20,7 @@
 #include "les_filter.h"
 #include "les_dyn.cuh"
 #include "sgs_mlp.cuh"
+#include "xys.cuh"
 #include "mixed.h"
 #include "step2_launch.cuh"
 #include "cheb_tc.cuh"
@@ -103,6 +104,14 @@ struct sgpu_ctx {
   double* stage = nullptr;   // host<->device staging (split re/im)
   Tw twz, twx, twy;
   Tw sgs_twz, sgs_twx;  // lengths nz and nx (iles = 2)
+  // xy statistics (sgpu_xys_sample): running sums xys [96][nyp][nx] and
+  // sumw, the 15 spectral fields, the z-group sums and physical u
+  double* xys = nullptr;
+  double2* xys_spec = nullptr;
+  double* xys_part = nullptr;
+  double* xys_u = nullptr;
+  double xys_sumw = 0.0;
+  Tw xys_twz, xys_twx;
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
   int it = 1;
@@ -380,7 +389,8 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
-                  c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->mlp_image, c->mlp_tau,
+                  c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
+                  c->xys_part, c->xys_u, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
@@ -1057,6 +1067,85 @@ extern "C" int sgpu_profile_read(sgpu_ctx* c, double* ms, int* count, int n) {
 // for the channel, dstar = 1, one process).  The per-plane sums run on the
 // device; the y-integrals of the row run here with the Clenshaw-Curtis weights
 // of bla/preprbl.f:78-87 and gridy = 1 + eta (:56-58).
+// xy statistics (bla/boxxys.f via bla/bla.f:2069-2107), see xys.cuh.
+static int xys_setup(sgpu_ctx* c) {
+  if (c->xys) return SGPU_OK;
+  const Dims& g = c->g;
+  constexpr int KB = 4;
+  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+  const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
+  if (g.nx > 512 || sz > 227 * 1024 || sx > 227 * 1024) return SGPU_E_PARAM;
+  int rc;
+  if (!c->xys_twz.d && (rc = make_tw(c->xys_twz, g.nz))) return rc;
+  if (!c->xys_twx.d && (rc = make_tw(c->xys_twx, g.nx))) return rc;
+  const size_t plane = (size_t)g.nyp * g.nx;
+  // c->xys last: its presence marks the set-up as complete
+  if ((!c->xys_spec && cudaMalloc(&c->xys_spec, XYS_NF * (size_t)g.nyp * g.NP * sizeof(double2)) != cudaSuccess) ||
+      (!c->xys_part &&
+       cudaMalloc(&c->xys_part, (size_t)XYS_GROUPS * XYS_NACC * plane * sizeof(double)) != cudaSuccess) ||
+      (!c->xys_u && cudaMalloc(&c->xys_u, plane * g.nz * sizeof(double)) != cudaSuccess) ||
+      cudaMalloc(&c->xys, XYS_NS * plane * sizeof(double)) != cudaSuccess)
+    return SGPU_E_CUDA;
+  CK(cudaMemsetAsync(c->xys, 0, XYS_NS * plane * sizeof(double), c->stream));
+  c->xys_sumw = 0.0;
+  cudaFuncSetAttribute(k_xys_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+  cudaFuncSetAttribute(k_xys_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+  cudaFuncSetAttribute(k_xys_acc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
+  if (c && sharded(c)) return SGPU_E_STATE;  // statistics read the whole state
+  if (!c || !(dtn >= 0.0)) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  int rc = xys_setup(c);
+  if (rc) return rc;
+  const Dims& g = c->g;
+  const SgsGrid G = sgs_grid(c);
+  constexpr int KB = 4;
+  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+  const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
+  const dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
+  if (c->mixed)
+    k_xys_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+                                                       c->alfa, c->beta);
+  else
+    k_xys_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+                                                        c->alfa, c->beta);
+  const int nt = (g.nx + 31) / 32 * 32;
+  k_xys_acc<<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
+                                                               c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
+  const size_t plane = (size_t)g.nyp * g.nx;
+  const int nb = (int)((plane + 255) / 256);
+  k_xys_add<<<nb, 256, 0, c->stream>>>(c->xys_part, c->xys, G);
+  k_xys_minmax<<<nb, 256, 0, c->stream>>>(c->xys_u, c->xys, G);
+  c->launches += 4;
+  c->xys_sumw += dtn;
+  CK(cudaGetLastError());
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_xys_get(sgpu_ctx* c, double* xys, double* sumw) {
+  if (!c || !xys) return SGPU_E_PARAM;
+  const Dims& g = c->g;
+  const size_t bytes = XYS_NS * (size_t)g.nyp * g.nx * sizeof(double);
+  if (!c->xys) {
+    memset(xys, 0, bytes);
+  } else {
+    CK(cudaMemcpyAsync(xys, c->xys, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  if (sumw) *sumw = c->xys_sumw;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_xys_reset(sgpu_ctx* c) {
+  if (!c) return SGPU_E_PARAM;
+  if (c->xys) CK(cudaMemsetAsync(c->xys, 0, XYS_NS * (size_t)c->g.nyp * c->g.nx * sizeof(double), c->stream));
+  c->xys_sumw = 0.0;
+  return SGPU_OK;
+}
+
 extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
   if (c && sharded(c)) return SGPU_E_STATE;  // statistics read the whole state
   if (!c || !amp) return SGPU_E_PARAM;

@@ -1,0 +1,78 @@
+"""xy statistics on the device (sgpu_xys_sample, the reference's
+bla/boxxys.f as bla/bla.f:2069-2107 samples it) against the translated
+reference run on the same state: every entry the reference fills without
+pressure, LES or MHD, two samples with different weights (running sums and
+the running min / max of entries 43-44), content in the kz = -nz/2 plane
+ignored as the reference's getxz ignores it.  FP64 path within 1e-12 of each
+entry's largest value; the mixed path (FP32 state storage) within 1e-5.
+Entry 51 (<dw/dz>_z, the z average of a z derivative) vanishes analytically
+and holds roundoff; it is measured against the scale of the other strain-rate
+entries 46-50."""
+import numpy as np
+import pytest
+
+from simson_b200.fields import channel_field
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ, RE, XL, ZL, DT = 48, 65, 48, 4200.0, 4 * np.pi, 2 * np.pi, 0.01
+# entries (1-based) boxxys fills with pressure = 0, no LES, no MHD
+FILLED = list(range(1, 16)) + list(range(25, 31)) + list(range(43, 52)) + list(range(63, 73)) + [75, 76, 77]
+
+
+def with_oddball(state, seed):
+    """Add content to the kz = -nz/2 plane of slots 1-5 (kx > 0), which the
+    statistics must not see."""
+    rng = np.random.default_rng(seed)
+    out = [np.array(s) for s in state]
+    for k in range(5):
+        sh = out[k][NZ // 2, :, 1:].shape
+        out[k][NZ // 2, :, 1:] += 1e-3 * (rng.standard_normal(sh) + 1j * rng.standard_normal(sh))
+    return out
+
+
+def compare(got, ref, tol):
+    errs = {}
+    for s in range(96):
+        scale = np.abs(ref[s]).max()
+        if s + 1 in FILLED:
+            assert scale > 0.0, f"entry {s + 1} not filled by the reference"
+            if s + 1 == 51:
+                scale = max(scale, np.abs(ref[45:50]).max())
+            errs[s + 1] = float(np.abs(got[s] - ref[s]).max() / scale)
+        else:
+            assert scale == 0.0 and np.abs(got[s]).max() == 0.0, f"entry {s + 1}"
+    worst = max(errs, key=errs.get)
+    print("worst entry", worst, "%.2e" % errs[worst])
+    assert errs[worst] <= tol, (worst, errs[worst])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_xys_matches_reference(need_ref, precision):
+    need_ref(NX, NY, NZ)
+    from refsim import RefSim
+    from simson_b200.bla import Channel
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.05, 5)
+    ref = RefSim(NX, NY, NZ, RE, XL, ZL, DT)
+    ref.set_velocity(u, v, w)
+    ref.start()
+    ref.step(2)
+    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT, precision=precision)
+    try:
+        tol = 1e-12 if precision == "fp64" else 1e-5
+        for i, dtn in enumerate((DT, 0.7 * DT)):
+            st = with_oddball(ref.state(), 7 + i)
+            for k in range(5):
+                ref.set_slot(k + 1, st[k])
+            xr, swr = ref.xys(dtn, reset=(i == 0))
+            ch.set_state(st)
+            ch.xys_sample(dtn)
+            xg, swg = ch.xys()
+            assert swg == swr
+            compare(xg, xr, tol)
+            ref.step(1)
+        ch.xys_reset()
+        xg, swg = ch.xys()
+        assert swg == 0.0 and not xg.any()
+    finally:
+        ch.close()
