@@ -125,6 +125,13 @@ struct sgpu_ctx {
   static constexpr int kbf = MIXED_KB, rbf = MIXED_RB, pbf = 8;  // FP32 tiles (mixed.h)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
+  // CUDA graph of one whole RK3 step (sgpu_step_rk), replayed while the step's
+  // launch pattern stays the same
+  cudaGraphExec_t step_exec = nullptr;
+  bool step_valid = false;
+  unsigned step_key = 0;         // CFL substep mask and LES mode of the captured step
+  long long step_launches = 0;   // kernels one captured step launches
+  bool graphs = true;
   std::vector<cudaEvent_t> pev;
   std::vector<int> pid;
   int pnext = 0;
@@ -379,6 +386,9 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
   c->dtn = P.dt;
+  // SIMSON_GRAPHS=0: launch every kernel directly (no CUDA-graph replay)
+  const char* ge = getenv("SIMSON_GRAPHS");
+  c->graphs = !(ge && ge[0] == '0');
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
   return SGPU_OK;
@@ -387,6 +397,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
 extern "C" int sgpu_finalize(sgpu_ctx* c) {
   if (!c) return SGPU_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
@@ -575,6 +586,7 @@ struct WholeDomain {
 };
 
 extern "C" int sgpu_set_shard(sgpu_ctx* c, int ylo, int yhi, int zlo, int zhi) {
+  if (c) c->step_valid = false;  // the captured step no longer matches
   if (!c) return SGPU_E_PARAM;
   const Dims& g = c->g;
   if (ylo < 0 || yhi > g.nyp || ylo >= yhi || zlo < 0 || zhi > g.nz || zlo >= zhi) return SGPU_E_PARAM;
@@ -800,16 +812,26 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   return cuda_fail(cudaGetLastError(), "nonlin launch");
 }
 
-static int enqueue_linear(sgpu_ctx* c) {
-  const Dims& g = c->g;
-  const sgpu_params& P = c->prm;
-  // RK weights (bla/bla.f:2384-2397)
+// RK weights of the coming linear step (bla/bla.f:2384-2397)
+static void rk_advance(sgpu_ctx* c) {
   c->an = c->anp1;
   c->bn = c->bnp1;
   const int k = c->it % 3;
   c->anp1 = c->dtn * ANRK[k];
   c->bnp1 = c->dtn * BNRK[k];
   c->cnp1 = c->dtn * CNRK[k];
+}
+
+// substep counter and time after a linear step (bla/bla.f:2598-2607)
+static void it_advance(sgpu_ctx* c) {
+  c->it += 1;
+  if ((c->it - 1) % 3 == 0) c->t = c->t + c->dtn;
+}
+
+static int enqueue_linear(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const sgpu_params& P = c->prm;
+  rk_advance(c);
   RKc rk{c->an, c->bn, c->anp1, c->bnp1};
   // Chebyshev transform of H, normalised by 1/(nxp nzp) (linearbl.f:262-273)
   prof_mark(c, K_CHEB_FWD);
@@ -882,9 +904,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   if (c->iles == 1) les_filter_velocity(c, 1);
   prof_mark(c, K_OTHER);
   c->launches += 2;
-  // bla/bla.f:2598-2607
-  c->it += 1;
-  if ((c->it - 1) % 3 == 0) c->t = c->t + c->dtn;
+  it_advance(c);
   return cuda_fail(cudaGetLastError(), "linear launch");
 }
 
@@ -916,17 +936,123 @@ extern "C" int sgpu_linear(sgpu_ctx* c) {
   return enqueue_linear(c);
 }
 
+// Launch pattern of the RK3 step that starts now: bits 0-2 the substeps that
+// evaluate the CFL number, bits 3-5 the LES mode.  0xffffffff: the step cannot
+// be replayed (not at a step boundary, or a stage's homogeneous solutions not
+// yet cached: that substep launches k_pencil_hom).
+static unsigned step_pattern(const sgpu_ctx* c) {
+  if ((c->it - 1) % 3 != 0) return 0xffffffffu;
+  unsigned key = (unsigned)c->iles << 3;
+  double anp1 = c->anp1, bnp1 = c->bnp1;
+  for (int s = 0; s < 3; ++s) {
+    const int it = c->it + s;
+    if (c->prm.icfl > 0 && (it - 1) % c->prm.icfl == 0) key |= 1u << s;
+    const double anbn = anp1 + bnp1;  // a_n + b_n of this substep's linear step
+    bool cached = false;
+    for (int h = 0; h < 3; ++h) cached = cached || c->hom_key[h] == anbn;
+    if (!cached) return 0xffffffffu;
+    anp1 = c->dtn * ANRK[it % 3];
+    bnp1 = c->dtn * BNRK[it % 3];
+  }
+  return key;
+}
+
+// Capture the three substeps of this step into c->step_exec (launching
+// nothing); the host bookkeeping advances as in a direct launch.  On failure
+// the host state is restored and the caller launches directly.
+static int capture_step(sgpu_ctx* c, unsigned key) {
+  const double an = c->an, bn = c->bn, anp1 = c->anp1, bnp1 = c->bnp1, cnp1 = c->cnp1, t = c->t, tc = c->tc;
+  const int it = c->it;
+  const long long launches = c->launches;
+  const bool cfl_pending = c->cfl_pending;
+  auto restore = [&] {
+    c->an = an; c->bn = bn; c->anp1 = anp1; c->bnp1 = bnp1; c->cnp1 = cnp1; c->t = t; c->tc = tc; c->it = it;
+    c->launches = launches; c->cfl_pending = cfl_pending;
+  };
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return SGPU_E_CUDA;
+  }
+  int r = SGPU_OK;
+  for (int s = 0; s < 3 && r == SGPU_OK; ++s) {
+    r = enqueue_nonlin(c);
+    if (r == SGPU_OK) r = enqueue_linear(c);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (r != SGPU_OK || e != cudaSuccess || !graph) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    restore();
+    return SGPU_E_CUDA;
+  }
+  bool ok = false;
+  if (c->step_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    ok = cudaGraphExecUpdate(c->step_exec, graph, &info) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(c->step_exec);
+      c->step_exec = nullptr;
+    }
+  }
+  if (!ok) ok = cudaGraphInstantiate(&c->step_exec, graph, 0) == cudaSuccess;
+  cudaGraphDestroy(graph);
+  if (!ok) {
+    cudaGetLastError();
+    c->step_exec = nullptr;
+    c->step_valid = false;
+    restore();
+    return SGPU_E_CUDA;
+  }
+  c->step_valid = true;
+  c->step_key = key;
+  c->step_launches = c->launches - launches;
+  return SGPU_OK;
+}
+
+// Host side of one replayed step: what enqueue_nonlin / enqueue_linear do to
+// the bookkeeping, without launching.
+static void replay_host(sgpu_ctx* c) {
+  for (int s = 0; s < 3; ++s) {
+    c->tc = c->t + c->cnp1;
+    rk_advance(c);
+    it_advance(c);
+  }
+  if (c->step_key & 7u) c->cfl_pending = true;
+  c->launches += c->step_launches;
+}
+
 extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
   if (!c || nsub < 0) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
   // a shard needs the block exchanges between its two steps (host-driven)
   if (sharded(c)) return SGPU_E_STATE;
-  for (int s = 0; s < nsub; ++s) {
+  int s = 0;
+  while (s < nsub) {
+    // whole steps with an unchanged launch pattern replay one CUDA graph;
+    // the rest (first steps, profiling, partial steps) launch directly
+    const unsigned key = (c->graphs && !c->prof && nsub - s >= 3) ? step_pattern(c) : 0xffffffffu;
+    if (key != 0xffffffffu) {
+      if (c->step_valid && c->step_key == key) {
+        CK(cudaGraphLaunch(c->step_exec, c->stream));
+        replay_host(c);
+        s += 3;
+        continue;
+      }
+      if (capture_step(c, key) == SGPU_OK) {
+        CK(cudaGraphLaunch(c->step_exec, c->stream));
+        s += 3;
+        continue;
+      }
+      c->graphs = false;  // capture not possible here: launch directly from now on
+    }
     // the CFL word is read back lazily (sgpu_get_scalars): no host sync per substep
     int r = enqueue_nonlin(c);
     if (r) return r;
     r = enqueue_linear(c);
     if (r) return r;
+    ++s;
   }
   return SGPU_OK;
 }
@@ -1261,6 +1387,7 @@ static int sgs_setup(sgpu_ctx* c) {
 // ADM-RT large-eddy model (bla/rparamles.f, bla/bla.f:1489-1518, 2212-2231):
 // filter tables on the host (les_filter.h), gu and the tables on the device.
 extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
+  if (c) c->step_valid = false;  // the captured step no longer matches
   if (c && sharded(c) && p && p->iles != 0) return SGPU_E_PARAM;  // LES needs the whole domain
   if (!c || !p) return SGPU_E_PARAM;
   if (p->iles == 0) {
@@ -1365,6 +1492,7 @@ static int mlp_image_upload(sgpu_ctx* c, const sgpu_sgs_mlp* p) {
 }
 
 extern "C" int sgpu_set_sgs_mlp(sgpu_ctx* c, const sgpu_sgs_mlp* p) {
+  if (c) c->step_valid = false;  // the captured step no longer matches
   if (!c || !p) return SGPU_E_PARAM;
   int rc = mlp_image_upload(c, p);
   if (rc) return rc;
