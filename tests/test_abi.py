@@ -28,3 +28,52 @@ def test_library_exports_every_declared_function():
     lib = ctypes.CDLL(build.build())
     missing = [n for n in declared() if not hasattr(lib, n)]
     assert not missing, missing
+
+
+SGPU_E_PARAM = -1
+
+
+def _lib():
+    from simson_b200 import build
+    from simson_b200.bla import load_library
+    build.build()
+    return load_library(build=False)
+
+
+def test_init_rejects_invalid_parameters():
+    """sgpu_init validates the grid and the run parameters before it touches
+    the device (nx a multiple of 4, nz even, ny odd and >= 9, nst = 3,
+    dt, Re and box lengths positive, a known precision)."""
+    from simson_b200.bla import SgpuParams
+    lib = _lib()
+    good = dict(nx=48, ny=65, nz=48, re=4200.0, xl=12.566, zl=6.283, dt=0.01, nst=3, cflux=1, mflux=4.0 / 3.0,
+                px=-2.0 / 4200.0, rot=0.0, icfl=3, precision=0, device=0)
+    bad = [dict(nx=46), dict(nx=0), dict(nz=47), dict(ny=64), dict(ny=7), dict(nst=4), dict(dt=0.0), dict(dt=-1.0),
+           dict(re=0.0), dict(xl=0.0), dict(zl=-1.0), dict(precision=2), dict(dt=float("nan"))]
+    for change in bad:
+        p = SgpuParams(**{**good, **change})
+        ctx = ctypes.c_void_p(1)
+        rc = lib.sgpu_init(ctypes.byref(p), ctypes.byref(ctx))
+        assert rc == SGPU_E_PARAM, change
+        assert not ctx.value, change
+    assert lib.sgpu_init(None, None) == SGPU_E_PARAM
+
+
+def test_entry_points_reject_a_null_context():
+    lib = _lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    buf = (ctypes.c_double * 16)()
+    p = ctypes.cast(buf, dp)
+    assert lib.sgpu_prhs(None) == SGPU_E_PARAM
+    assert lib.sgpu_nonlin(None) == SGPU_E_PARAM
+    assert lib.sgpu_linear(None) == SGPU_E_PARAM
+    assert lib.sgpu_step_rk(None, 3) == SGPU_E_PARAM
+    assert lib.sgpu_offload_steps(None, p, p, 1) == SGPU_E_PARAM
+    assert lib.sgpu_amplitudes(None, p, p) == SGPU_E_PARAM
+    assert lib.sgpu_xys_sample(None, ctypes.c_double(0.01)) == SGPU_E_PARAM
+    assert lib.sgpu_xys_get(None, p, p) == SGPU_E_PARAM
+    assert lib.sgpu_xys_reset(None) == SGPU_E_PARAM
+    assert lib.sgpu_set_shard(None, 0, 1, 0, 1) == SGPU_E_PARAM
+    assert lib.sgpu_finalize(None) == 0
+    for rc in (0, -1, -2, -3, -4, -5):
+        assert lib.sgpu_error_string(rc)
