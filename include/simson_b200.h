@@ -176,6 +176,17 @@ int sgpu_xys_get(sgpu_ctx* ctx, double* xys, double* sumw);
 /* Zero the running sums (a new averaging period, bla/bla.f:1573). */
 int sgpu_xys_reset(sgpu_ctx* ctx);
 
+/* Training sample for the learned SGS stress (sgpu_set_sgs_mlp) from the
+ * resolved state.  No reference counterpart (the reference's dynamic model
+ * forms the analogous filtered products internally with a spectral cut-off,
+ * bla/les.f:709-881): here a top-hat box filter over cells of f x f points of
+ * the nx x nz grid (f divides nx and nz; y unfiltered).  Per point of the coarse grid
+ * (ny x nz/f x nx/f, x fastest): features[10] = the nine filtered velocity
+ * gradients du_i/dx_j (i-major) and the wall distance 1 - |y|, targets[6] =
+ * tau_ij = <u_i u_j> - <u_i><u_j> (11 12 13 22 23 33), float.  Synchronises
+ * the library's stream.  Not on a shard. */
+int sgpu_box_filter_sample(sgpu_ctx* ctx, int factor, float* features, float* targets);
+
 /* The driver keeps the state: advance it by nsteps RK3 steps, each step
  * uploading all 7 slots from ur, ui (reference layout, as sgpu_upload_state;
  * pinned host memory for full speed) and downloading the result into them

@@ -93,6 +93,30 @@ def learned_tau(state, alfa, beta, nx, nz, w, s_in, s_y, s_out):
     return np.stack([_to_spec(tau[..., c] / (nx * nz), nz) for c in range(6)])
 
 
+def box_filter_sample(state, alfa, beta, nx, nz, f):
+    """Training sample of the learned model (sgpu_box_filter_sample): top-hat
+    averages over cells of f x f points of the nx x nz grid of u_i, of the
+    gradients and of u_i u_j; returns features (nyp, nz/f, nx/f, 10) = the
+    nine filtered gradients and 1 - |y|, targets (nyp, nz/f, nx/f, 6) =
+    <u_i u_j> - <u_i><u_j> (11 12 13 22 23 33), float64."""
+    u, v, ww, ox, oz = state[:5]
+    nyp = u.shape[1]
+    vel = np.stack([_to_phys(q, nx, nz) for q in (u, v, ww)])
+    grad = velocity_gradient(u, v, ww, ox, oz, alfa, beta, nx, nz)
+
+    def box(p):
+        return p.reshape(p.shape[:-2] + (nz // f, f, nx // f, f)).mean(axis=(-3, -1))
+
+    ub = box(vel)
+    pairs = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
+    tau = np.stack([box(vel[i] * vel[j]) - ub[i] * ub[j] for i, j in pairs])
+    eta = np.cos(np.pi * np.arange(nyp) / (nyp - 1))
+    feats = np.empty((nyp, nz // f, nx // f, 10))
+    feats[..., :9] = np.moveaxis(box(grad), 0, -1)
+    feats[..., 9] = (1.0 - np.abs(eta))[:, None, None]
+    return feats, np.moveaxis(tau, 0, -1)
+
+
 def viscosity_weights(nu_t, a=0.1, s_in=0.2):
     """Weights under which the network is, to O((a s_in du)^2), the linear
     eddy-viscosity stress tau_ij = -2 nu_t S_ij: layer 1 passes the nine

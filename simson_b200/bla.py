@@ -89,6 +89,8 @@ def load_library(build: bool = True):
     lib.sgpu_xys_sample.argtypes = [vp, ctypes.c_double]
     lib.sgpu_xys_get.argtypes = [vp, dp, dp]
     lib.sgpu_xys_reset.argtypes = [vp]
+    lib.sgpu_box_filter_sample.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_float)]
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
@@ -323,6 +325,18 @@ class Channel:
 
     def xys_reset(self):
         self._check(self.lib.sgpu_xys_reset(self._ctx), "xys_reset")
+
+    def box_filter_sample(self, factor=4):
+        """Training sample of the learned SGS model from the current state:
+        (features (ny, nz/f, nx/f, 10), targets (ny, nz/f, nx/f, 6)), float32;
+        see sgpu_box_filter_sample."""
+        shape = (self.ny, self.nz // factor, self.nx // factor)
+        feats = np.empty(shape + (10,), np.float32)
+        tau = np.empty(shape + (6,), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.sgpu_box_filter_sample(self._ctx, int(factor), feats.ctypes.data_as(fp),
+                                                    tau.ctypes.data_as(fp)), "box_filter_sample")
+        return feats, tau
 
     KERNELS = ("zinv", "xpass", "zfwd", "cheb_fwd", "pencil", "mean", "cheb_inv", "other")
 

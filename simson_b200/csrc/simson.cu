@@ -112,6 +112,8 @@ struct sgpu_ctx {
   double* xys_u = nullptr;
   double xys_sumw = 0.0;
   Tw xys_twz, xys_twx;
+  float* box_out = nullptr;  // sgpu_box_filter_sample: features then targets
+  size_t box_n = 0;          // coarse points box_out holds
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
   int it = 1;
@@ -401,7 +403,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
-                  c->xys_part, c->xys_u, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
+                  c->xys_part, c->xys_u, c->box_out, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
@@ -1217,6 +1219,53 @@ static int xys_setup(sgpu_ctx* c) {
   cudaFuncSetAttribute(k_xys_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
   cudaFuncSetAttribute(k_xys_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
   cudaFuncSetAttribute(k_xys_acc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  cudaFuncSetAttribute(k_box_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  return SGPU_OK;
+}
+
+// The 15 spectral fields of the statistics on the nx x nz grid, z physical.
+static void xys_fields(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const SgsGrid G = sgs_grid(c);
+  constexpr int KB = 4;
+  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
+  const dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
+  if (c->mixed)
+    k_xys_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+                                                       c->alfa, c->beta);
+  else
+    k_xys_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+                                                        c->alfa, c->beta);
+  c->launches++;
+}
+
+extern "C" int sgpu_box_filter_sample(sgpu_ctx* c, int factor, float* features, float* targets) {
+  if (c && sharded(c)) return SGPU_E_STATE;  // reads the whole state
+  if (!c || !features || !targets || factor < 1) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  const Dims& g = c->g;
+  if (g.nx % factor || g.nz % factor) return SGPU_E_PARAM;
+  int rc = xys_setup(c);
+  if (rc) return rc;
+  const int nxc = g.nx / factor, nzc = g.nz / factor;
+  const size_t npts = (size_t)g.nyp * nzc * nxc;
+  if (c->box_n < npts) {
+    if (c->box_out) cudaFree(c->box_out);
+    c->box_out = nullptr;
+    c->box_n = 0;
+    if (cudaMalloc(&c->box_out, npts * 16 * sizeof(float)) != cudaSuccess) return SGPU_E_CUDA;
+    c->box_n = npts;
+  }
+  xys_fields(c);
+  const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
+  const int nt = std::max(128, (nxc + 31) / 32 * 32);
+  k_box_sample<<<dim3(nzc, g.nyp), nt, sx, c->stream>>>(c->xys_spec, sgs_grid(c), c->xys_twx.plan, c->xys_twx.d,
+                                                        factor, c->box_out, c->box_out + npts * 10);
+  c->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(features, c->box_out, npts * 10 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(targets, c->box_out + npts * 10, npts * 6 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
 }
 
@@ -1228,16 +1277,8 @@ extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
   if (rc) return rc;
   const Dims& g = c->g;
   const SgsGrid G = sgs_grid(c);
-  constexpr int KB = 4;
-  const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
   const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
-  const dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
-  if (c->mixed)
-    k_xys_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
-                                                       c->alfa, c->beta);
-  else
-    k_xys_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
-                                                        c->alfa, c->beta);
+  xys_fields(c);
   const int nt = (g.nx + 31) / 32 * 32;
   k_xys_acc<<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
                                                                c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
@@ -1245,7 +1286,7 @@ extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
   const int nb = (int)((plane + 255) / 256);
   k_xys_add<<<nb, 256, 0, c->stream>>>(c->xys_part, c->xys, G);
   k_xys_minmax<<<nb, 256, 0, c->stream>>>(c->xys_u, c->xys, G);
-  c->launches += 4;
+  c->launches += 3;
   c->xys_sumw += dtn;
   CK(cudaGetLastError());
   return SGPU_OK;

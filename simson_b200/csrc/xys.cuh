@@ -225,4 +225,78 @@ __global__ void k_xys_minmax(const double* __restrict__ uphys, double* __restric
   xys[(size_t)43 * plane + i] = umax;
 }
 
+// Training sample of the learned SGS model from the resolved state (the box
+// filtering of the high-resolution channel that produces its data): on the
+// nx x nz grid, per y-plane, the top-hat average over cells of f x f points
+// (x in [f X, f X + f), z in [f Z, f Z + f)) of u_i, of the nine gradients
+// du_i/dx_j and of the products u_i u_j.  Per coarse point, features[10] =
+// the nine filtered gradients (i-major) and the wall distance 1 - |y|, and
+// targets[6] = tau_ij = <u_i u_j> - <u_i> <u_j> (11 12 13 22 23 33): the
+// inputs and the output of the model of sgs_mlp.cuh, unscaled.  One CTA per
+// (Z, y), blockDim >= nx / f; reads the spectral fields of k_xys_zinv.
+__global__ void __launch_bounds__(512) k_box_sample(const double2* __restrict__ spec, SgsGrid G, FFTPlan plan,
+                                                    const double2* __restrict__ tw, int f,
+                                                    float* __restrict__ features, float* __restrict__ targets) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* bA = reinterpret_cast<double2*>(smem_raw);
+  double2* bB = bA + (size_t)G.nx * XYS_NC;
+  const int Z = blockIdx.x, y = blockIdx.y;
+  const int n = G.nx, nxc = G.nx / f, nzc = G.nz / f;
+  const int X = threadIdx.x;
+  const size_t fs = (size_t)G.nyp * G.nz * G.nx2;
+  double acc[18];
+#pragma unroll
+  for (int k = 0; k < 18; ++k) acc[k] = 0.0;
+  for (int rr = 0; rr < f; ++rr) {
+    const size_t row = ((size_t)y * G.nz + (size_t)f * Z + rr) * G.nx2;
+    for (int t = threadIdx.x; t < n * XYS_NC; t += blockDim.x) {
+      const int k = t / XYS_NC, cc = t - XYS_NC * (t / XYS_NC);
+      const double2* a = spec + (size_t)(2 * cc) * fs + row;
+      const double2* b = (2 * cc + 1 < XYS_NF) ? spec + (size_t)(2 * cc + 1) * fs + row : nullptr;
+      bA[k * XYS_NC + cc] = sgs_pair(a, b, k, n, G.nx2);
+    }
+    __syncthreads();
+    const double2* res = fft_columns<double, XYS_NC>(bA, bB, plan, tw, +1);
+    if (X < nxc) {
+      for (int xx = 0; xx < f; ++xx) {
+        const int j = f * X + xx;
+        double q[16];
+#pragma unroll
+        for (int cc = 0; cc < XYS_NC; ++cc) {
+          const double2 zv = res[j * XYS_NC + cc];
+          q[2 * cc] = zv.x;
+          q[2 * cc + 1] = zv.y;
+        }
+        const double u = q[0], v = q[1], w = q[2];
+        acc[0] += u;
+        acc[1] += v;
+        acc[2] += w;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[3 + k] += q[6 + k];
+        acc[12] += u * u;
+        acc[13] += u * v;
+        acc[14] += u * w;
+        acc[15] += v * v;
+        acc[16] += v * w;
+        acc[17] += w * w;
+      }
+    }
+    __syncthreads();
+  }
+  if (X < nxc) {
+    const double inv = 1.0 / ((double)f * (double)f);
+    const double ub[3] = {acc[0] * inv, acc[1] * inv, acc[2] * inv};
+    const size_t pt = ((size_t)y * nzc + Z) * nxc + X;
+    float* fo = features + pt * 10;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fo[k] = (float)(acc[3 + k] * inv);
+    const double eta = cos(3.14159265358979323846 * (double)y / (double)(G.nyp - 1));
+    fo[9] = (float)(1.0 - fabs(eta));
+    float* to = targets + pt * 6;
+    const int pi_[6] = {0, 0, 0, 1, 1, 2}, pj_[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) to[c] = (float)(acc[12 + c] * inv - ub[pi_[c]] * ub[pj_[c]]);
+  }
+}
+
 }  // namespace sb
