@@ -82,7 +82,11 @@ int sgpu_linear(sgpu_ctx* ctx);
 int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
 
 /* Scalars, in this order: px, mflux, t, cfl (CFL*dt of the last evaluated
- * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises. */
+ * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises.
+ * Returns SGPU_E_CFL when CFL*dt > 10 (the reference's stop, wcflbl.f:93)
+ * and SGPU_E_NAN when px or the mass flux is not finite (a non-finite value
+ * anywhere in u, v, w reaches them within one substep); the driver calls it
+ * after each step it checks, as the reference checks every icfl substeps. */
 int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
 /* Large-eddy model, the reference's sgs.i (bla/rparamles.f:31-60):

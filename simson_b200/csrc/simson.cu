@@ -646,6 +646,10 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   c->it = 1;
   c->t = 0.0;
   c->tc = 0.0;
+  // px and the mass flux of the run's start (bla/bla.f:1622-1633): a restart
+  // on the same context does not inherit the last run's values
+  const double sc0[4] = {c->prm.px, c->prm.mflux, 0.0, 0.0};
+  CK(cudaMemcpyAsync(c->scal, sc0, sizeof(sc0), cudaMemcpyHostToDevice, c->stream));
   // Chebyshev coefficients of u, v, w, from the FP64 copy uploaded with the
   // state (also under SGPU_MIXED: p_v needs four y-derivatives of v)
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->st, fld, czf(c, 0), fld, 3, 0, 1.0, 0, c->twy.d);
@@ -1127,6 +1131,10 @@ extern "C" int sgpu_get_scalars(sgpu_ctx* c, double* out, int n) {
     fprintf(stderr, "simson_b200: tensor-core Chebyshev transform: a wait timed out\n");
     return SGPU_E_CUDA;
   }
+  // a non-finite value anywhere in u, v, w reaches the kx = kz = 0 mode of H
+  // through the forward transforms within one substep, and with it px
+  // (constant flux) or the mass flux
+  if (r == SGPU_OK && c->have_state && !(std::isfinite(sc[0]) && std::isfinite(sc[1]))) return SGPU_E_NAN;
   return r;
 }
 
