@@ -21,6 +21,8 @@
 #include "les_dyn.cuh"
 #include "sgs_mlp.cuh"
 #include "xys.cuh"
+
+#include <nvtx3/nvToolsExt.h>
 #include "mixed.h"
 #include "step2_launch.cuh"
 #include "cheb_tc.cuh"
@@ -140,6 +142,15 @@ struct sgpu_ctx {
 };
 
 enum KernelId { K_ZINV = 0, K_XPASS, K_ZFWD, K_CHEB_FWD, K_PENCIL, K_MEAN, K_CHEB_INV, K_OTHER, K_COUNT };
+
+// NVTX range over a host scope (phases of the step for nsys / ncu --nvtx;
+// no-ops unless a tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 static void prof_mark(sgpu_ctx* c, int id) {
   if (!c->prof) return;
@@ -631,6 +642,7 @@ extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int 
 }
 
 extern "C" int sgpu_prhs(sgpu_ctx* c) {
+  NvtxRange nv("prhs");
   if (!c) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
   WholeDomain whole(c);
@@ -752,6 +764,7 @@ static void enqueue_sgs(sgpu_ctx* c) {
 }
 
 static int enqueue_nonlin(sgpu_ctx* c) {
+  NvtxRange nv("step 2 (nonlinbl)");
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   c->tc = c->t + c->cnp1;
@@ -835,6 +848,7 @@ static void it_advance(sgpu_ctx* c) {
 }
 
 static int enqueue_linear(sgpu_ctx* c) {
+  NvtxRange nv("step 3 (linearbl)");
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   rk_advance(c);
@@ -967,6 +981,7 @@ static unsigned step_pattern(const sgpu_ctx* c) {
 // nothing); the host bookkeeping advances as in a direct launch.  On failure
 // the host state is restored and the caller launches directly.
 static int capture_step(sgpu_ctx* c, unsigned key) {
+  NvtxRange nv("capture RK3 step");
   const double an = c->an, bn = c->bn, anp1 = c->anp1, bnp1 = c->bnp1, cnp1 = c->cnp1, t = c->t, tc = c->tc;
   const int it = c->it;
   const long long launches = c->launches;
@@ -1041,6 +1056,7 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
     const unsigned key = (c->graphs && !c->prof && nsub - s >= 3) ? step_pattern(c) : 0xffffffffu;
     if (key != 0xffffffffu) {
       if (c->step_valid && c->step_key == key) {
+        NvtxRange nv("RK3 step (graph)");
         CK(cudaGraphLaunch(c->step_exec, c->stream));
         replay_host(c);
         s += 3;
@@ -1064,6 +1080,7 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
 }
 
 extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
+  NvtxRange nv("offload steps");
   if (!c || !ur || !ui || nsteps < 0) return SGPU_E_PARAM;
   if (sharded(c)) return SGPU_E_STATE;
   const Dims& g = c->g;
@@ -1278,6 +1295,7 @@ extern "C" int sgpu_box_filter_sample(sgpu_ctx* c, int factor, float* features, 
 }
 
 extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
+  NvtxRange nv("xy statistics");
   if (c && sharded(c)) return SGPU_E_STATE;  // statistics read the whole state
   if (!c || !(dtn >= 0.0)) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;

@@ -44,6 +44,17 @@ def run(graphs, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_runs_are_deterministic(precision):
+    """Same inputs, same bytes: two runs of the same sequence (no atomics
+    whose order reaches a result: the CFL maximum is order-free)."""
+    s1, sc1, _ = run(True, precision)
+    s2, sc2, _ = run(True, precision)
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    assert sc1 == sc2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_replay_equals_direct_launches(precision):
     s_g, sc_g, l_g = run(True, precision)
     s_d, sc_d, l_d = run(False, precision)
