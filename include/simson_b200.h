@@ -180,6 +180,15 @@ int sgpu_xys_get(sgpu_ctx* ctx, double* xys, double* sumw);
 /* Zero the running sums (a new averaging period, bla/bla.f:1573). */
 int sgpu_xys_reset(sgpu_ctx* ctx);
 
+/* Pressure of the current state, as bla/bla.f:2486-2527 computes it after a
+ * step whose field is saved (bla/nonlinp.f, bla/linearp.f: the Poisson
+ * equation with the Neumann conditions of the wall-normal momentum equation,
+ * the mean mode by integration of H2): p in the layout of one slot of ur, ui
+ * (Fourier x/z, physical y; the kz = -nz/2 plane is zero).  The state is not
+ * changed.  FP64 contexts only (SGPU_E_PARAM under SGPU_MIXED).
+ * Synchronises the library's stream.  Not on a shard. */
+int sgpu_pressure(sgpu_ctx* ctx, double* pr, double* pi);
+
 /* Training sample for the learned SGS stress (sgpu_set_sgs_mlp) from the
  * resolved state.  No reference counterpart (the reference's dynamic model
  * forms the analogous filtered products internally with a spectral cut-off,

@@ -5,7 +5,8 @@ TEST INFRASTRUCTURE ONLY (see ``oracle/f77c.py``).  The product never loads it.
 It reads the reference's Fortran sources where they lie (``$SIMSON_REFERENCE``,
 default the read-only reference checkout), edits only the compile-time grid
 in ``par.f`` exactly as the reference's own instructions say to do per case
-(nx, ny, nz, nthread, pressure=0), translates the hot-path units to C with
+(nx, ny, nz, nthread, and pressure = 0, or 1 for the pressure variant in
+``oracle/_ref/<grid>_p``), translates the hot-path units to C with
 ``oracle/f77c.py`` and compiles them, together with ``oracle/ref_harness.c``,
 with ``gcc -O3 -fopenmp``.  Nothing derived from the reference is written
 outside ``oracle/_ref/`` (git-ignored).
@@ -23,6 +24,7 @@ Translated units (reference file: what it contributes):
   bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
   bla/boxamp.f                                                             (plane statistics)
   bla/boxxys.f xzsh.f + bla.f 2069-2107                                    (xy statistics)
+  bla/nonlinp.f linearp.f crhsc.f setmac.f tridc.f icheb.f + bla.f 2486-2527 (pressure)
   bla/init_filter.f lpf_y.f hpf_y.f bandsolver.f + bla.f 1489-1545         (ADM-RT LES filters)
   bla/les.f sgs_stress.f filter_cutoff.f + bla.f 1945-2020                 (eddy-viscosity LES)
 For grids up to SMAG_MAX_POINTS the driver's compile-time switch iiles_smag
@@ -54,6 +56,7 @@ UNIT_FILES = [
     "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
     "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
     "les.f", "sgs_stress.f", "filter_cutoff.f", "boxxys.f", "xzsh.f",
+    "nonlinp.f", "linearp.f", "crhsc.f", "setmac.f", "tridc.f", "icheb.f",
 ]
 
 MAIN_RANGES = [
@@ -71,6 +74,7 @@ MAIN_RANGES = [
     ("bla_cfl", 2349, 2351),
     ("bla_rkweights", 2384, 2397),
     ("bla_linear", 2433, 2475),
+    ("bla_press", 2486, 2527),
     ("bla_itinc", 2598, 2598),
 ]
 
@@ -79,19 +83,19 @@ SMAG_MAX_POINTS = 2_000_000  # nx*ny*nz; larger oracle grids keep iiles_smag = 0
 NTHREAD = 64  # compile-time thread slots (par.f nthread); the harness never runs more
 
 
-def par_text(nx: int, ny: int, nz: int, nthread: int = NTHREAD) -> str:
+def par_text(nx: int, ny: int, nz: int, nthread: int = NTHREAD, pressure: bool = False) -> str:
     with open(os.path.join(REF_BLA, "par.f")) as f:
         txt = f.read()
     txt, n1 = re.subn(r"parameter \(nx=\d+,ny=\d+,nz=\d+\)",
                       f"parameter (nx={nx},ny={ny},nz={nz})", txt)
     txt, n2 = re.subn(r"parameter \(nthread=\d+\)", f"parameter (nthread={nthread})", txt)
-    txt, n3 = re.subn(r"parameter \(pressure=\d\)", "parameter (pressure=0)", txt)
+    txt, n3 = re.subn(r"parameter \(pressure=\d\)", f"parameter (pressure={1 if pressure else 0})", txt)
     if (n1, n2, n3) != (1, 1, 1):
         raise RuntimeError("par.f layout not recognised")
     return txt
 
 
-def generate_c(nx: int, ny: int, nz: int) -> str:
+def generate_c(nx: int, ny: int, nz: int, pressure: bool = False) -> str:
     sources = []
     for fn in UNIT_FILES:
         with open(os.path.join(REF_BLA, fn)) as f:
@@ -103,23 +107,28 @@ def generate_c(nx: int, ny: int, nz: int) -> str:
         if n != 1:
             raise RuntimeError("bla.f iiles_smag switch not recognised")
     sources.append(("bla.f", bla))
-    return translate(sources, par_text(nx, ny, nz), defines={"OPENMP"},
+    return translate(sources, par_text(nx, ny, nz, pressure=pressure), defines={"OPENMP"},
                      main_ranges=MAIN_RANGES, stubs_noop=NOOP_STUBS,
                      skip_units=("fft_identify",), provided=("stopnow",))
 
 
-def lib_path(nx: int, ny: int, nz: int, fma: bool = False) -> str:
-    return os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}" + ("_fma" if fma else ""), "libsimson_ref.so")
+def _dir(nx: int, ny: int, nz: int, fma: bool = False, pressure: bool = False) -> str:
+    return os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}" + ("_fma" if fma else "") + ("_p" if pressure else ""))
 
 
-def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False, fma: bool = False) -> str:
+def lib_path(nx: int, ny: int, nz: int, fma: bool = False, pressure: bool = False) -> str:
+    return os.path.join(_dir(nx, ny, nz, fma, pressure), "libsimson_ref.so")
+
+
+def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False, fma: bool = False,
+          pressure: bool = False) -> str:
     """Translate + compile the reference for one grid; returns the .so path.
 
     fma=True builds a second copy with fused multiply-add contraction
     (-mfma -ffp-contract=fast): the same reference with roundoff-level
     different arithmetic, used to measure how far the reference agrees with
     itself."""
-    out_dir = os.path.join(OUT_ROOT, f"{nx}x{ny}x{nz}" + ("_fma" if fma else ""))
+    out_dir = _dir(nx, ny, nz, fma, pressure)
     so = os.path.join(out_dir, "libsimson_ref.so")
     harness = os.path.join(HERE, "ref_harness.c")
     translator = os.path.join(HERE, "f77c.py")
@@ -138,7 +147,7 @@ def build(nx: int, ny: int, nz: int, force: bool = False, verbose: bool = False,
             return so
         raise FileNotFoundError(f"reference sources not found at {REF_BLA} and no prebuilt {so}")
     os.makedirs(out_dir, exist_ok=True)
-    csrc = generate_c(nx, ny, nz)
+    csrc = generate_c(nx, ny, nz, pressure)
     gen = os.path.join(out_dir, "ref_gen.c")
     with open(gen, "w") as f:
         f.write(csrc)

@@ -142,6 +142,22 @@ void sref_grid(double *eta, double *wint) {
 void sref_set_iamp(int iamp) { v_iamp = iamp > 0 ? iamp : -1000000; }
 void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(double)); }
 
+/* Pressure of the current state: the block of bla/bla.f:2486-2527 (nonlinp
+ * on every xz-plane, linearp on every kz plane) with do_press set, as the
+ * driver runs it after a step that saves a field.  Needs the variant built
+ * with pressure = 1 (slot 8 holds p afterwards; linearp also recomputes
+ * omega_x, omega_z in slots 4-5).  Returns -1 on a pressure = 0 build. */
+int sref_pressure(double *re_part, double *im_part) {
+  if (v_pressure != 1) return -1;
+  v_do_press = 1;
+  bla_press();
+  v_do_press = 0;
+  long n = slot_size();
+  memcpy(re_part, v_ur + 7 * n, n * sizeof(double));
+  memcpy(im_part, v_ui + 7 * n, n * sizeof(double));
+  return 0;
+}
+
 /* xy statistics: the sampling block of bla/bla.f:2069-2107 (boxxys on every
  * xz-plane with weight dtn, then sumw(istat) += dtn) run on the current
  * state, as bla.f does at the start of a step that takes statistics.  With

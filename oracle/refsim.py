@@ -19,11 +19,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _lib(nx, ny, nz, build=True, fma=False):
+def _lib(nx, ny, nz, build=True, fma=False, pressure=False):
     import sys
     sys.path.insert(0, HERE)
     from build_ref import build as _build, lib_path
-    path = _build(nx, ny, nz, fma=fma) if build else lib_path(nx, ny, nz, fma=fma)
+    path = (_build(nx, ny, nz, fma=fma, pressure=pressure) if build
+            else lib_path(nx, ny, nz, fma=fma, pressure=pressure))
     if not os.path.exists(path):
         raise FileNotFoundError(path)
     lib = ctypes.CDLL(path)
@@ -43,6 +44,7 @@ def _lib(nx, ny, nz, build=True, fma=False):
     lib.sref_get_gu.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_amp.argtypes = [dp]
     lib.sref_xys.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp]
+    lib.sref_pressure.argtypes = [dp, dp]
     return lib
 
 
@@ -53,8 +55,9 @@ def _dp(a):
 class RefSim:
     """The reference channel time stepper (temporal channel, RK3/CN, cflux)."""
 
-    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True, fma=False):
-        self.lib = _lib(nx, ny, nz, build, fma)
+    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True, fma=False,
+                 pressure=False):
+        self.lib = _lib(nx, ny, nz, build, fma, pressure)
         dims = (ctypes.c_int * 12)()
         self.lib.sref_dims(dims)
         self.dims = list(dims)
@@ -159,6 +162,15 @@ class RefSim:
         sw = np.zeros(1)
         self.lib.sref_xys(float(dtn), 1 if reset else 0, _dp(out), _dp(sw))
         return out, float(sw[0])
+
+    def pressure(self):
+        """Pressure of the current state (bla/bla.f:2486-2527); needs
+        pressure=True.  Complex (nz, nyp, nx/2), Fourier x/z, physical y."""
+        re_ = np.empty(self.shape)
+        im_ = np.empty(self.shape)
+        if self.lib.sref_pressure(_dp(re_), _dp(im_)) != 0:
+            raise RuntimeError("oracle built without pressure")
+        return re_ + 1j * im_
 
     def state(self):
         return [self.get_slot(k) for k in range(1, 8)]

@@ -91,6 +91,7 @@ def load_library(build: bool = True):
     lib.sgpu_xys_reset.argtypes = [vp]
     lib.sgpu_box_filter_sample.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                            ctypes.POINTER(ctypes.c_float)]
+    lib.sgpu_pressure.argtypes = [vp, dp, dp]
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
@@ -325,6 +326,14 @@ class Channel:
 
     def xys_reset(self):
         self._check(self.lib.sgpu_xys_reset(self._ctx), "xys_reset")
+
+    def pressure(self):
+        """Pressure of the current state (bla/nonlinp.f + bla/linearp.f),
+        complex (nz, ny, nx/2): Fourier x/z, physical y.  FP64 contexts."""
+        re_ = np.empty(self.shape)
+        im_ = np.empty(self.shape)
+        self._check(self.lib.sgpu_pressure(self._ctx, _dp(re_), _dp(im_)), "pressure")
+        return re_ + 1j * im_
 
     def box_filter_sample(self, factor=4):
         """Training sample of the learned SGS model from the current state:

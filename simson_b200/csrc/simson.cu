@@ -21,6 +21,7 @@
 #include "les_dyn.cuh"
 #include "sgs_mlp.cuh"
 #include "xys.cuh"
+#include "press.cuh"
 
 #include <nvtx3/nvToolsExt.h>
 #include "mixed.h"
@@ -115,6 +116,8 @@ struct sgpu_ctx {
   double xys_sumw = 0.0;
   Tw xys_twz, xys_twx;
   float* box_out = nullptr;  // sgpu_box_filter_sample: features then targets
+  double2* press = nullptr;     // sgpu_pressure: p [nyp][NP] (Fourier x/z, physical y)
+  double* press_wd = nullptr;   // [2][nyp] second-derivative weights at y = +1, -1
   size_t box_n = 0;          // coarse points box_out holds
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
@@ -414,7 +417,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
   void* ptrs[] = {c->st, c->stf, c->meanp, c->ampd, c->les_gu, c->les_coef, c->les_lpf, c->les_filt,
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
-                  c->xys_part, c->xys_u, c->box_out, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
+                  c->xys_part, c->xys_u, c->box_out, c->press, c->press_wd, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
@@ -1336,6 +1339,94 @@ extern "C" int sgpu_xys_reset(sgpu_ctx* c) {
   if (!c) return SGPU_E_PARAM;
   if (c->xys) CK(cudaMemsetAsync(c->xys, 0, XYS_NS * (size_t)c->g.nyp * c->g.nx * sizeof(double), c->stream));
   c->xys_sumw = 0.0;
+  return SGPU_OK;
+}
+
+// Pressure of the current state (press.cuh; bla/nonlinp.f + bla/linearp.f as
+// bla/bla.f:2486-2527 runs them), FP64 state only.
+extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
+  NvtxRange nv("pressure");
+  if (c && sharded(c)) return SGPU_E_STATE;  // reads the whole state
+  if (!c || !pr || !pi) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  if (c->mixed) return SGPU_E_PARAM;  // the FP64 state is not kept under SGPU_MIXED
+  const Dims& g = c->g;
+  const int n = g.nyp;
+  if (n < 9) return SGPU_E_PARAM;
+  const size_t fld = (size_t)n * g.NP;
+  if (!c->press) {
+    // second-derivative weights at y = +1 and y = -1 on the Gauss-Lobatto
+    // points (bla/preprbl.f:90-118: wd1(:,2) and wd1(:,4))
+    const double pi_ = 3.1415926535897932385;
+    std::vector<double> wd(2 * (size_t)n, 0.0), cw(n, 1.0);
+    cw[0] = 0.5;
+    cw[n - 1] = 0.5;
+    double sgn = 1.0;
+    for (int i = 1; i <= n; ++i) {
+      sgn = -sgn;
+      const double kk = (double)(i - 1) * (double)(i - 1);
+      for (int y = 1; y <= n; ++y) {
+        const double cs = cos(pi_ * (double)((i - 1) * (y - 1)) / (double)(n - 1));
+        wd[y - 1] = wd[y - 1] + kk * (kk - 1.) / 3. * cw[y - 1] * cw[i - 1] * cs * (2. / (double)(n - 1));
+        wd[n + y - 1] =
+            wd[n + y - 1] - kk * (kk - 1.) / 3. * cw[y - 1] * cw[i - 1] * sgn * cs * (2. / (double)(n - 1));
+      }
+    }
+    if (cudaMalloc(&c->press_wd, 2 * (size_t)n * sizeof(double)) != cudaSuccess) {
+      c->press_wd = nullptr;
+      return SGPU_E_CUDA;
+    }
+    if (cudaMalloc(&c->press, fld * sizeof(double2)) != cudaSuccess) {
+      cudaFree(c->press_wd);
+      c->press_wd = nullptr;
+      c->press = nullptr;
+      return SGPU_E_CUDA;
+    }
+    CK(cudaMemcpyAsync(c->press_wd, wd.data(), wd.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->press, 0, fld * sizeof(double2), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  const sgpu_params& P = c->prm;
+  // step-2 transforms of u, omega and the products H, 2E (nonlinp.f)
+  dim3 gz((g.nx2 + c->kb - 1) / c->kb, n);
+  const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
+  launch_zinv<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa,
+                                            c->beta, 0);
+  const size_t s_xp = 2 * (size_t)g.nxp * 3 * sizeof(double2);
+  cudaFuncSetAttribute(k_xpass_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_xp);
+  k_xpass_p<<<dim3(g.nzp, n), 256, s_xp, c->stream>>>(c->zb, g, c->twx.plan, c->twx.d, P.rot);
+  const size_t fz = (size_t)n * g.nzp * g.nx2;  // one field of zb
+  launch_zfwd<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->zb, czf(c, 0), g, c->twz.plan, c->twz.d,
+                                            nullptr, 0.0);  // H1, H2, H3
+  launch_zfwd<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->zb + 3 * fz, czf(c, 3), g, c->twz.plan,
+                                            c->twz.d, nullptr, 0.0);  // 2E (fields 4, 5 overwritten below)
+  k_press_div<<<(unsigned)((fld + 255) / 256), 256, 0, c->stream>>>(czf(c, 0), g, c->alfa, c->beta);
+  // Chebyshev coefficients (linearp.f:89-114)
+  const double cn = 1.0 / ((double)g.nxp * (double)g.nzp);
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 0), fld, czf(c, 4), fld, 2, 0, cn, 1, c->twy.d);
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 3), fld, czf(c, 6), fld, 1, 0,
+                                                      1.0 / (2.0 * (double)g.nxp * (double)g.nzp), 1, c->twy.d);
+  PressArgs A;
+  A.CD = czf(c, 4); A.CH2 = czf(c, 5); A.CE = czf(c, 6);
+  A.PH2 = czf(c, 1); A.PE = czf(c, 3); A.V = slot(c, 1);
+  A.X = czf(c, 7);
+  A.Q = reinterpret_cast<double*>(czf(c, 8)); A.Cc = A.Q + fld;
+  A.Dd = reinterpret_cast<double*>(czf(c, 9)); A.Ee = A.Dd + fld;
+  A.wd = c->press_wd; A.alfa = c->alfa; A.beta = c->beta;
+  A.re = P.re;
+  A.c4t = 1. / c->dtn * (double)(1 - 1 / c->it);
+  A.cn = cn;
+  A.e2n = 2. * (double)g.nxp * (double)g.nzp;
+  A.cim = 0;
+  k_press<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(A, g);
+  // back to physical y (vchbb), the oddball plane left out (linearp.f:64)
+  launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 7), fld, c->press, fld, 1, 1, 1.0, 1, c->twy.d);
+  c->launches += 9;
+  CK(cudaGetLastError());
+  k_to_ref<<<592, 256, 0, c->stream>>>(c->press, c->stage, c->stage + fld, g, 1);
+  CK(cudaMemcpyAsync(pr, c->stage, fld * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(pi, c->stage + fld, fld * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return SGPU_OK;
 }
 

@@ -1,0 +1,77 @@
+"""The pressure solver (sgpu_pressure: bla/nonlinp.f + bla/linearp.f as
+bla/bla.f:2486-2527 runs them) against the translated reference built with
+pressure = 1, on the same state after two steps: FP64, relative L2 within
+1e-10 (the kz = -nz/2 plane, which linearp skips, excluded).  Laminar flow
+has zero pressure in this formulation (H2 = dE/dy); under SGPU_MIXED the
+call is refused."""
+import os
+
+import numpy as np
+import pytest
+
+from simson_b200.fields import channel_field
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ, RE, XL, ZL, DT = 48, 65, 48, 4200.0, 4 * np.pi, 2 * np.pi, 0.01
+
+
+def need_pressure_ref():
+    from build_ref import REF_BLA, lib_path
+    if not (os.path.isdir(REF_BLA) or os.path.exists(lib_path(NX, NY, NZ, pressure=True))):
+        pytest.skip("pressure oracle neither buildable nor prebuilt")
+
+
+def rel(a, b):
+    keep = np.ones(a.shape[0], bool)
+    keep[a.shape[0] // 2] = False
+    return float(np.linalg.norm(a[keep] - b[keep]) / np.linalg.norm(b[keep]))
+
+
+@pytest.mark.parametrize("rms", [0.05, 0.1])
+def test_pressure_matches_reference(rms):
+    need_pressure_ref()
+    from refsim import RefSim
+    from simson_b200.bla import Channel
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, rms, 5)
+    ref = RefSim(NX, NY, NZ, RE, XL, ZL, DT, pressure=True)
+    ref.set_velocity(u, v, w)
+    ref.start()
+    ref.step(2)
+    state = ref.state()
+    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT)
+    try:
+        ch.set_state(state)
+        got = ch.pressure()
+        again = ch.pressure()
+        after = ch.state(7)
+    finally:
+        ch.close()
+    want = ref.pressure()
+    err = rel(got, want)
+    print("pressure rel L2 vs reference: %.2e" % err)
+    assert err <= 1e-10
+    assert np.array_equal(got, again)
+    assert not got[NZ // 2].any()
+    for a, b in zip(after, state):  # the state is left as it was
+        assert np.array_equal(a, b)
+
+
+def test_laminar_pressure_is_zero_and_mixed_is_refused():
+    from simson_b200.bla import Channel, SimsonError
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.0, 1)
+    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT)
+    try:
+        ch.set_velocity(u, v, w)
+        ch.prhs()
+        p = ch.pressure()
+    finally:
+        ch.close()
+    assert np.abs(p).max() <= 1e-12
+    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT, precision="mixed")
+    try:
+        ch.set_velocity(u, v, w)
+        with pytest.raises(SimsonError):
+            ch.pressure()
+    finally:
+        ch.close()
