@@ -167,9 +167,11 @@ int sgpu_amplitudes(sgpu_ctx* ctx, double* amp, double* row);
  * (1-based, the reference's numbering): 1-15 means and second moments of
  * u_i, omega_i and uv, uw, vw; 25-30 the dissipation tensor du_i/dx_k
  * du_j/dx_k; 43-44 running min / max over z of u - <u>_z; 45-51 S_ij S_ij
- * and S_ij; 63-72 third moments; 75-77 u_i^4.  The pressure, LES and MHD
- * entries stay zero (the reference built with pressure = 0, no LES or MHD
- * statistics).  nx <= 512.  Not on a shard. */
+ * and S_ij; 63-72 third moments; 75-77 u_i^4.  When sgpu_pressure has
+ * been called on the current state (the reference needs the pressure of the
+ * sampled state, bla/bla.f:1833-1840), also the pressure entries 31-42,
+ * 73-74, 78-79; any step or upload makes that pressure stale.  LES and MHD
+ * entries stay zero.  nx <= 512.  Not on a shard. */
 int sgpu_xys_sample(sgpu_ctx* ctx, double dtn);
 
 /* The running sums: xys[96*ny*nx] in the layout of the reference's

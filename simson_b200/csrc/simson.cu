@@ -117,6 +117,7 @@ struct sgpu_ctx {
   Tw xys_twz, xys_twx;
   float* box_out = nullptr;  // sgpu_box_filter_sample: features then targets
   double2* press = nullptr;     // sgpu_pressure: p [nyp][NP] (Fourier x/z, physical y)
+  bool press_valid = false;     // press belongs to the current state
   double* press_wd = nullptr;   // [2][nyp] second-derivative weights at y = +1, -1
   size_t box_n = 0;          // coarse points box_out holds
   // RK bookkeeping (host mirror of the reference driver scalars)
@@ -441,6 +442,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
 }
 
 extern "C" int sgpu_upload_state(sgpu_ctx* c, const double* ur, const double* ui, int nslots) {
+  if (c) c->press_valid = false;  // the state changes
   if (!c || !ur || !ui || nslots < 1 || nslots > 7) return SGPU_E_PARAM;
   const size_t n = (size_t)nslots * c->g.nyp * c->g.NP;
   CK(cudaMemcpyAsync(c->stage, ur, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -615,6 +617,7 @@ extern "C" int sgpu_set_shard(sgpu_ctx* c, int ylo, int yhi, int zlo, int zhi) {
 
 extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int yhi, int zlo, int zhi, void* buf,
                                int to_state, size_t* bytes) {
+  if (c) c->press_valid = false;  // may write the state
   if (!c || !bytes) return SGPU_E_PARAM;
   const Dims& g = c->g;
   if (slot0 < 0 || nslots < 1 || slot0 + nslots > 7 || ylo < 0 || yhi > g.nyp || ylo >= yhi || zlo < 0 ||
@@ -645,6 +648,7 @@ extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int 
 }
 
 extern "C" int sgpu_prhs(sgpu_ctx* c) {
+  if (c) c->press_valid = false;
   NvtxRange nv("prhs");
   if (!c) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
@@ -767,6 +771,7 @@ static void enqueue_sgs(sgpu_ctx* c) {
 }
 
 static int enqueue_nonlin(sgpu_ctx* c) {
+  c->press_valid = false;
   NvtxRange nv("step 2 (nonlinbl)");
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
@@ -852,6 +857,7 @@ static void it_advance(sgpu_ctx* c) {
 
 static int enqueue_linear(sgpu_ctx* c) {
   NvtxRange nv("step 3 (linearbl)");
+  c->press_valid = false;
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   rk_advance(c);
@@ -1049,6 +1055,7 @@ static void replay_host(sgpu_ctx* c) {
 
 extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
   if (!c || nsub < 0) return SGPU_E_PARAM;
+  c->press_valid = false;
   if (!c->have_state) return SGPU_E_STATE;
   // a shard needs the block exchanges between its two steps (host-driven)
   if (sharded(c)) return SGPU_E_STATE;
@@ -1083,6 +1090,7 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
 }
 
 extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
+  if (c) c->press_valid = false;  // the state changes
   NvtxRange nv("offload steps");
   if (!c || !ur || !ui || nsteps < 0) return SGPU_E_PARAM;
   if (sharded(c)) return SGPU_E_STATE;
@@ -1238,7 +1246,7 @@ static int xys_setup(sgpu_ctx* c) {
   // c->xys last: its presence marks the set-up as complete
   if ((!c->xys_spec && cudaMalloc(&c->xys_spec, XYS_NF * (size_t)g.nyp * g.NP * sizeof(double2)) != cudaSuccess) ||
       (!c->xys_part &&
-       cudaMalloc(&c->xys_part, (size_t)XYS_GROUPS * XYS_NACC * plane * sizeof(double)) != cudaSuccess) ||
+       cudaMalloc(&c->xys_part, (size_t)XYS_GROUPS * XYS_NACC_P * plane * sizeof(double)) != cudaSuccess) ||
       (!c->xys_u && cudaMalloc(&c->xys_u, plane * g.nz * sizeof(double)) != cudaSuccess) ||
       cudaMalloc(&c->xys, XYS_NS * plane * sizeof(double)) != cudaSuccess)
     return SGPU_E_CUDA;
@@ -1246,23 +1254,24 @@ static int xys_setup(sgpu_ctx* c) {
   c->xys_sumw = 0.0;
   cudaFuncSetAttribute(k_xys_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
   cudaFuncSetAttribute(k_xys_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
-  cudaFuncSetAttribute(k_xys_acc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  cudaFuncSetAttribute(k_xys_acc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  cudaFuncSetAttribute(k_xys_acc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
   cudaFuncSetAttribute(k_box_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
   return SGPU_OK;
 }
 
 // The 15 spectral fields of the statistics on the nx x nz grid, z physical.
-static void xys_fields(sgpu_ctx* c) {
+static void xys_fields(sgpu_ctx* c, const double2* pr) {
   const Dims& g = c->g;
   const SgsGrid G = sgs_grid(c);
   constexpr int KB = 4;
   const size_t sz = 2 * (size_t)g.nz * KB * sizeof(double2);
   const dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);
   if (c->mixed)
-    k_xys_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+    k_xys_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, pr, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
                                                        c->alfa, c->beta);
   else
-    k_xys_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
+    k_xys_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, pr, c->xys_spec, G, c->xys_twz.plan, c->xys_twz.d,
                                                         c->alfa, c->beta);
   c->launches++;
 }
@@ -1284,7 +1293,7 @@ extern "C" int sgpu_box_filter_sample(sgpu_ctx* c, int factor, float* features, 
     if (cudaMalloc(&c->box_out, npts * 16 * sizeof(float)) != cudaSuccess) return SGPU_E_CUDA;
     c->box_n = npts;
   }
-  xys_fields(c);
+  xys_fields(c, nullptr);
   const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
   const int nt = std::max(128, (nxc + 31) / 32 * 32);
   k_box_sample<<<dim3(nzc, g.nyp), nt, sx, c->stream>>>(c->xys_spec, sgs_grid(c), c->xys_twx.plan, c->xys_twx.d,
@@ -1307,13 +1316,19 @@ extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
   const Dims& g = c->g;
   const SgsGrid G = sgs_grid(c);
   const size_t sx = 2 * (size_t)g.nx * XYS_NC * sizeof(double2);
-  xys_fields(c);
+  // the pressure entries when the pressure of this state has been computed
+  const bool pres = c->press_valid && c->press;
+  xys_fields(c, pres ? c->press : nullptr);
   const int nt = (g.nx + 31) / 32 * 32;
-  k_xys_acc<<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
-                                                               c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
+  if (pres)
+    k_xys_acc<true><<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
+                                                                    c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
+  else
+    k_xys_acc<false><<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
+                                                                     c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
   const size_t plane = (size_t)g.nyp * g.nx;
   const int nb = (int)((plane + 255) / 256);
-  k_xys_add<<<nb, 256, 0, c->stream>>>(c->xys_part, c->xys, G);
+  k_xys_add<<<nb, 256, 0, c->stream>>>(c->xys_part, c->xys, G, pres ? XYS_NACC_P : XYS_NACC);
   k_xys_minmax<<<nb, 256, 0, c->stream>>>(c->xys_u, c->xys, G);
   c->launches += 3;
   c->xys_sumw += dtn;
@@ -1427,6 +1442,7 @@ extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
   CK(cudaMemcpyAsync(pr, c->stage, fld * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(pi, c->stage + fld, fld * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->press_valid = true;
   return SGPU_OK;
 }
 

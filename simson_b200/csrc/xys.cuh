@@ -11,10 +11,14 @@
 //   45    S_ij S_ij       46-51 S_11, S_12, S_13, S_22, S_23, S_33
 //   63-65 u_i^3           66-72 u^2 v, u^2 w, v^2 u, v^2 w, w^2 u, w^2 v, u v w
 //   75-77 u_i^4
-// The pressure (31-42, 73-74, 78-79), LES (52-62, 80-82) and MHD (83-96)
-// entries need fields this path does not carry and stay zero, as in the
-// reference built with pressure = 0 and no LES or MHD; 16-24 are never
-// written by the reference.
+// With the pressure of the sampled state at hand (sgpu_pressure since the
+// last change of the state, as the reference requires a pressure computed
+// at the end of the previous step, bla/bla.f:1833-1840), also
+//   31 p   32 p^2   33-35 u_i p   36-38 p du_i/dx_i   39-42 p uy, p vz, p wx, p uz
+//   73-74 p vx, p wy   78-79 p^3, p^4          (boxxys.f:895-990, 1343-1400)
+// The LES (52-62, 80-82) and MHD (83-96) entries need fields this path does
+// not carry and stay zero, as in the reference built without them; 16-24
+// are never written by the reference.
 //
 //   k_xys_zinv    per plane and kx block: the 15 spectral fields
 //                 (boxxys.f:246-350: omega_y from u and w, the y derivatives
@@ -38,20 +42,22 @@
 
 namespace sb {
 
-constexpr int XYS_NF = 15;     // spectral fields: u v w, omega x y z, du_ij (i-major)
-constexpr int XYS_NC = 8;      // complex x transforms carrying the 15 real rows
-constexpr int XYS_NACC = 41;   // accumulated entries (all but 43-44)
+constexpr int XYS_NF = 16;     // spectral fields: u v w, omega x y z, du_ij (i-major), p
+constexpr int XYS_NC = 8;      // complex x transforms carrying the 16 real rows
+constexpr int XYS_NACC = 41;   // accumulated velocity entries (all but 43-44)
+constexpr int XYS_NACC_P = 57;  // with the pressure entries
 constexpr int XYS_NS = 96;     // entries of the reference's xys (bla/par.f nxys)
 constexpr int XYS_GROUPS = 8;  // z-row groups per plane in k_xys_acc
 
 // reference entry (1-based) of accumulator k
 __device__ __host__ constexpr int xys_entry(int k) {
-  return k < 15 ? k + 1 : k < 21 ? k + 10 : k < 28 ? k + 24 : k < 38 ? k + 35 : k + 37;
+  return k < 15 ? k + 1 : k < 21 ? k + 10 : k < 28 ? k + 24 : k < 38 ? k + 35 : k < 41 ? k + 37
+       : k < 53 ? k - 10 : k == 53 ? 73 : k == 54 ? 74 : k == 55 ? 78 : 79;
 }
 
 template <class V>
-__device__ __forceinline__ double2 xys_spec_field(const V* st, size_t slot, size_t off, int f, double a,
-                                                  double b) {
+__device__ __forceinline__ double2 xys_spec_field(const V* st, const double2* pr, size_t slot, size_t off, int f,
+                                                  double a, double b) {
   auto ld = [&](int s) { const V q = st[(size_t)s * slot + off]; return double2{(double)q.x, (double)q.y}; };
   switch (f) {
     case 0: return ld(0);
@@ -64,14 +70,15 @@ __device__ __forceinline__ double2 xys_spec_field(const V* st, size_t slot, size
       return double2{-b * u.y + a * w.y, b * u.x - a * w.x};
     }
     case 5: return ld(4);
+    case 15: return pr ? pr[off] : double2{0.0, 0.0};  // pressure (getxz of slot 8)
     default: return sgs_spec_field(st, slot, off, f - 6, a, b, 1);  // du_i/dx_j (boxxys.f:323-366)
   }
 }
 
 template <class V, int KB>
-__global__ void k_xys_zinv(const V* __restrict__ st, double2* __restrict__ spec, SgsGrid G, FFTPlan plan,
-                           const double2* __restrict__ tw, const double* __restrict__ alfa,
-                           const double* __restrict__ beta) {
+__global__ void k_xys_zinv(const V* __restrict__ st, const double2* __restrict__ pr, double2* __restrict__ spec,
+                           SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
+                           const double* __restrict__ alfa, const double* __restrict__ beta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* b0 = reinterpret_cast<double2*>(smem_raw);
   double2* b1 = b0 + (size_t)G.nz * KB;
@@ -84,7 +91,7 @@ __global__ void k_xys_zinv(const V* __restrict__ st, double2* __restrict__ spec,
       const int kx = kx0 + t - iz * KB;
       double2 val{0.0, 0.0};
       if (kx < G.nx2 && iz != G.zodd)
-        val = xys_spec_field(st, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz]);
+        val = xys_spec_field(st, pr, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz]);
       b0[t] = val;
     }
     __syncthreads();
@@ -98,9 +105,11 @@ __global__ void k_xys_zinv(const V* __restrict__ st, double2* __restrict__ spec,
   }
 }
 
-// blockDim.x >= nx (nx <= 512); thread j owns x = j.  part: [XYS_GROUPS][XYS_NACC][nyp][nx];
+// blockDim.x >= nx (nx <= 512); thread j owns x = j.  part: [XYS_GROUPS][XYS_NACC_P][nyp][nx];
+// PRES: the pressure entries too (field 15 holds p).
 // uphys: [nyp][nz][nx].  c = dtn / nz, the weight of one point
 // (boxxys.f:556, nfzsym = 0).
+template <bool PRES>
 __global__ void __launch_bounds__(512) k_xys_acc(const double2* __restrict__ spec, double* __restrict__ part,
                                                   double* __restrict__ uphys, SgsGrid G, FFTPlan plan,
                                                   const double2* __restrict__ tw, double c) {
@@ -112,9 +121,10 @@ __global__ void __launch_bounds__(512) k_xys_acc(const double2* __restrict__ spe
   const int j = threadIdx.x;
   const size_t fs = (size_t)G.nyp * G.nz * G.nx2;
   const int m0 = (int)((long long)G.nz * grp / XYS_GROUPS), m1 = (int)((long long)G.nz * (grp + 1) / XYS_GROUPS);
-  double acc[XYS_NACC];
+  constexpr int NACC = PRES ? XYS_NACC_P : XYS_NACC;
+  double acc[NACC];
 #pragma unroll
-  for (int k = 0; k < XYS_NACC; ++k) acc[k] = 0.0;
+  for (int k = 0; k < NACC; ++k) acc[k] = 0.0;
   for (int m = m0; m < m1; ++m) {
     const size_t row = ((size_t)y * G.nz + m) * G.nx2;
     for (int t = threadIdx.x; t < n * XYS_NC; t += blockDim.x) {
@@ -184,24 +194,43 @@ __global__ void __launch_bounds__(512) k_xys_acc(const double2* __restrict__ spe
       acc[38] += uu * uu * c;
       acc[39] += vv * vv * c;
       acc[40] += ww * ww * c;
+      if constexpr (PRES) {
+        const double p = q[15];
+        acc[41] += p * c;
+        acc[42] += p * p * c;
+        acc[43] += u * p * c;
+        acc[44] += v * p * c;
+        acc[45] += w * p * c;
+        acc[46] += p * du[0] * c;  // p ux
+        acc[47] += p * du[4] * c;  // p vy
+        acc[48] += p * du[8] * c;  // p wz
+        acc[49] += p * du[1] * c;  // p uy
+        acc[50] += p * du[5] * c;  // p vz
+        acc[51] += p * du[6] * c;  // p wx
+        acc[52] += p * du[2] * c;  // p uz
+        acc[53] += p * du[3] * c;  // p vx
+        acc[54] += p * du[7] * c;  // p wy
+        acc[55] += p * p * p * c;
+        acc[56] += p * p * (p * p) * c;
+      }
     }
     __syncthreads();
   }
   if (j < n) {
     const size_t plane = (size_t)G.nyp * n;
 #pragma unroll
-    for (int k = 0; k < XYS_NACC; ++k)
-      part[((size_t)grp * XYS_NACC + k) * plane + (size_t)y * n + j] = acc[k];
+    for (int k = 0; k < NACC; ++k)
+      part[((size_t)grp * XYS_NACC_P + k) * plane + (size_t)y * n + j] = acc[k];
   }
 }
 
-__global__ void k_xys_add(const double* __restrict__ part, double* __restrict__ xys, SgsGrid G) {
+__global__ void k_xys_add(const double* __restrict__ part, double* __restrict__ xys, SgsGrid G, int nacc) {
   const size_t plane = (size_t)G.nyp * G.nx;
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= plane) return;
-  for (int k = 0; k < XYS_NACC; ++k) {
+  for (int k = 0; k < nacc; ++k) {
     double s = 0.0;
-    for (int grp = 0; grp < XYS_GROUPS; ++grp) s += part[((size_t)grp * XYS_NACC + k) * plane + i];
+    for (int grp = 0; grp < XYS_GROUPS; ++grp) s += part[((size_t)grp * XYS_NACC_P + k) * plane + i];
     xys[(size_t)(xys_entry(k) - 1) * plane + i] += s;
   }
 }

@@ -5,6 +5,8 @@ pressure, LES or MHD, two samples with different weights (running sums and
 the running min / max of entries 43-44), content in the kz = -nz/2 plane
 ignored as the reference's getxz ignores it.  FP64 path within 1e-12 of each
 entry's largest value; the mixed path (FP32 state storage) within 1e-5.
+With the pressure of the sampled state computed (sgpu_pressure), the
+pressure entries too, against the reference built with pressure = 1.
 Entry 51 (<dw/dz>_z, the z average of a z derivative) vanishes analytically
 and holds roundoff; it is measured against the scale of the other strain-rate
 entries 46-50."""
@@ -31,11 +33,14 @@ def with_oddball(state, seed):
     return out
 
 
-def compare(got, ref, tol):
+PRESSURE = list(range(31, 43)) + [73, 74, 78, 79]
+
+
+def compare(got, ref, tol, filled=FILLED):
     errs = {}
     for s in range(96):
         scale = np.abs(ref[s]).max()
-        if s + 1 in FILLED:
+        if s + 1 in filled:
             assert scale > 0.0, f"entry {s + 1} not filled by the reference"
             if s + 1 == 51:
                 scale = max(scale, np.abs(ref[45:50]).max())
@@ -76,3 +81,37 @@ def test_xys_matches_reference(need_ref, precision):
         assert swg == 0.0 and not xg.any()
     finally:
         ch.close()
+
+
+def test_xys_pressure_entries_match_reference(need_ref):
+    import os
+    from build_ref import REF_BLA, lib_path
+    if not (os.path.isdir(REF_BLA) or os.path.exists(lib_path(NX, NY, NZ, pressure=True))):
+        pytest.skip("pressure oracle neither buildable nor prebuilt")
+    from refsim import RefSim
+    from simson_b200.bla import Channel
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.05, 5)
+    ref = RefSim(NX, NY, NZ, RE, XL, ZL, DT, pressure=True)
+    ref.set_velocity(u, v, w)
+    ref.start()
+    ref.step(2)
+    ref.pressure()  # slot 8 for boxxys (and omega_x, omega_z recomputed, as the driver leaves them)
+    state = ref.state()
+    xr, _ = ref.xys(DT, reset=True)
+    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT)
+    try:
+        ch.set_state(state)
+        ch.pressure()
+        ch.xys_sample(DT)
+        xg, _ = ch.xys()
+        ch.step(1)           # a new state: its pressure is not known, the entries stay as they were
+        ch.xys_sample(DT)
+        xg2, _ = ch.xys()
+    finally:
+        ch.close()
+    # the device pressure comes from the state after the reference's own
+    # recomputation of omega_x, omega_z (roundoff apart from the one the
+    # reference's p was formed from): 1e-10
+    compare(xg, xr, 1e-10, FILLED + PRESSURE)
+    for e in PRESSURE:
+        assert np.array_equal(xg2[e - 1], xg[e - 1]), e
