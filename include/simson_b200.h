@@ -187,7 +187,7 @@ int sgpu_xys_reset(sgpu_ctx* ctx);
  * equation with the Neumann conditions of the wall-normal momentum equation,
  * the mean mode by integration of H2): p in the layout of one slot of ur, ui
  * (Fourier x/z, physical y; the kz = -nz/2 plane is zero).  The state is not
- * changed.  FP64 contexts only (SGPU_E_PARAM under SGPU_MIXED).
+ * changed.  FP64 arithmetic; under SGPU_MIXED from the FP32 state.
  * Synchronises the library's stream.  Not on a shard. */
 int sgpu_pressure(sgpu_ctx* ctx, double* pr, double* pi);
 

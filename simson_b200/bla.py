@@ -329,7 +329,7 @@ class Channel:
 
     def pressure(self):
         """Pressure of the current state (bla/nonlinp.f + bla/linearp.f),
-        complex (nz, ny, nx/2): Fourier x/z, physical y.  FP64 contexts."""
+        complex (nz, ny, nx/2): Fourier x/z, physical y."""
         re_ = np.empty(self.shape)
         im_ = np.empty(self.shape)
         self._check(self.lib.sgpu_pressure(self._ctx, _dp(re_), _dp(im_)), "pressure")

@@ -19,7 +19,8 @@
 //                solve of bla/crhsc.f, bla/setmac.f (neumann = 1) and
 //                bla/tridc.f, the mean mode by bla/icheb.f, minus E
 //   inverse Chebyshev transform of p (k_cheb)
-// All FP64; the pencil arithmetic follows the reference's operation order.
+// All FP64 (under FP32 state storage the FP32 fields are read and widened);
+// the pencil arithmetic follows the reference's operation order.
 #pragma once
 #include "fft.cuh"
 #include "layout.cuh"
@@ -101,7 +102,8 @@ __global__ void k_press_div(double2* __restrict__ h, Dims g, const double* __res
 struct PressArgs {
   const double2 *CD, *CH2, *CE;  // Chebyshev coefficients: i alpha H1 + i beta H3, H2 (1/(nxp nzp)), E
   const double2 *PH2, *PE;       // physical H2 and 2E (walls, unnormalised)
-  const double2* V;              // state slot 1 (v, physical y)
+  const double2* V;              // state slot 1 (v, physical y), FP64 storage
+  const float2* Vf;              // the same under FP32 storage (V unused when set)
   double2* X;                    // right-hand side, then the Chebyshev coefficients of p
   double *Q, *Cc, *Dd, *Ee;      // real scratch columns [nyp][NP]
   const double* wd;              // [2][nyp]: second-derivative weights at y = +1 and y = -1
@@ -148,6 +150,11 @@ __device__ __forceinline__ void press_crhsc(Col F, int n, double bc1, double bc2
   F[1] = bc2;
 }
 
+__device__ __forceinline__ double2 vload(const PressArgs& A, size_t i) {
+  if (A.Vf) return double2{(double)A.Vf[i].x, (double)A.Vf[i].y};
+  return A.V[i];
+}
+
 __global__ void __launch_bounds__(128) k_press(PressArgs A, Dims g) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= g.NP) return;
@@ -174,13 +181,13 @@ __global__ void __launch_bounds__(128) k_press(PressArgs A, Dims g) {
   // step is zero for the no-slip channel)
   double dr1 = 0., dr2 = 0., di1 = 0., di2 = 0.;
   for (int y = 0; y < n; ++y) {
-    const double2 vv = A.V[(size_t)y * NP + p];
+    const double2 vv = vload(A, (size_t)y * NP + p);
     dr1 = dr1 + vv.x * A.wd[y];
     dr2 = dr2 + vv.x * A.wd[n + y];
     di1 = di1 + vv.y * A.wd[y];
     di2 = di2 + vv.y * A.wd[n + y];
   }
-  const double2 v0 = A.V[p], vn = A.V[(size_t)(n - 1) * NP + p];
+  const double2 v0 = vload(A, p), vn = vload(A, (size_t)(n - 1) * NP + p);
   vr1 = vr1 + (dr1 - k2 * v0.x) / A.re - (v0.x - 0.0) * A.c4t;
   vr2 = vr2 + (dr2 - k2 * vn.x) / A.re - (vn.x - 0.0) * A.c4t;
   vi1 = vi1 + (di1 - k2 * v0.y) / A.re - (v0.y - 0.0) * A.c4t;

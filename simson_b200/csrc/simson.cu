@@ -1358,13 +1358,12 @@ extern "C" int sgpu_xys_reset(sgpu_ctx* c) {
 }
 
 // Pressure of the current state (press.cuh; bla/nonlinp.f + bla/linearp.f as
-// bla/bla.f:2486-2527 runs them), FP64 state only.
+// bla/bla.f:2486-2527 runs them); FP64 arithmetic under either storage.
 extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
   NvtxRange nv("pressure");
   if (c && sharded(c)) return SGPU_E_STATE;  // reads the whole state
   if (!c || !pr || !pi) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
-  if (c->mixed) return SGPU_E_PARAM;  // the FP64 state is not kept under SGPU_MIXED
   const Dims& g = c->g;
   const int n = g.nyp;
   if (n < 9) return SGPU_E_PARAM;
@@ -1405,8 +1404,12 @@ extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
   // step-2 transforms of u, omega and the products H, 2E (nonlinp.f)
   dim3 gz((g.nx2 + c->kb - 1) / c->kb, n);
   const size_t s_z = smem_fft(g.nzp, c->kb, sizeof(double2));
-  launch_zinv<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->st, c->zb, g, c->twz.plan, c->twz.d, c->alfa,
-                                            c->beta, 0);
+  if (c->mixed)
+    launch_zinv<double, sgpu_ctx::kb, float>(gz, s_z, c->stream, c->stf, c->zb, g, c->twz.plan, c->twz.d, c->alfa,
+                                             c->beta, 0);
+  else
+    launch_zinv<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->st, c->zb, g, c->twz.plan, c->twz.d,
+                                              c->alfa, c->beta, 0);
   const size_t s_xp = 2 * (size_t)g.nxp * 3 * sizeof(double2);
   cudaFuncSetAttribute(k_xpass_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_xp);
   k_xpass_p<<<dim3(g.nzp, n), 256, s_xp, c->stream>>>(c->zb, g, c->twx.plan, c->twx.d, P.rot);
@@ -1423,7 +1426,9 @@ extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
                                                       1.0 / (2.0 * (double)g.nxp * (double)g.nzp), 1, c->twy.d);
   PressArgs A;
   A.CD = czf(c, 4); A.CH2 = czf(c, 5); A.CE = czf(c, 6);
-  A.PH2 = czf(c, 1); A.PE = czf(c, 3); A.V = slot(c, 1);
+  A.PH2 = czf(c, 1); A.PE = czf(c, 3);
+  A.V = slot(c, 1);
+  A.Vf = c->mixed ? c->stf + fld : nullptr;
   A.X = czf(c, 7);
   A.Q = reinterpret_cast<double*>(czf(c, 8)); A.Cc = A.Q + fld;
   A.Dd = reinterpret_cast<double*>(czf(c, 9)); A.Ee = A.Dd + fld;

@@ -2,8 +2,8 @@
 bla/bla.f:2486-2527 runs them) against the translated reference built with
 pressure = 1, on the same state after two steps: FP64, relative L2 within
 1e-10 (the kz = -nz/2 plane, which linearp skips, excluded).  Laminar flow
-has zero pressure in this formulation (H2 = dE/dy); under SGPU_MIXED the
-call is refused."""
+has zero pressure in this formulation (H2 = dE/dy).  Under SGPU_MIXED the
+pressure of the FP32-stored state is within 1e-5 of the FP64 one."""
 import os
 
 import numpy as np
@@ -57,8 +57,8 @@ def test_pressure_matches_reference(rms):
         assert np.array_equal(a, b)
 
 
-def test_laminar_pressure_is_zero_and_mixed_is_refused():
-    from simson_b200.bla import Channel, SimsonError
+def test_laminar_pressure_is_zero_and_mixed_close_to_fp64():
+    from simson_b200.bla import Channel
     u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.0, 1)
     ch = Channel(NX, NY, NZ, RE, XL, ZL, DT)
     try:
@@ -68,10 +68,16 @@ def test_laminar_pressure_is_zero_and_mixed_is_refused():
     finally:
         ch.close()
     assert np.abs(p).max() <= 1e-12
-    ch = Channel(NX, NY, NZ, RE, XL, ZL, DT, precision="mixed")
-    try:
-        ch.set_velocity(u, v, w)
-        with pytest.raises(SimsonError):
-            ch.pressure()
-    finally:
-        ch.close()
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.05, 5)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        ch = Channel(NX, NY, NZ, RE, XL, ZL, DT, precision=prec)
+        try:
+            ch.set_velocity(u, v, w)
+            ch.prhs()
+            out[prec] = ch.pressure()
+        finally:
+            ch.close()
+    err = rel(out["mixed"], out["fp64"])
+    print("mixed vs FP64 pressure: %.2e" % err)
+    assert err <= 1e-5
