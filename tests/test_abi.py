@@ -19,7 +19,8 @@ def test_header_declares_the_step_and_its_neighbours():
     names = declared()
     for must in ("sgpu_init", "sgpu_prhs", "sgpu_nonlin", "sgpu_linear", "sgpu_step_rk", "sgpu_upload_state",
                  "sgpu_download_state", "sgpu_amplitudes", "sgpu_xys_sample", "sgpu_set_les", "sgpu_set_shard",
-                 "sgpu_copy_block", "sgpu_offload_steps", "sgpu_finalize"):
+                 "sgpu_copy_block", "sgpu_offload_steps", "sgpu_pressure", "sgpu_box_filter_sample",
+                 "sgpu_xys_get", "sgpu_xys_reset", "sgpu_finalize"):
         assert must in names
 
 
