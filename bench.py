@@ -177,6 +177,12 @@ def own_arm(args, rank, world, precision):
         ch.xys_sample()
     ch.record(1)
     xys_ms = ch.elapsed_ms(0, 1) / 3
+    # one pressure computation (nonlinp + linearp) including its download to the host
+    ch.pressure()
+    ch.record(0)
+    ch.pressure()
+    ch.record(1)
+    press_ms = ch.elapsed_ms(0, 1)
     # end-to-end through the public API with host buffers
     nslots = 7
     shape = (nslots, w["nz"], w["ny"], w["nx"] // 2)
@@ -199,7 +205,8 @@ def own_arm(args, rank, world, precision):
     finite = bool(np.isfinite(sc["px"]))
     ch.close()
     return dict(ms=ms, launches=launches, clocks=clocks, prof=prof, e2e_s=e2e_s, e2e_steps=e2e_steps,
-                e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw, xys_ms=xys_ms)
+                e2e_bytes=nbytes, scalars=sc, finite=finite, uvw=uvw, xys_ms=xys_ms,
+                press_ms=press_ms)
 
 
 LES_WORKLOAD = dict(nx=64, ny=97, nz=64, re=4200.0, xl=2 * np.pi, zl=np.pi, dt=0.005, rms=0.1, seed=4)
@@ -427,6 +434,7 @@ def main():
         "clocks": res["clocks"],
         "finite": res["finite"],
         "xys_sample_ms": res["xys_ms"],
+        "pressure_ms": res["press_ms"],
     }
     if "fp64" in runs and "mixed" in runs:
         r64 = runs["fp64"]
