@@ -112,3 +112,35 @@ def test_bf16_rounding_of_the_mlp_oracle():
     x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 0.0], np.float32)
     # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: to even (1); 1 + 3 * 2^-8 -> 1 + 2^-6
     np.testing.assert_array_equal(bf16(x), np.array([1.0, 1.0, 1.0 + 2 ** -6, -2.5, 0.0], np.float32))
+
+
+def test_pressure_of_mean_profiles_vanishes():
+    """Pressure oracle (bla/nonlinp.f + bla/linearp.f, built with pressure =
+    1): for any flow made of mean profiles U(y), W(y) the wall-normal
+    nonlinear term is H2 = U U' + W W' = dE/dy, so p = phi - E is zero
+    (up to roundoff) whatever the profiles; the pressure of a perturbed
+    field is finite and not zero."""
+    import os
+    from build_ref import REF_BLA, lib_path
+    if not (os.path.isdir(REF_BLA) or os.path.exists(lib_path(16, 17, 16, pressure=True))):
+        pytest.skip("pressure oracle neither buildable nor prebuilt")
+    from refsim import RefSim
+    nx, ny, nz = 16, 17, 16
+    xl, zl = 4 * np.pi, 2 * np.pi
+    y = gl_points(ny)
+    u = np.zeros((nz, ny, nx // 2), complex)
+    w = np.zeros_like(u)
+    u[0, :, 0] = (1 - y ** 2) * (1 + 0.3 * y)
+    w[0, :, 0] = 0.2 * (1 - y ** 4)
+    r = RefSim(nx, ny, nz, 4200.0, xl, zl, 0.01, pressure=True)
+    r.set_velocity(u, np.zeros_like(u), w)
+    r.start()
+    p = r.pressure()
+    keep = np.ones(nz, bool)
+    keep[nz // 2] = False
+    assert np.abs(p[keep]).max() < 1e-12
+    uu, vv, ww = channel_field(nx, ny, nz, xl, zl, 0.05, 3)
+    r.set_velocity(uu, vv, ww)
+    r.start()
+    p = r.pressure()
+    assert np.isfinite(p).all() and np.abs(p[keep]).max() > 1e-6
