@@ -250,6 +250,12 @@ class Channel:
         self._check(self.lib.sgpu_download_state(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp), nslots),
                     "download")
 
+    def pressure_raw(self, re_ptr, im_ptr):
+        """sgpu_pressure into caller-owned host buffers (page-locked ones make
+        the download run at full PCIe speed)."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.sgpu_pressure(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp)), "pressure")
+
     def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1, cs=0.0, ineg=1):
         """Large-eddy model (defaults of bla/rparamles.f): iles 1 ADM-RT, 2 eddy
         viscosity (cs = 0: dynamic Smagorinsky).  Call before prhs()."""
