@@ -407,7 +407,7 @@ def main():
     dom_ms = prof[dom][0] / prof[dom][1]
     dom_bytes = kernel_bytes(dom, w, head)
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    # from ncu captures of this build at this workload, summarised in
+    # from ncu captures of these kernels at this workload, summarised in
     # profiles/: the pencil kernel captured at 384x193x384 (one pass), the x
     # pass at 384x33x384 scaled by ny (its traffic grows with the planes)
     measured_traffic = {("mixed", "pencil"): 2.64e9 + 2.53e9, ("mixed", "xpass"): (175.30e6 + 60.77e6) * 193 / 33}
