@@ -145,6 +145,23 @@ typedef struct {
  * model set with sgpu_set_les).  Needs nx, nz divisible by 4. */
 int sgpu_set_sgs_mlp(sgpu_ctx* ctx, const sgpu_sgs_mlp* p);
 
+/* Training of the learned SGS model (no counterpart in the reference):
+ * iters full-batch Adam steps (beta1 0.9, beta2 0.999, eps 1e-8, learning
+ * rate lr; *adam_step counts the steps taken, for the bias corrections) on
+ * the mean squared error sum (y - t)^2 / (6 n) of the network of
+ * sgpu_sgs_mlp without its scales, y = W3 tanh(W2 tanh(W1 x + b1) + b2) + b3,
+ * over n samples x[n][10], t[n][6] (host arrays, e.g. the features and
+ * targets of sgpu_box_filter_sample, scaled as they will be at inference).
+ * params: the 5254 FP32 weights packed W1 [64][10], b1 [64], W2 [64][64],
+ * b2 [64], W3 [6][64], b3 [6]; adam_m, adam_v the same size; all three are
+ * updated.  On return *loss (if not NULL) holds the loss and grad (if not
+ * NULL, 5254 values) the gradient at the final weights (iters = 0: at the
+ * given ones).  FP32 arithmetic; allocates its device buffers for the call.
+ * Synchronises the library's stream. */
+int sgpu_sgs_mlp_train(sgpu_ctx* ctx, float* params, float* adam_m, float* adam_v, int* adam_step,
+                       const float* x, const float* t, long long n, int iters, float lr, float* loss,
+                       float* grad);
+
 /* The MLP alone on n feature rows: x[n][10] -> y[n][6] (host arrays), the
  * same tensor-core kernel the step runs.  Loads p's weights. */
 int sgpu_sgs_mlp_eval(sgpu_ctx* ctx, const sgpu_sgs_mlp* p, const float* x, float* y, long long n);

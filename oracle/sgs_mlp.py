@@ -135,3 +135,51 @@ def viscosity_weights(nu_t, a=0.1, s_in=0.2):
         w3[c, q] += g
     z = np.zeros(64, np.float32)
     return {"w1": w1, "b1": z, "w2": w2, "b2": z.copy(), "w3": w3, "b3": np.zeros(6, np.float32)}
+
+
+# ---------------------------------------------------------------------------
+# Training (sgpu_sgs_mlp_train): FP64 restatement of the loss, its gradient
+# and the Adam step, on the packed weights W1 [64][10], b1 [64], W2 [64][64],
+# b2 [64], W3 [6][64], b3 [6].
+# ---------------------------------------------------------------------------
+MLP_SLICES = (("w1", 0, (64, 10)), ("b1", 640, (64,)), ("w2", 704, (64, 64)), ("b2", 4800, (64,)),
+              ("w3", 4864, (6, 64)), ("b3", 5248, (6,)))
+MLP_NPAR = 5254
+
+
+def mlp_pack(w):
+    """Weights dict (init_weights) -> packed vector (float32)."""
+    return np.concatenate([np.asarray(w[k], np.float32).ravel() for k, _, _ in MLP_SLICES])
+
+
+def mlp_unpack(p):
+    return {k: np.asarray(p[o:o + int(np.prod(sh))], np.float64).reshape(sh) for k, o, sh in MLP_SLICES}
+
+
+def mlp_loss_grad(p, x, t):
+    """Loss sum (y - t)^2 / (6 n) of y = W3 tanh(W2 tanh(W1 x + b1) + b2) + b3
+    (no BF16 rounding, no scales) and its gradient, packed, in float64."""
+    w = mlp_unpack(p)
+    x = np.asarray(x, np.float64)
+    t = np.asarray(t, np.float64)
+    n = x.shape[0]
+    h1 = np.tanh(x @ w["w1"].T + w["b1"])
+    h2 = np.tanh(h1 @ w["w2"].T + w["b2"])
+    y = h2 @ w["w3"].T + w["b3"]
+    r = y - t
+    loss = float((r * r).sum() / (6 * n))
+    d3 = 2.0 * r / (6 * n)
+    g2 = (d3 @ w["w3"]) * (1 - h2 * h2)
+    g1 = (g2 @ w["w2"]) * (1 - h1 * h1)
+    grad = {"w1": g1.T @ x, "b1": g1.sum(0), "w2": g2.T @ h1, "b2": g2.sum(0), "w3": d3.T @ h2, "b3": d3.sum(0)}
+    return loss, np.concatenate([grad[k].ravel() for k, _, _ in MLP_SLICES])
+
+
+def adam_step(p, m, v, g, step, lr, b1=0.9, b2=0.999, eps=1e-8):
+    """One Adam update (step counts from 1), float64."""
+    m = b1 * m + (1 - b1) * g
+    v = b2 * v + (1 - b2) * g * g
+    mh = m / (1 - b1 ** step)
+    vh = v / (1 - b2 ** step)
+    return p - lr * mh / (np.sqrt(vh) + eps), m, v
+

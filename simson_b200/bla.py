@@ -92,6 +92,11 @@ def load_library(build: bool = True):
     lib.sgpu_box_filter_sample.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                                            ctypes.POINTER(ctypes.c_float)]
     lib.sgpu_pressure.argtypes = [vp, dp, dp]
+    lib.sgpu_sgs_mlp_train.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                       ctypes.c_longlong, ctypes.c_int, ctypes.c_float,
+                                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
     lib.sgpu_set_les.argtypes = [vp, ctypes.POINTER(SgpuLesParams)]
     lib.sgpu_download_les.argtypes = [vp, dp, dp]
     lib.sgpu_download_sgs_stress.argtypes = [vp, dp, dp]
@@ -332,6 +337,26 @@ class Channel:
 
     def xys_reset(self):
         self._check(self.lib.sgpu_xys_reset(self._ctx), "xys_reset")
+
+    def sgs_mlp_train(self, params, adam_m, adam_v, adam_step, x, t, iters, lr):
+        """Full-batch Adam training of the learned SGS model on the device
+        (sgpu_sgs_mlp_train).  params, adam_m, adam_v: packed float32 (5254);
+        x [n][10], t [n][6].  Returns (params, adam_m, adam_v, adam_step,
+        loss, grad) after iters steps (loss and grad at the final weights)."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        p = np.ascontiguousarray(params, np.float32).copy()
+        m = np.ascontiguousarray(adam_m, np.float32).copy()
+        v = np.ascontiguousarray(adam_v, np.float32).copy()
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        step = ctypes.c_int(int(adam_step))
+        loss = ctypes.c_float()
+        grad = np.empty(p.size, np.float32)
+        self._check(self.lib.sgpu_sgs_mlp_train(self._ctx, p.ctypes.data_as(fp), m.ctypes.data_as(fp),
+                                                v.ctypes.data_as(fp), ctypes.byref(step), x.ctypes.data_as(fp),
+                                                t.ctypes.data_as(fp), x.shape[0], int(iters), float(lr),
+                                                ctypes.byref(loss), grad.ctypes.data_as(fp)), "sgs_mlp_train")
+        return p, m, v, step.value, loss.value, grad
 
     def pressure(self):
         """Pressure of the current state (bla/nonlinp.f + bla/linearp.f),

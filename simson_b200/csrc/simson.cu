@@ -22,6 +22,7 @@
 #include "sgs_mlp.cuh"
 #include "xys.cuh"
 #include "press.cuh"
+#include "mlp_train.cuh"
 
 #include <nvtx3/nvToolsExt.h>
 #include "mixed.h"
@@ -1449,6 +1450,68 @@ extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
   CK(cudaStreamSynchronize(c->stream));
   c->press_valid = true;
   return SGPU_OK;
+}
+
+// Training of the learned SGS model (mlp_train.cuh): iters full-batch Adam
+// steps on n host samples, then the loss and the gradient at the final
+// weights.  Device buffers are allocated for the call and freed after it.
+extern "C" int sgpu_sgs_mlp_train(sgpu_ctx* c, float* params, float* adam_m, float* adam_v, int* adam_step,
+                                  const float* x, const float* t, long long n, int iters, float lr, float* loss,
+                                  float* grad) {
+  NvtxRange nv("learned SGS training");
+  if (!c || !params || !adam_m || !adam_v || !adam_step || !x || !t || n < 1 || iters < 0 || !(lr >= 0.0f))
+    return SGPU_E_PARAM;
+  const long long nchunk = (n + MLP_CHUNK - 1) / MLP_CHUNK;
+  if (nchunk > 0x7fffffffLL) return SGPU_E_PARAM;
+  const size_t np = MLP_NPAR, np1 = MLP_NPAR + 1;
+  float *d_par = nullptr, *d_m = nullptr, *d_v = nullptr, *d_g = nullptr, *d_part = nullptr, *d_x = nullptr,
+        *d_t = nullptr;
+  auto release = [&] {
+    for (float* q : {d_par, d_m, d_v, d_g, d_part, d_x, d_t})
+      if (q) cudaFree(q);
+  };
+  if (cudaMalloc(&d_par, np * sizeof(float)) != cudaSuccess || cudaMalloc(&d_m, np * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&d_v, np * sizeof(float)) != cudaSuccess || cudaMalloc(&d_g, np1 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&d_part, (size_t)nchunk * np1 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&d_x, (size_t)n * MLP_NIN * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&d_t, (size_t)n * MLP_NOUT * sizeof(float)) != cudaSuccess) {
+    release();
+    return SGPU_E_CUDA;
+  }
+  int rc = SGPU_OK;
+  auto chk = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == SGPU_OK) rc = cuda_fail(e, "sgs mlp training");
+  };
+  chk(cudaMemcpyAsync(d_par, params, np * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  chk(cudaMemcpyAsync(d_m, adam_m, np * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  chk(cudaMemcpyAsync(d_v, adam_v, np * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  chk(cudaMemcpyAsync(d_x, x, (size_t)n * MLP_NIN * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  chk(cudaMemcpyAsync(d_t, t, (size_t)n * MLP_NOUT * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  chk(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_TRAIN_SMEM));
+  const int gb = (int)((np1 + 255) / 256);
+  for (int it = 0; it <= iters && rc == SGPU_OK; ++it) {
+    k_mlp_grad<<<(unsigned)nchunk, MLP_TRAIN_THREADS, MLP_TRAIN_SMEM, c->stream>>>(d_par, d_x, d_t, n, d_part);
+    k_mlp_reduce<<<gb, 256, 0, c->stream>>>(d_part, (int)nchunk, d_g);
+    c->launches += 2;
+    if (it == iters) break;  // the gradient and loss at the final weights
+    const int step = ++*adam_step;
+    const float c1 = (float)(1.0 / (1.0 - pow(0.9, (double)step)));
+    const float c2 = (float)(1.0 / (1.0 - pow(0.999, (double)step)));
+    k_mlp_adam<<<gb, 256, 0, c->stream>>>(d_par, d_m, d_v, d_g, lr, c1, c2);
+    c->launches++;
+    chk(cudaGetLastError());
+  }
+  chk(cudaGetLastError());
+  float sse = 0.0f;
+  chk(cudaMemcpyAsync(params, d_par, np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  chk(cudaMemcpyAsync(adam_m, d_m, np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  chk(cudaMemcpyAsync(adam_v, d_v, np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  if (grad) chk(cudaMemcpyAsync(grad, d_g, np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  chk(cudaMemcpyAsync(&sse, d_g + np, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  chk(cudaStreamSynchronize(c->stream));
+  if (loss) *loss = sse / (6.0f * (float)n);
+  release();
+  return rc;
 }
 
 extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
