@@ -19,6 +19,8 @@
 #ifndef SIMSON_B200_H
 #define SIMSON_B200_H
 
+#include <stddef.h> /* size_t */
+
 #ifdef __cplusplus
 extern "C" {
 #endif

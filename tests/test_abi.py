@@ -5,6 +5,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "simson_b200.h")
 
@@ -78,3 +80,19 @@ def test_entry_points_reject_a_null_context():
     assert lib.sgpu_finalize(None) == 0
     for rc in (0, -1, -2, -3, -4, -5):
         assert lib.sgpu_error_string(rc)
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
+def test_header_compiles_on_its_own(tmp_path, lang, std):
+    """A C or C++ host includes the header first: it must bring what it uses."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / "host.txt"
+    src.write_text('#include "simson_b200.h"\nint main(void) { return 0; }\n')
+    r = subprocess.run([cc, "-std=" + std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                        os.path.join(ROOT, "include"), "-x", lang, str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
