@@ -1,5 +1,5 @@
 """The reference's velocity field file (``.u``): written by bla/wdiscbl.f,
-read by bla/rdiscbl.f; the checkpoint of a run (a restart at a full step is
+read by bla/rdiscbl.f (and its pressure file ``.p`` of bla/wdiscp.f); the checkpoint of a run (a restart at a full step is
 exact in exact arithmetic: the first RK stage has b_1 = 0, so the partial
 right-hand sides are rebuilt from u by prhs).
 
@@ -34,6 +34,16 @@ _EXTRA = {-1: ("rlam",), -2: ("rlam", "spanv"), 4: ("bstart", "blength"), 5: ("b
 _VALID = set(range(-3, 0)) | set(range(1, 10)) | {20, -20}
 
 
+# extra header record of the pressure file (bla/wdiscp.f, the .p file): every
+# fltype >= 6 writes bstart, blength, rlam, spanv, 20 included
+def _extra_names(fltype, pressure_file=False):
+    if not pressure_file:
+        return _EXTRA.get(fltype)
+    if fltype >= 6:
+        return ("bstart", "blength", "rlam", "spanv")
+    return {-1: ("rlam",), -2: ("rlam", "spanv"), 4: ("bstart", "blength"), 5: ("bstart", "blength")}.get(fltype)
+
+
 class UFileError(ValueError):
     """A .u file the reader cannot take (the cases where rdiscbl stops)."""
 
@@ -45,7 +55,15 @@ def _record(f, payload: bytes):
     f.write(n)
 
 
-def write_u(path, fields, re, xl, zl, t, dstar=1.0, fltype=1, **extra):
+def write_p(path, p, re, xl, zl, t, dstar=1.0, fltype=1, **extra):
+    """Write a pressure field (complex (nz, nyp, nx/2), e.g. from
+    Channel.pressure) as bla/wdiscp.f does: the header of the velocity file
+    and the one field (slot 8).  The reference names the file after the
+    velocity file with '.p' appended; path is the full name."""
+    write_u(path, [p], re, xl, zl, t, dstar, fltype, _pressure_file=True, **extra)
+
+
+def write_u(path, fields, re, xl, zl, t, dstar=1.0, fltype=1, _pressure_file=False, **extra):
     """Write fields (m complex arrays (nz, nyp, nx/2)) as wdiscbl does with
     xs = zs = 0 (no box shift) and gall = .false.."""
     fields = [np.asarray(q) for q in fields]
@@ -57,8 +75,8 @@ def write_u(path, fields, re, xl, zl, t, dstar=1.0, fltype=1, **extra):
         _record(f, struct.pack("<di4d", re, 0, xl, zl, t, 0.0))
         _record(f, struct.pack("<4i", nx, nyp, nz, 0))
         _record(f, struct.pack("<id", fltype, dstar))
-        if fltype in _EXTRA:
-            names = _EXTRA[fltype]
+        names = _extra_names(fltype, _pressure_file)
+        if names is not None:
             _record(f, struct.pack("<%dd" % len(names), *[float(extra.get(k, 0.0)) for k in names]))
         row = np.empty(nx, "<f8")
         for q in fields:
@@ -109,13 +127,14 @@ def _cheb_regrid(q, nyp_out):
     return np.einsum("yk,zkx->zyx", np.cos(np.outer(theta_out, j)), a)
 
 
-def read_u(path, m=3, nx=None, nyp=None, nz=None, varsiz=True):
+def read_u(path, m=3, nx=None, nyp=None, nz=None, varsiz=True, pressure_file=False):
     """Read a .u file.  Returns (header dict, list of m fields (nz, nyp,
     nx/2)).  With a target size different from the file's, as rdiscbl does
     with varsiz: x and z modes truncated or zero-padded, y refined (never
     reduced) by Chebyshev re-expansion; the kz = -nzin/2 mode of an even
     file grid, which is not an oddball on a larger grid, is zeroed.  Raises
-    UFileError where rdiscbl stops."""
+    UFileError where rdiscbl stops.  pressure_file: a .p file of wdiscp
+    (its header record by flow type; read it with m = 1)."""
     r = _Reader(path)
     rec = r.record()
     if len(rec) != 44:
@@ -135,9 +154,12 @@ def read_u(path, m=3, nx=None, nyp=None, nz=None, varsiz=True):
         raise UFileError(f"the file does not contain a known flow type: {fltype}")
     head = dict(re=re, pou=bool(pou), xl=xl, zl=zl, t=t, xs=xs, nx=nxin, nyp=nypin, nzc=nzcin, nfzsym=nfzsin,
                 fltype=fltype, dstar=dstar)
-    if fltype in _EXTRA:
-        names = _EXTRA[fltype]
-        vals = struct.unpack("<%dd" % len(names), r.record())
+    names = _extra_names(fltype, pressure_file)
+    if names is not None:
+        rec = r.record()
+        if len(rec) != 8 * len(names):
+            raise UFileError(f"flow-type {fltype} header record of the wrong length")
+        vals = struct.unpack("<%dd" % len(names), rec)
         head.update(zip(names, vals))
     if nfzsin != 0:
         raise UFileError("z-symmetric fields (nfzsym = 1) are not supported")

@@ -116,3 +116,22 @@ def test_refuses_corrupt_files(tmp_path):
         read_u(bad)
     with pytest.raises(UFileError):
         read_u(p, nx=16, varsiz=False)
+
+
+def test_pressure_file(tmp_path):
+    """bla/wdiscp.f's .p file: the velocity file's header and one field; its
+    flow-type record differs for fltype >= 6 (four values, 20 included)."""
+    from simson_b200.ufile import write_p
+    (p,) = fields(8, 9, 6, 11, m=1)
+    f = tmp_path / "field.u.p"
+    write_p(f, p, 4200.0, 12.5, 6.25, 3.0)
+    b = f.read_bytes()
+    assert len(b) == 96 + 6 * 9 * (8 + 8 * 8)   # header as the .u file, one field
+    head, (back,) = read_u(f, m=1, pressure_file=True)
+    assert head["t"] == 3.0 and np.array_equal(back, p)
+    write_p(f, p, 400.0, 100.0, 10.0, 0.0, fltype=20, bstart=1.0, blength=2.0, rlam=0.5, spanv=0.25)
+    head, (back,) = read_u(f, m=1, pressure_file=True)
+    assert (head["bstart"], head["blength"], head["rlam"], head["spanv"]) == (1.0, 2.0, 0.5, 0.25)
+    assert np.array_equal(back, p)
+    with pytest.raises(UFileError):  # read as a velocity file the fltype-20 record does not fit
+        read_u(f, m=1)
