@@ -37,6 +37,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+REF_MAX_STEPS = 20
 WORKLOAD = dict(nx=384, ny=193, nz=384, re=9000.0, xl=2 * np.pi, zl=np.pi, dt=0.002, rms=0.1, seed=3)
 METRIC = "RK3 steps/s at 384x193x384"
 
@@ -304,26 +305,47 @@ def dist_max(x, world):
     return float(t.item())
 
 
-def cpu_reference(steps, threads, sample_note):
-    """Time the reference's own implementation (translated Fortran) on host cores."""
+def cpu_reference(steps, threads, sample_note, warmup_substeps=1):
+    """Time the reference's own implementation (translated Fortran) on host
+    cores: `steps` full RK3 steps after `warmup_substeps` untimed substeps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from build_ref import REF_BLA
     from refsim import RefSim
     from simson_b200.fields import channel_field
     w = WORKLOAD
     ref = RefSim(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], threads=threads,
-                 build=os.path.isdir(os.environ.get("SIMSON_REFERENCE", "/root/reference")))
+                 build=os.path.isdir(REF_BLA))
     u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"])
     ref.set_velocity(u, v, wv)
     ref.start()
-    ref.substep()  # warm-up substep (page faults, caches)
+    for _ in range(warmup_substeps):
+        ref.substep()  # page faults, caches
     t0 = time.perf_counter()
-    ref.substep()
-    ref.substep()
-    ref.substep()
+    ref.step(steps)
     dt = time.perf_counter() - t0
-    return dict(value=1.0 / dt, unit="steps/s", cores=threads, kind="reference",
-                sample=f"{sample_note}: 1 full RK3 step (3 substeps) after 1 warm-up substep, "
-                       f"translated reference bla (gcc -O3 -fopenmp), {threads} threads")
+    return dict(value=steps / dt, unit="steps/s", cores=threads, kind="reference", steps=steps,
+                sample=f"{sample_note}: {steps} full RK3 steps ({3 * steps} substeps) after {warmup_substeps} "
+                       f"warm-up substep(s), translated reference bla (gcc -O3 -fopenmp, the reference's own "
+                       f"Fortran translated to C: no Fortran compiler exists on either machine, so bla's own "
+                       f"'Wall time' lines cannot be used), {threads} threads")
+
+
+def profile_case(grid, substeps, precision):
+    """A few substeps of the channel step on one grid, for profiler captures
+    (ncu -k ... -s ... python bench.py --case GRID): prints the per-kernel
+    milliseconds of the last substep (CUDA events)."""
+    from simson_b200.bla import FP64, MIXED, Channel
+    from simson_b200.fields import channel_field
+    nx, ny, nz = (int(v) for v in grid.split("x"))
+    xl, zl = 4 * np.pi, 2 * np.pi
+    ch = Channel(nx, ny, nz, 4200.0, xl, zl, 0.005, precision=MIXED if precision == "mixed" else FP64)
+    ch.set_velocity(*channel_field(nx, ny, nz, xl, zl, 0.1, 2))
+    ch.prhs()
+    ch.substeps(substeps)
+    ch.profile(True)
+    ch.substeps(1)
+    print({k: round(v[0], 4) for k, v in ch.profile_read().items() if v[1]})
+    ch.close()
 
 
 def main():
@@ -336,10 +358,17 @@ def main():
                     help="both: time FP64 and mixed; value is the mixed-precision step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-les", action="store_true", help="skip the LES-configuration timings")
+    ap.add_argument("--case", default=None, metavar="NXxNYxNZ",
+                    help="profiling case: run --substeps substeps on this grid and print per-kernel times "
+                         "(no JSON line; for ncu captures)")
+    ap.add_argument("--substeps", type=int, default=3)
     ap.add_argument("--shard", action="store_true",
                     help="one channel split over the ranks (z-slab shards, NCCL all-to-alls; strong scaling) "
                          "instead of one replica per rank")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args.case, args.substeps, "mixed" if args.precision == "mixed" else "fp64")
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if world > 1:
@@ -352,20 +381,24 @@ def main():
     w = WORKLOAD
     config = {"workload": "temporal channel 384x193x384 (576x193x576 dealiased), box 2pi x 2 x pi, Re_cl 9000, "
                           "cflux, dt 0.002, seeded rms 0.1 perturbation", "nx": w["nx"], "ny": w["ny"], "nz": w["nz"],
-              "precision": args.precision, "l2": "state 1.6 GB > L2, no flush needed",
-              "parallelism": f"replicas x{args.gpus}"}
+              "l2": "state 1.6 GB > L2, no flush needed",
+              "parallelism": f"independent replicas x{args.gpus} (one whole channel per GPU, no exchange)"}
     if args.impl == "reference":
-        config["precision"] = "fp64 (the reference computes in double precision)"
         if rank != 0:
             return
+        # each timed step is one full RK3 step of the workload on all host
+        # cores (about 1.7 s on 16 cores); at most REF_MAX_STEPS of them so
+        # that the arm ends within a few minutes
+        nsteps = max(1, min(args.steps, REF_MAX_STEPS))
         try:
-            r = cpu_reference(args.steps, threads, "per step")
+            r = cpu_reference(nsteps, threads, "per step", warmup_substeps=3 * max(1, min(args.warmup, 1)))
         except Exception as e:  # pragma: no cover
             print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build failed: {e}"}))
             return
-        line = {"metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": args.gpus, "steps": 1,
+        line = {"metric": METRIC, "value": r["value"], "unit": "steps/s", "n_gpus": args.gpus, "steps": nsteps,
                 "warmup": 1, "ms_per_step": 1000.0 / r["value"], "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "precision": "fp64 (the reference computes in double precision)", "impl": "reference",
                 "cpu_baseline": r, "e2e": {"value": r["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -378,8 +411,8 @@ def main():
             dist.destroy_process_group()
         if rank == 0:
             config["parallelism"] = f"z-slab shards x{world} (step 2 on ny/{world} planes, step 3 on nz/{world} kz planes)"
-            config["precision"] = prec
             print(json.dumps({
+                "precision": prec,
                 "metric": METRIC, "value": args.steps / (r["ms"] / 1000.0), "unit": "steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
@@ -420,10 +453,11 @@ def main():
         roof.update(achieved=None, frac=None, algorithmic_bytes=None)
     stage_bytes = substep_bytes(nc, head)
     step_ach = 3 * stage_bytes / (ms_step / 1000.0) / 1e9
-    config["precision"] = {"mixed": "mixed: FP32 x/z FFTs, products, Chebyshev transforms and u,v,w,omega storage; "
-                                    "FP64 tau solves, mean flow, partial RHS",
-                           "fp64": "fp64: every transform and solve in FP64"}[head]
+    precision_note = {"mixed": "mixed: FP32 x/z FFTs, products, Chebyshev transforms and u,v,w,omega storage; "
+                               "FP64 tau solves, mean flow, partial RHS",
+                      "fp64": "fp64: every transform and solve in FP64"}[head]
     line = {
+        "precision": precision_note,
         "metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
@@ -459,7 +493,7 @@ def main():
         line["les"] = les_arm(max(args.steps, 20), max(args.warmup, 3))
     if world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_reference(1, threads, "bounded sample")
+            line["cpu_baseline"] = cpu_reference(3, threads, "bounded sample")
         except Exception as e:  # pragma: no cover
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     print(json.dumps(line))

@@ -269,12 +269,17 @@ int sgpu_sync(sgpu_ctx* ctx);
  * complex doubles (kx fastest, the library's device layout); h_out: device
  * array of H1, H2, H3 in the same layout; cflp_max (host, may be NULL): the
  * CFL partial maximum max|u|/dx+|v|/dy+|w|/dz of bla/boxcfl.f; stream: a
- * cudaStream_t or NULL.  Allocates nothing: the step's intermediates sit in
- * one static device array of 64 MiB that every GPU loading the library holds
- * until exit; grids needing more (9*ny*(3nz/2)*(nx/2)*16 bytes) are rejected
- * with SGPU_E_PARAM.  Every call shares that array, so calls that overlap on
- * the GPU race; the first call on a device looks up the array's address
- * (make it before any stream capture). */
+ * cudaStream_t or NULL.  prm->precision must be SGPU_FP64 (the arrays are
+ * complex doubles); no LES term is added.  Allocates nothing: the step's
+ * intermediates sit in one static device array of 64 MiB that every GPU
+ * loading the library holds until exit; grids needing more
+ * (9*ny*(3nz/2)*(nx/2)*16 bytes) are rejected with SGPU_E_PARAM.  Every call
+ * shares that array, so calls that overlap on the GPU race.  Every call looks
+ * up the array's device address with the caller's device current (the first
+ * lookup on a device may load the library's device code: make the first call
+ * on a device before any stream capture), copies its small tables from host
+ * memory into the array, and, when cflp_max is given, waits for the stream to
+ * read the CFL maximum back. */
 int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in, void* h_out, double* cflp_max,
                         void* stream);
 

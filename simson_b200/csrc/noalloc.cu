@@ -15,13 +15,20 @@
 //     SGPU_NOALLOC_TABLE_BYTES of tables; every GPU that loads the library
 //     holds it until the process exits;
 //   * grids whose intermediates need more (9*ny*(3nz/2)*(nx/2) complex doubles)
-//     are rejected with SGPU_E_PARAM and a message on stderr;
+//     are rejected with SGPU_E_PARAM and a message on stderr; so are
+//     precision != SGPU_FP64 (the arrays are complex doubles) and the LES
+//     models (this entry point forms H = u x omega only);
 //   * every call uses the same array and leaves its contents behind; calls that
 //     overlap on the GPU (different streams, or different host threads on the
 //     same device) race on it and must be serialised by the caller;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//   * every call looks up the array's device address (cudaGetSymbolAddress)
+//     with the caller's device current, so a device reset or another context
+//     on the same device never sees a stale address; the first lookup on a
+//     device may load the library's device code, so make the first call on a
+//     device before any stream capture;
+//   * every call copies its small tables (twiddles, wavenumbers, CFL spacing)
+//     from host memory into the array and, when cflp_max is given, waits for
+//     the stream to read the CFL maximum back.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -45,29 +52,19 @@ static __device__ __align__(256) unsigned char g_noalloc_area[SGPU_NOALLOC_SCRAT
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-unsigned char* g_area_ptr[kMaxDevices] = {};
-
-// Host address of the static array is a stand-in, not a device address: the
-// device address is looked up once per device with that device current.
+// The host-side name of the static array is a stand-in, not a device
+// address: the device address is looked up on every call, with the caller's
+// device current (cheap, and it allocates nothing).
 int area_for_current_device(unsigned char** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SGPU_E_CUDA;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_area_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_area);
-    if (e != cudaSuccess || p == nullptr) {
-      fprintf(stderr, "simson_b200: sgpu_nonlin_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
-      return SGPU_E_CUDA;
-    }
-    g_area_ptr[dev] = static_cast<unsigned char*>(p);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_area);
+  if (e != cudaSuccess || p == nullptr) {
+    fprintf(stderr, "simson_b200: sgpu_nonlin_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+    return SGPU_E_CUDA;
   }
-  *out = g_area_ptr[dev];
+  *out = static_cast<unsigned char*>(p);
   return SGPU_OK;
 }
-
 
 }  // namespace
 
@@ -77,6 +74,10 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   const sgpu_params& P = *prm;
   if (P.nx < 4 || P.nz < 4 || P.nx % 4 || P.nz % 2 || P.ny < 9 || (P.ny % 2) == 0 || !(P.xl > 0) || !(P.zl > 0))
     return SGPU_E_PARAM;
+  if (P.precision != SGPU_FP64) {
+    fprintf(stderr, "simson_b200: sgpu_nonlin_noalloc: only precision SGPU_FP64 (complex double arrays)\n");
+    return SGPU_E_PARAM;
+  }
   Dims g{};
   g.nx = P.nx; g.ny = P.ny; g.nz = P.nz;
   g.nx2 = P.nx / 2; g.nyp = P.ny;
@@ -111,34 +112,39 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   double* dyi = beta + SGPU_NOALLOC_MAX_MODES;
   unsigned long long* cfl_bits = reinterpret_cast<unsigned long long*>(dyi + SGPU_NOALLOC_MAX_MODES);
 
-  // tables on the host stack (no allocation), copied into the area; the
-  // same formulas as sgpu_init so the results match sgpu_nonlin bit for bit
+  // tables on the host stack (no allocation), packed as they sit in the area
+  // and copied with one call; the same formulas as sgpu_init so the results
+  // match sgpu_nonlin bit for bit
   {
-    double2 tw[SGPU_NOALLOC_MAX_FFT];
+    static_assert(sizeof(double2) * 2 * SGPU_NOALLOC_MAX_FFT + sizeof(double) * 3 * SGPU_NOALLOC_MAX_MODES <=
+                      SGPU_NOALLOC_TABLE_BYTES - 256,
+                  "tables exceed their part of the area");
+    constexpr size_t kTab = sizeof(double2) * 2 * SGPU_NOALLOC_MAX_FFT + sizeof(double) * 3 * SGPU_NOALLOC_MAX_MODES;
+    // one static host block for every caller, held under a lock while it is
+    // filled and staged by the copy below
+    alignas(16) static unsigned char host_tab[kTab];
+    static std::mutex host_tab_lock;
+    std::lock_guard<std::mutex> lock(host_tab_lock);
+    double2* htwz = reinterpret_cast<double2*>(host_tab);
+    double2* htwx = htwz + SGPU_NOALLOC_MAX_FFT;
+    double* halfa = reinterpret_cast<double*>(htwx + SGPU_NOALLOC_MAX_FFT);
+    double* hbeta = halfa + SGPU_NOALLOC_MAX_MODES;
+    double* hdyi = hbeta + SGPU_NOALLOC_MAX_MODES;
     for (int pass = 0; pass < 2; ++pass) {
       const int n = pass ? g.nxp : g.nzp;
+      double2* tw = pass ? htwx : htwz;
       for (int m = 0; m < n; ++m) {
         long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
         tw[m] = double2{(double)cosl(ang), (double)sinl(ang)};
       }
-      if (cudaMemcpyAsync(pass ? twx : twz, tw, n * sizeof(double2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-          cudaStreamSynchronize(st) != cudaSuccess)
-        return SGPU_E_CUDA;
     }
     const double pi = 3.1415926535897932385;
-    double t[SGPU_NOALLOC_MAX_MODES];
-    for (int x = 0; x < g.nx2; ++x) t[x] = 2. * pi / P.xl * (double)x;
-    if (cudaMemcpyAsync(alfa, t, g.nx2 * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return SGPU_E_CUDA;
-    for (int z = 0; z < g.nz; ++z) t[z] = 0.0;
+    for (int x = 0; x < g.nx2; ++x) halfa[x] = 2. * pi / P.xl * (double)x;
+    for (int z = 0; z < g.nz; ++z) hbeta[z] = 0.0;
     for (int z = 1; z <= g.nz / 2; ++z) {
-      t[z] = 2. * pi / P.zl * (double)z;
-      t[g.nz - z] = -2. * pi / P.zl * (double)z;
+      hbeta[z] = 2. * pi / P.zl * (double)z;
+      hbeta[g.nz - z] = -2. * pi / P.zl * (double)z;
     }
-    if (cudaMemcpyAsync(beta, t, g.nz * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return SGPU_E_CUDA;
     double eta[SGPU_NOALLOC_MAX_MODES], deta[SGPU_NOALLOC_MAX_MODES];
     for (int y = 0; y < g.nyp; ++y) eta[y] = cos(pi * (double)y / (double)(g.nyp - 1));
     deta[0] = 1. - eta[1];
@@ -147,11 +153,11 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
     for (int y = 0; y < g.nyp; ++y) {
       double d = (double)(g.ny - 1) / (double)(g.nyp - 1) / deta[y];
       if (g.ny >= 17) d = fmin(d, (double)(g.ny - 1) * (double)(g.ny - 1) / 10. / 3.14);
-      t[y] = d;
+      hdyi[y] = d;
     }
-    if (cudaMemcpyAsync(dyi, t, g.nyp * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return SGPU_E_CUDA;
+    // a copy from pageable memory: it returns once the block is staged, so the
+    // block may be refilled after it
+    if (cudaMemcpyAsync(twz, host_tab, kTab, cudaMemcpyHostToDevice, st) != cudaSuccess) return SGPU_E_CUDA;
   }
   // the CFL word starts at zero every call
   if (cudaMemsetAsync(cfl_bits, 0, sizeof(unsigned long long), st) != cudaSuccess) return SGPU_E_CUDA;
@@ -160,9 +166,16 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   const size_t s_z = 2 * (size_t)g.nzp * KB * sizeof(double2);
   const size_t s_x = 2 * (size_t)g.nxp * 3 * RB * sizeof(double2);
   if (s_z > 227 * 1024 || s_x > 227 * 1024) return SGPU_E_PARAM;
-  cudaFuncSetAttribute(k_zinv<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_zfwd<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z);
-  cudaFuncSetAttribute(k_xpass<double, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x);
+  if (cudaFuncSetAttribute(k_zinv<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_zfwd<double, KB, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_z) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_xpass<double, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_x) !=
+          cudaSuccess) {
+    fprintf(stderr, "simson_b200: sgpu_nonlin_noalloc: shared-memory opt-in refused: %s\n",
+            cudaGetErrorString(cudaGetLastError()));
+    return SGPU_E_CUDA;
+  }
   const double2* in = static_cast<const double2*>(fields_in);
   double2* out = static_cast<double2*>(h_out);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp);

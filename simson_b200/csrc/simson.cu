@@ -1090,22 +1090,11 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
   return SGPU_OK;
 }
 
-extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
-  if (c) c->press_valid = false;  // the state changes
-  NvtxRange nv("offload steps");
-  if (!c || !ur || !ui || nsteps < 0) return SGPU_E_PARAM;
-  if (sharded(c)) return SGPU_E_STATE;
+// The steps of sgpu_offload_steps; on an error the caller drains the copy
+// streams before returning, so no copy of ur, ui is still running.
+static int offload_enqueue(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
   const Dims& g = c->g;
   const size_t n1 = (size_t)g.nyp * g.NP;  // one slot of the reference layout
-  if (!c->h2d) {
-    CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
-    for (int k = 0; k < 7; ++k) {
-      CK(cudaEventCreateWithFlags(&c->up_done[k], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->out_ready[k], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->down_done[k], cudaEventDisableTiming));
-    }
-  }
   double* sre = c->stage;           // staging of the reference layout, slot k at k * n1
   double* sim = c->stage + 7 * n1;
   for (int step = 0; step < nsteps; ++step) {
@@ -1141,8 +1130,33 @@ extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nstep
     }
   }
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(c->d2h));
-  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_offload_steps(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
+  if (c) c->press_valid = false;  // the state changes
+  NvtxRange nv("offload steps");
+  if (!c || !ur || !ui || nsteps < 0) return SGPU_E_PARAM;
+  if (sharded(c)) return SGPU_E_STATE;
+  if (!c->h2d) {
+    CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+    for (int k = 0; k < 7; ++k) {
+      CK(cudaEventCreateWithFlags(&c->up_done[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->out_ready[k], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->down_done[k], cudaEventDisableTiming));
+    }
+  }
+  const int r = offload_enqueue(c, ur, ui, nsteps);
+  // returns only when no copy of the caller's arrays is in flight, on success
+  // and on every error path
+  const cudaError_t e1 = cudaStreamSynchronize(c->h2d);
+  const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  const cudaError_t e3 = cudaStreamSynchronize(c->d2h);
+  if (r) return r;
+  CK(e1);
+  CK(e2);
+  CK(e3);
   return SGPU_OK;
 }
 

@@ -22,7 +22,7 @@ def test_header_declares_the_step_and_its_neighbours():
     for must in ("sgpu_init", "sgpu_prhs", "sgpu_nonlin", "sgpu_linear", "sgpu_step_rk", "sgpu_upload_state",
                  "sgpu_download_state", "sgpu_amplitudes", "sgpu_xys_sample", "sgpu_set_les", "sgpu_set_shard",
                  "sgpu_copy_block", "sgpu_offload_steps", "sgpu_pressure", "sgpu_box_filter_sample",
-                 "sgpu_xys_get", "sgpu_xys_reset", "sgpu_finalize"):
+                 "sgpu_xys_get", "sgpu_xys_reset", "sgpu_finalize", "sgpu_nonlin_noalloc"):
         assert must in names
 
 
@@ -80,6 +80,26 @@ def test_entry_points_reject_a_null_context():
     assert lib.sgpu_finalize(None) == 0
     for rc in (0, -1, -2, -3, -4, -5):
         assert lib.sgpu_error_string(rc)
+
+
+def test_nonlin_noalloc_rejects_invalid_arguments():
+    """The allocation-free step 2 checks its arguments before it touches the
+    device: null pointers, an invalid grid and a precision other than FP64
+    (its arrays are complex doubles) come back as SGPU_E_PARAM."""
+    from simson_b200.bla import SgpuParams
+    lib = _lib()
+    lib.sgpu_nonlin_noalloc.argtypes = [ctypes.POINTER(SgpuParams), ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    good = dict(nx=48, ny=65, nz=48, re=4200.0, xl=12.566, zl=6.283, dt=0.01, nst=3, cflux=1, mflux=4.0 / 3.0,
+                px=-2.0 / 4200.0, rot=0.0, icfl=3, precision=0, device=0)
+    buf = ctypes.c_void_p(16)  # never dereferenced: every case below is rejected first
+    p = SgpuParams(**good)
+    assert lib.sgpu_nonlin_noalloc(None, buf, buf, None, None) == SGPU_E_PARAM
+    assert lib.sgpu_nonlin_noalloc(ctypes.byref(p), None, buf, None, None) == SGPU_E_PARAM
+    assert lib.sgpu_nonlin_noalloc(ctypes.byref(p), buf, None, None, None) == SGPU_E_PARAM
+    for change in (dict(nx=46), dict(nx=0), dict(ny=64), dict(ny=7), dict(nz=47), dict(xl=0.0), dict(precision=1)):
+        q = SgpuParams(**{**good, **change})
+        assert lib.sgpu_nonlin_noalloc(ctypes.byref(q), buf, buf, None, None) == SGPU_E_PARAM, change
 
 
 @pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
