@@ -215,32 +215,60 @@ def own_arm(args, rank, world, precision):
                 press_ms=press_ms)
 
 
-LES_WORKLOAD = dict(nx=64, ny=97, nz=64, re=4200.0, xl=2 * np.pi, zl=np.pi, dt=0.005, rms=0.1, seed=4)
+LES_WORKLOAD = dict(nx=64, ny=97, nz=64, re=9000.0, xl=2 * np.pi, zl=np.pi, dt=0.005, rms=0.1, seed=3)
+LEARNED_WEIGHTS = os.path.join(ROOT, "tests", "golden", "learned_sgs_re395.npz")
+
+
+def learned_model():
+    """The learned SGS network trained on the DNS of the Re_tau ~ 395 channel
+    (tests/golden/make_learned_sgs.py): (weights, (s_in, s_y, s_out), label);
+    without that file, the eddy-viscosity weight set of oracle/sgs_mlp.py
+    (the same network size and cost)."""
+    if os.path.exists(LEARNED_WEIGHTS):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from sgs_mlp import mlp_unpack
+        g = np.load(LEARNED_WEIGHTS)
+        w = {k: v.astype(np.float32) for k, v in mlp_unpack(g["params"]).items()}
+        return w, (float(g["s_in"]), float(g["s_y"]), float(g["s_out"])), "trained on the Re_tau~395 DNS"
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from sgs_mlp import viscosity_weights
+    return viscosity_weights(1e-5), (0.2, 1.0, 1.0), "eddy-viscosity weight set"
+
+
+def setup_les(ch, model):
+    if model == "adm":
+        ch.set_les(iles=1)
+    elif model == "dyn":
+        ch.set_les(iles=2)
+    elif model in ("mlp", "mlp_fb"):
+        w, (s_in, s_y, s_out), _ = learned_model()
+        ch.set_sgs_mlp(w, s_in=s_in, s_y=s_y, s_out=s_out)
+        if model == "mlp_fb":
+            ch.set_sgs_fallback(bound=0.0, cs=0.0, ineg=1)
 
 
 def les_arm(steps, warmup):
-    """RK3 steps/s of the LES configuration 64x97x64 with each SGS model
-    (reported beside the headline; ADM-RT, dynamic Smagorinsky and the learned
-    model as the reference's sgs.i defaults / a fixed weight set)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from sgs_mlp import viscosity_weights
+    """RK3 steps/s of the LES configuration 64x97x64 (Re_cl 9000, the box of
+    the 384x193x384 workload) with each SGS model: ADM-RT and dynamic
+    Smagorinsky with the reference's sgs.i defaults, the learned model alone
+    and with its per-plane fallback to dynamic Smagorinsky."""
     from simson_b200.bla import Channel, FP64, MIXED
     from simson_b200.fields import channel_field
     w = LES_WORKLOAD
-    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"], kmax=30)
+    u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"])
     out = {}
     variants = [("no_model_fp64", FP64, None), ("adm_rt_fp64", FP64, "adm"), ("dyn_smagorinsky_fp64", FP64, "dyn"),
-                ("learned_mlp_fp64", FP64, "mlp"), ("learned_mlp_mixed", MIXED, "mlp"), ("no_model_mixed", MIXED, None)]
+                ("learned_mlp_fp64", FP64, "mlp"), ("learned_mlp_fallback_fp64", FP64, "mlp_fb"),
+                ("dyn_smagorinsky_mixed", MIXED, "dyn"), ("learned_mlp_mixed", MIXED, "mlp"),
+                ("learned_mlp_fallback_mixed", MIXED, "mlp_fb"), ("no_model_mixed", MIXED, None)]
     for tag, prec, model in variants:
         ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], precision=prec)
-        if model == "adm":
-            ch.set_les(iles=1)
-        elif model == "dyn":
-            ch.set_les(iles=2)
         ch.set_velocity(u, v, wv)
+        if model == "adm":
+            setup_les(ch, model)  # before prhs: it filters the start-up velocities
         ch.prhs()
-        if model == "mlp":
-            ch.set_sgs_mlp(viscosity_weights(1e-5), s_in=0.2)
+        if model != "adm":
+            setup_les(ch, model)
         for _ in range(warmup):
             ch.step(1)
         ch.sync()
@@ -250,9 +278,14 @@ def les_arm(steps, warmup):
         ms = ch.elapsed_ms(0, 1)
         out[tag] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps}
         ch.close()
-    return {"workload": "temporal channel 64x97x64, 2pi x 2 x pi, Re_cl 4200, dt 0.005, seeded rms 0.1 "
-                        "broadband perturbation (the LES configuration)", "steps": steps, "warmup": warmup,
-            "variants": out}
+    v = out
+    ratio = {k: v[k]["steps_per_s"] / v["dyn_smagorinsky_fp64"]["steps_per_s"]
+             for k in ("learned_mlp_fp64", "learned_mlp_fallback_fp64", "learned_mlp_mixed",
+                       "learned_mlp_fallback_mixed")}
+    return {"workload": "temporal channel 64x97x64, 2pi x 2 x pi, Re_cl 9000, dt 0.005, the seeded rms 0.1 "
+                        "field of the DNS workload (the learned-LES configuration)", "steps": steps,
+            "warmup": warmup, "learned_weights": learned_model()[2], "variants": out,
+            "learned_over_dyn_smagorinsky_fp64": ratio}
 
 
 def shard_arm(args, rank, world, precision):
@@ -330,17 +363,22 @@ def cpu_reference(steps, threads, sample_note, warmup_substeps=1):
                        f"'Wall time' lines cannot be used), {threads} threads")
 
 
-def profile_case(grid, substeps, precision):
+def profile_case(grid, substeps, precision, les=None):
     """A few substeps of the channel step on one grid, for profiler captures
     (ncu -k ... -s ... python bench.py --case GRID): prints the per-kernel
-    milliseconds of the last substep (CUDA events)."""
+    milliseconds of the last substep (CUDA events).  les: an SGS model
+    (adm, dyn, mlp, mlp_fb) on the box and Re of the LES configuration."""
     from simson_b200.bla import FP64, MIXED, Channel
     from simson_b200.fields import channel_field
     nx, ny, nz = (int(v) for v in grid.split("x"))
-    xl, zl = 4 * np.pi, 2 * np.pi
-    ch = Channel(nx, ny, nz, 4200.0, xl, zl, 0.005, precision=MIXED if precision == "mixed" else FP64)
+    xl, zl, re = (4 * np.pi, 2 * np.pi, 4200.0) if not les else (2 * np.pi, np.pi, 9000.0)
+    ch = Channel(nx, ny, nz, re, xl, zl, 0.005, precision=MIXED if precision == "mixed" else FP64)
     ch.set_velocity(*channel_field(nx, ny, nz, xl, zl, 0.1, 2))
+    if les == "adm":
+        setup_les(ch, les)
     ch.prhs()
+    if les and les != "adm":
+        setup_les(ch, les)
     ch.substeps(substeps)
     ch.profile(True)
     ch.substeps(1)
@@ -362,12 +400,14 @@ def main():
                     help="profiling case: run --substeps substeps on this grid and print per-kernel times "
                          "(no JSON line; for ncu captures)")
     ap.add_argument("--substeps", type=int, default=3)
+    ap.add_argument("--les", default=None, choices=["adm", "dyn", "mlp", "mlp_fb"],
+                    help="profiling case: SGS model")
     ap.add_argument("--shard", action="store_true",
                     help="one channel split over the ranks (z-slab shards, NCCL all-to-alls; strong scaling) "
                          "instead of one replica per rank")
     args = ap.parse_args()
     if args.case:
-        profile_case(args.case, args.substeps, "mixed" if args.precision == "mixed" else "fp64")
+        profile_case(args.case, args.substeps, "mixed" if args.precision == "mixed" else "fp64", args.les)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

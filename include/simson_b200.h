@@ -31,6 +31,7 @@ extern "C" {
 #define SGPU_E_STATE (-3)      /* call out of order (no state uploaded)    */
 #define SGPU_E_CFL (-4)        /* CFL*dt > 10: the reference stops (wcflbl.f:93) */
 #define SGPU_E_NAN (-5)        /* non-finite value detected in the state   */
+#define SGPU_E_TIMEOUT (-6)    /* a bounded device wait ran out (a lost completion) */
 
 #define SGPU_FP64 0            /* every transform and solve in FP64 */
 #define SGPU_MIXED 1           /* FP32 x/z FFTs, products, Chebyshev transforms and u,v,w,omega
@@ -87,8 +88,10 @@ int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
  * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises.
  * Returns SGPU_E_CFL when CFL*dt > 10 (the reference's stop, wcflbl.f:93)
  * and SGPU_E_NAN when px or the mass flux is not finite (a non-finite value
- * anywhere in u, v, w reaches them within one substep); the driver calls it
- * after each step it checks, as the reference checks every icfl substeps. */
+ * anywhere in u, v, w reaches them within one substep), SGPU_E_TIMEOUT when a
+ * bounded wait of a tensor-core kernel ran out since the last call (see
+ * sgpu_set_wait_limit); the driver calls it after each step it checks, as
+ * the reference checks every icfl substeps. */
 int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
 /* Large-eddy model, the reference's sgs.i (bla/rparamles.f:31-60):
@@ -146,6 +149,24 @@ typedef struct {
 /* Enables the learned model for the following substeps (replaces any LES
  * model set with sgpu_set_les).  Needs nx, nz divisible by 4. */
 int sgpu_set_sgs_mlp(sgpu_ctx* ctx, const sgpu_sgs_mlp* p);
+
+/* Per-plane fallback of the learned model to the eddy-viscosity model (no
+ * counterpart in the reference; the plain model is bla/les.f's, dynamic when
+ * cs = 0, clipping ineg as in sgpu_les_params).  enable = 1: every substep,
+ * after the network's stress, each xz-plane y sums P = tau_ij S_ij and |P|
+ * over its points (tau the network's stress, S_ij the resolved strain rate;
+ * P > 0 is backscatter, energy from the subgrid to the resolved scales) and
+ * takes the eddy-viscosity stress instead when sum P > bound * sum |P|
+ * (bound 1: never; bound below -1: always; 0: on net backscatter).  The
+ * eddy-viscosity model runs on the switched planes only.  enable = 0: off.
+ * Call after sgpu_set_sgs_mlp. */
+int sgpu_set_sgs_fallback(sgpu_ctx* ctx, int enable, double bound, double cs, int ineg);
+
+/* The plane switches of the last substep: planes[ny] (1 = eddy-viscosity
+ * stress), and, if sums is not NULL, sums[2*ny] = (sum P, sum |P|) per plane.
+ * Synchronises the library's stream.  SGPU_E_STATE before the fallback was
+ * enabled once. */
+int sgpu_sgs_fallback_planes(sgpu_ctx* ctx, int* planes, double* sums);
 
 /* Training of the learned SGS model (no counterpart in the reference):
  * iters full-batch Adam steps (beta1 0.9, beta2 0.999, eps 1e-8, learning
@@ -254,6 +275,39 @@ int sgpu_set_shard(sgpu_ctx* ctx, int ylo, int yhi, int zlo, int zhi);
  * Synchronises. */
 int sgpu_copy_block(sgpu_ctx* ctx, int slot0, int nslots, int ylo, int yhi, int zlo, int zhi, void* buf,
                     int to_state, size_t* bytes);
+/* OR'ed into sgpu_copy_block's to_state: only enqueue the copy on the
+ * library's stream (sgpu_stream), without synchronising; the transport of the
+ * blocks (e.g. NCCL) is then ordered on the same stream. */
+#define SGPU_BLOCK_NOSYNC 2
+
+/* The library's CUDA stream (a cudaStream_t), for work that a host orders
+ * with the step's kernels. */
+int sgpu_stream(sgpu_ctx* ctx, void** stream);
+
+/* Sharded runs: the CFL number needs the maximum over all shards, as the
+ * reference all-reduces it over its MPI ranks (bla/wcflbl.f:82-85) before its
+ * stop test (:93).  On a shard, sgpu_nonlin and sgpu_get_scalars leave that
+ * test to the host: sgpu_cfl_partial gives this shard's partial maximum
+ * max(|u|/dx + |v|/dy + |w|/dz) of the last substep that evaluated it and
+ * *pending = 1 if it has not been reduced yet (then it synchronises; with
+ * *pending = 0 it returns 0 at once);
+ * sgpu_cfl_set_global takes the maximum over the shards, forms CFL*dt
+ * (bla/wcflbl.f:87) and returns SGPU_E_CFL (above 10) or SGPU_E_NAN. */
+int sgpu_cfl_partial(sgpu_ctx* ctx, double* cflp, int* pending);
+int sgpu_cfl_set_global(sgpu_ctx* ctx, double cflp);
+
+/* Failure detection of the tensor-core kernels (the mixed path's Chebyshev
+ * transforms and the learned SGS model): every wait of theirs on an mbarrier
+ * is bounded.  limit: iterations of each wait in their main loops (0: the
+ * default, 2^20); a wait that runs out makes the kernel let its own copies
+ * and MMAs in flight finish (with the default limit), free its tensor memory
+ * and return, and the next sgpu_get_scalars (or sgpu_sgs_mlp_eval) returns
+ * SGPU_E_TIMEOUT once; the state of that substep is not valid (upload it
+ * again).  test_timeout = 1 makes the first wait of every such launch wait on
+ * a barrier that nothing completes, so that the timeout path can be tested
+ * without a fault; 0 turns that off.  The reference has no counterpart (its
+ * stopnow codes, bla/stopnow.f, stop the run). */
+int sgpu_set_wait_limit(sgpu_ctx* ctx, int limit, int test_timeout);
 
 /* Stream-ordered timing on the library's stream: record event slot (0..15),
  * elapsed milliseconds between two recorded slots (synchronises on b). */

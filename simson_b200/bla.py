@@ -51,7 +51,11 @@ class SgpuSgsMlp(ctypes.Structure):
 
 
 class SimsonError(RuntimeError):
-    pass
+    """A non-zero status of the C ABI; .code holds the SGPU_E_* value."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 _LIB = None
@@ -103,6 +107,12 @@ def load_library(build: bool = True):
     fp = ctypes.POINTER(ctypes.c_float)
     lib.sgpu_set_sgs_mlp.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp)]
     lib.sgpu_sgs_mlp_eval.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp), fp, fp, ctypes.c_longlong]
+    lib.sgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.sgpu_set_wait_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.sgpu_cfl_partial.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
+    lib.sgpu_cfl_set_global.argtypes = [vp, ctypes.c_double]
+    lib.sgpu_set_sgs_fallback.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    lib.sgpu_sgs_fallback_planes.argtypes = [vp, ctypes.POINTER(ctypes.c_int), dp]
     lib.sgpu_offload_steps.argtypes = [vp, dp, dp, ctypes.c_int]
     lib.sgpu_set_shard.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.sgpu_copy_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -139,7 +149,7 @@ class Channel:
 
     def _check(self, rc, what):
         if rc != 0:
-            raise SimsonError(f"{what}: {self.lib.sgpu_error_string(rc).decode()} ({rc})")
+            raise SimsonError(f"{what}: {self.lib.sgpu_error_string(rc).decode()} ({rc})", rc)
 
     def close(self):
         if getattr(self, "_ctx", None):
@@ -193,16 +203,42 @@ class Channel:
         (bla/par.f:102 z-slabs; simson_b200.shard moves the blocks)."""
         self._check(self.lib.sgpu_set_shard(self._ctx, ylo, yhi, zlo, zhi), "set_shard")
 
-    def copy_block(self, slot0, nslots, ylo, yhi, zlo, zhi, buf_ptr=None, to_state=False):
+    def copy_block(self, slot0, nslots, ylo, yhi, zlo, zhi, buf_ptr=None, to_state=False, nosync=False):
         """Pack (to_state=False) or unpack a block of state slots between the
         state and the device buffer at buf_ptr ([slot][y][kz][kx], the
         state's storage); returns its size in bytes (buf_ptr None: size
-        only)."""
+        only).  nosync: only enqueue the copy on the library's stream."""
         n = ctypes.c_size_t(0)
+        flag = int(to_state) | (2 if nosync else 0)
         self._check(self.lib.sgpu_copy_block(self._ctx, slot0, nslots, ylo, yhi, zlo, zhi,
-                                             ctypes.c_void_p(buf_ptr) if buf_ptr else None, int(to_state),
+                                             ctypes.c_void_p(buf_ptr) if buf_ptr else None, flag,
                                              ctypes.byref(n)), "copy_block")
         return n.value
+
+    def set_wait_limit(self, limit=0, test_timeout=False):
+        """Bounded waits of the tensor-core kernels: iterations per wait
+        (0: default); test_timeout makes each launch's first wait run out
+        (sgpu_set_wait_limit)."""
+        self._check(self.lib.sgpu_set_wait_limit(self._ctx, int(limit), int(bool(test_timeout))), "set_wait_limit")
+
+    def stream_ptr(self):
+        """The library's CUDA stream (cudaStream_t) as an integer."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.sgpu_stream(self._ctx, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    def cfl_partial(self):
+        """(partial CFL maximum of this shard's planes, pending) -- see
+        sgpu_cfl_partial."""
+        m = ctypes.c_double()
+        p = ctypes.c_int()
+        self._check(self.lib.sgpu_cfl_partial(self._ctx, ctypes.byref(m), ctypes.byref(p)), "cfl_partial")
+        return m.value, bool(p.value)
+
+    def cfl_set_global(self, cflp):
+        """The all-reduced partial maximum: the reference's stop test (raises
+        SimsonError on CFL*dt > 10 or a non-finite value)."""
+        self._check(self.lib.sgpu_cfl_set_global(self._ctx, float(cflp)), "cfl")
 
     def prhs(self):
         self._check(self.lib.sgpu_prhs(self._ctx), "prhs")
@@ -288,6 +324,22 @@ class Channel:
         """Learned SGS model: weights dict w1 (64,10), b1 (64), w2 (64,64), b2, w3 (6,64), b3 (6)."""
         st, keep = self._mlp_struct(weights, s_in, s_y, s_out)
         self._check(self.lib.sgpu_set_sgs_mlp(self._ctx, ctypes.byref(st)), "set_sgs_mlp")
+
+    def set_sgs_fallback(self, bound=0.0, cs=0.0, ineg=1, enable=True):
+        """Per-plane switch of the learned model to the eddy-viscosity model
+        (dynamic when cs = 0) on planes where sum tau_ij S_ij > bound * sum
+        |tau_ij S_ij| (predicted backscatter)."""
+        self._check(self.lib.sgpu_set_sgs_fallback(self._ctx, int(bool(enable)), float(bound), float(cs), int(ineg)),
+                    "set_sgs_fallback")
+
+    def sgs_fallback_planes(self):
+        """(planes (ny,) int: 1 where the last substep used the eddy-viscosity
+        stress, sums (ny, 2): sum tau_ij S_ij and sum |tau_ij S_ij| per plane)."""
+        planes = np.zeros(self.ny, np.int32)
+        sums = np.zeros((self.ny, 2))
+        self._check(self.lib.sgpu_sgs_fallback_planes(self._ctx, planes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                      _dp(sums)), "sgs_fallback_planes")
+        return planes, sums
 
     def sgs_mlp_eval(self, weights, x, s_in=1.0, s_y=1.0, s_out=1.0):
         """The tensor-core MLP on feature rows x (n, 10) -> (n, 6)."""

@@ -112,6 +112,8 @@ struct ChebTCArgs {
   const unsigned char* mat;      // ne + no chunks in the order e0 o0 e1 o1 ..., each (hi, lo) tiles
   int skip_oddball, nx2, zodd;   // inverse of step 3: leave the kz = -nz/2 plane alone
   int* err;
+  int wait_limit;                // iterations of each bounded wait of the main loop (<= 0: MLP_WAIT_LIMIT)
+  int test_timeout;              // 1: the MMA thread first waits on a barrier nothing completes
 };
 
 __device__ __forceinline__ void chb_bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned mbar) {
@@ -233,6 +235,7 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
   auto dpar = [](int q) { return (unsigned)((q >> 1) & 1); };
   int issued = 0, consumed = 0;  // MMA thread: matrix copies issued / waited for
   const bool mma_thread = t == CHB_PRODUCERS;
+  const int limit = a.wait_limit > 0 ? a.wait_limit : MLP_WAIT_LIMIT;
   if (mma_thread) {
     const unsigned idesc_e = chb_idesc(CHB_TILE, a.nre), idesc_o = chb_idesc(CHB_TILE, a.nro);
     auto issue_matrix = [&](int q) {
@@ -242,15 +245,18 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
     };
     issue_matrix(0);
     if (nch > 1) issue_matrix(1);
-    for (int q = 0; q < nch; ++q) {
+    // test of the timeout path: accb completes only with the commit after
+    // the loop, so this wait runs out as a lost completion would
+    if (a.test_timeout && !mlp_wait(accb, 0u, limit)) s_fail = 1;
+    for (int q = 0; q < nch && !s_fail; ++q) {
       const int ms = q % CHB_MSTAGES, ds = q & 1;
       const bool odd = chb_is_odd(q, no);
-      if (!mlp_wait(mfull0 + 8 * ms, mpar(q), MLP_WAIT_LIMIT)) {
+      if (!mlp_wait(mfull0 + 8 * ms, mpar(q), limit)) {
         s_fail = 1;
         break;
       }
       consumed = q + 1;
-      if (!mlp_wait(dfull0 + 8 * ds, dpar(q), MLP_WAIT_LIMIT)) {
+      if (!mlp_wait(dfull0 + 8 * ds, dpar(q), limit)) {
         s_fail = 1;
         break;
       }
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
       mlp_commit(mempty0 + 8 * ms);
       if (q + 2 < nch) {
         // matrix stage of chunk q+2 was last read by chunk q-1
-        if (q >= 1 && !mlp_wait(mempty0 + 8 * ((q - 1) % CHB_MSTAGES), mpar(q - 1), MLP_WAIT_LIMIT)) {
+        if (q >= 1 && !mlp_wait(mempty0 + 8 * ((q - 1) % CHB_MSTAGES), mpar(q - 1), limit)) {
           s_fail = 1;
           break;
         }
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(CHB_THREADS, 2) k_cheb_tc(ChebTCArgs a) {
         if (odd && i >= no) break;
         const int q = 2 * i + odd;
         // the stage was last read by chunk q-2
-        if (q >= 2 && !mlp_wait(dempty0 + 8 * odd, dpar(q - 2), MLP_WAIT_LIMIT)) return false;
+        if (q >= 2 && !mlp_wait(dempty0 + 8 * odd, dpar(q - 2), limit)) return false;
         chb_store_tile(a, p, odd, i, pt, Dhi(odd), Dlo(odd));
         async_proxy_fence();
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(dfull0 + 8 * odd) : "memory");

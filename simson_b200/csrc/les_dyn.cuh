@@ -23,6 +23,9 @@
 //                (les.f:1385-1480, ineg = 1 clipping, zero at the walls)
 //   k_sgs_tau_x  tau_ij / (nx nz) (les.f:1489-1560), forward x FFT
 //   k_sgs_zfwd   forward z FFT, oddball zeroed: tau in the state layout
+//   k_sgs_backscatter (learned model) per plane: the plane sums of
+//                tau_ij S_ij and |tau_ij S_ij| of the network's stress, and
+//                the plane's switch to the eddy-viscosity model
 //   k_sgs_sigma  per pencil, on Chebyshev coefficients of tau:
 //                sigma_i = i alpha tau_i1 + i beta tau_i3 + D tau_i2
 //                (bla/sgs_stress.f)
@@ -43,7 +46,16 @@ struct SgsBufs {
   double* cxy;      // [nyp][nx]            C(x, y)
   double2* tauz6;   // [6][nyp][nz][nx/2]   tau, z physical, x spectral
   double2* tau;     // [6][nyp][NP]         tau, state layout
+  // learned model with the per-plane fallback: planes y with plane_on[y] != 0
+  // take the eddy-viscosity stress, the others the network's; the
+  // eddy-viscosity kernels skip the other planes.  nullptr: every plane
+  // (the plain eddy-viscosity model).
+  const int* plane_on;
 };
+
+__device__ __forceinline__ bool sgs_plane_off(const SgsBufs& B, int y) {
+  return B.plane_on != nullptr && B.plane_on[y] == 0;
+}
 
 struct SgsGrid {
   int nx, nz, nx2, nx4, nyp, NP, zodd;
@@ -116,6 +128,7 @@ __global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPl
   double2* b0 = reinterpret_cast<double2*>(smem_raw);
   double2* b1 = b0 + (size_t)G.nz * KB;
   const int y = blockIdx.y;
+  if (set == 0 && sgs_plane_off(B, y)) return;
   const int kx0 = blockIdx.x * KB;
   const size_t slot = (size_t)G.nyp * G.NP;
   for (int f = 0; f < 9; ++f) {
@@ -167,6 +180,7 @@ __global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
   double2* bA = reinterpret_cast<double2*>(smem_raw);
   double2* bB = bA + (size_t)G.nx * NC;
   const int m = blockIdx.x, y = blockIdx.y;
+  if (sgs_plane_off(B, y)) return;
   const int n = G.nx;
   const size_t fs9 = (size_t)G.nyp * G.nz * G.nx2;
   const size_t row = ((size_t)y * G.nz + m) * G.nx2;
@@ -264,6 +278,7 @@ __global__ void k_sgs_zfilt(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
   double2* b0 = reinterpret_cast<double2*>(smem_raw);
   double2* b1 = b0 + (size_t)G.nz * KB;
   const int y = blockIdx.y;
+  if (sgs_plane_off(B, y)) return;
   const int kx0 = blockIdx.x * KB;
   const size_t fs21 = (size_t)G.nyp * G.nz * G.nx4;
   const int zlo = G.nz / 4 + 1, zhi = G.nz - G.nz / 4 - 1;
@@ -301,6 +316,7 @@ __global__ void k_sgs_xpass2(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
   double2* bA = reinterpret_cast<double2*>(smem_raw);
   double2* bB = bA + (size_t)G.nx * NC;
   const int m = blockIdx.x, y = blockIdx.y;
+  if (sgs_plane_off(B, y)) return;
   const int n = G.nx;
   const size_t fs21 = (size_t)G.nyp * G.nz * G.nx4;
   const size_t frow = ((size_t)y * G.nz + m) * G.nx4;
@@ -350,7 +366,7 @@ __global__ void k_sgs_xpass2(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
 __global__ void k_sgs_coef(SgsBufs B, SgsGrid G, double cs, int ineg) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
-  if (x >= G.nx) return;
+  if (x >= G.nx || sgs_plane_off(B, y)) return;
   double c;
   if (cs != 0.0) {
     c = cs * cs;
@@ -376,7 +392,8 @@ __global__ void k_sgs_coef(SgsBufs B, SgsGrid G, double cs, int ineg) {
 // tau_ij / (nx nz) = -2 C Delta^2 |S| S_ij / (nx nz) in physical space, then
 // the forward x FFT (three complex FFTs for the six real rows).
 // tau_phys != nullptr: the stress is given in physical space ([6][nyp*nz*nx],
-// the learned model) instead of -2 C Delta^2 |S| S_ij.
+// the learned model) instead of -2 C Delta^2 |S| S_ij, except on the planes
+// that B.plane_on switches to the eddy-viscosity model.
 __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
                             const double* __restrict__ delta2, double re, int ineg,
                             const double* __restrict__ tau_phys) {
@@ -389,9 +406,10 @@ __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
   const size_t prow = ((size_t)y * G.nz + m) * G.nx;
   const double gd2 = 1. / (double)(G.nx * G.nz);
   const double d2 = delta2[y];
+  const bool learned = tau_phys != nullptr && (B.plane_on == nullptr || B.plane_on[y] == 0);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     double t[6];
-    if (tau_phys != nullptr) {
+    if (learned) {
       for (int l = 0; l < 6; ++l) t[l] = tau_phys[(size_t)l * fs10 + prow + j] * gd2;
     } else {
       double dr = B.cxy[(size_t)y * G.nx + j] * B.phys10[9 * fs10 + prow + j] * d2;
@@ -411,6 +429,60 @@ __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
     const double2 b = res[((n - k) % n) * 3 + c];
     B.tauz6[(size_t)(2 * c) * fs + row + k] = double2{(a.x + b.x) * .5, (a.y - b.y) * .5};
     B.tauz6[(size_t)(2 * c + 1) * fs + row + k] = double2{(a.y + b.y) * .5, (b.x - a.x) * .5};
+  }
+}
+
+// Per-plane switch of the learned model (no counterpart in the reference):
+// one CTA per plane y sums, in a fixed order, P = tau_ij S_ij and
+// |tau_ij S_ij| over the plane's nz x nx points (tau the network's physical
+// stress, S_ij = (du_i/dx_j + du_j/dx_i) / 2 from the nine gradients in
+// phys10 fields 0-8).  P > 0 is backscatter (energy from the SGS to the
+// resolved scales, the SGS dissipation -tau_ij S_ij being negative).  The
+// plane switches to the eddy-viscosity model when sum P > bound * sum |P|
+// (bound in [-1, 1]: 1 never, below -1 always).  sums[2 y], sums[2 y + 1]
+// keep the two sums for diagnostics.
+__global__ void __launch_bounds__(256) k_sgs_backscatter(SgsBufs B, SgsGrid G, const double* __restrict__ tau,
+                                                         double bound, int* __restrict__ plane_on,
+                                                         double* __restrict__ sums) {
+  const int y = blockIdx.x;
+  const size_t plane = (size_t)G.nz * G.nx;
+  const size_t fs = (size_t)G.nyp * plane;
+  const size_t o0 = (size_t)y * plane;
+  double p = 0.0, pa = 0.0;
+  for (size_t i = threadIdx.x; i < plane; i += blockDim.x) {
+    const size_t o = o0 + i;
+    double g[9], t[6];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = B.phys10[(size_t)k * fs + o];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) t[k] = tau[(size_t)k * fs + o];
+    const double s11 = g[0], s22 = g[4], s33 = g[8];
+    const double s12 = .5 * (g[1] + g[3]), s13 = .5 * (g[2] + g[6]), s23 = .5 * (g[5] + g[7]);
+    const double q = t[0] * s11 + t[3] * s22 + t[5] * s33 + 2. * (t[1] * s12 + t[2] * s13 + t[4] * s23);
+    p += q;
+    pa += fabs(q);
+  }
+  // fixed-order reduction: warps by shuffles, then warp 0 over the warps
+  __shared__ double rp[8], ra[8];
+  for (int d = 16; d > 0; d >>= 1) {
+    p += __shfl_down_sync(0xffffffffu, p, d);
+    pa += __shfl_down_sync(0xffffffffu, pa, d);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    rp[warp] = p;
+    ra[warp] = pa;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sp = 0.0, sa = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      sp += rp[w];
+      sa += ra[w];
+    }
+    plane_on[y] = (sp > bound * sa) ? 1 : 0;
+    sums[2 * y] = sp;
+    sums[2 * y + 1] = sa;
   }
 }
 

@@ -57,6 +57,8 @@ struct MlpArgs {
   int nyp;
   float s_in, s_y, s_out;
   int* err;                    // set to 1 if a wait ran out
+  int wait_limit;              // iterations of each bounded wait of the main loop (<= 0: MLP_WAIT_LIMIT)
+  int test_timeout;            // 1: first wait on a barrier nothing completes (tests the timeout path)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -182,6 +184,15 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
   unsigned phase = 0;
   bool fail = false;
 
+  const int limit = a.wait_limit > 0 ? a.wait_limit : MLP_WAIT_LIMIT;
+  bool mma_pending = false;  // an MMA committed whose completion nobody has seen
+  if (a.test_timeout) {
+    // the barrier's phase 0 completes only with a commit, and none is made
+    // before this wait: it runs out, as a lost completion would
+    if (!mlp_wait(mb, phase, limit)) s_fail = 1;
+    __syncthreads();
+    fail = s_fail != 0;
+  }
   const long long ntiles = (a.n + MLP_ROWS - 1) / MLP_ROWS;
   for (long long tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
     const long long i = tile * MLP_ROWS + t;
@@ -213,9 +224,11 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
       mlp_mma(tmem, mlp_desc(smem_u32(A1), 128, 256), mlp_desc(smem_u32(B1), 128, 256), mlp_idesc(128, 64), 0u);
       mlp_commit(mb);
     }
+    mma_pending = true;
     for (int layer = 0; layer < 3; ++layer) {
-      const bool ok = mlp_wait(mb, phase, MLP_WAIT_LIMIT);
+      const bool ok = mlp_wait(mb, phase, limit);
       if (!ok) s_fail = 1;
+      if (ok) mma_pending = false;
       phase ^= 1u;
       tc_fence_after();
       __syncthreads();
@@ -249,6 +262,7 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
                     idn, kc > 0 ? 1u : 0u);
           mlp_commit(mb);
         }
+        mma_pending = true;
       } else {
         // output layer: columns 0..5 of D
         float v[16];
@@ -272,8 +286,8 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
   if (fail) {
     if (t == 0) atomicExch(a.err, 1);
     // let the committed MMA whose wait ran out finish before its accumulator
-    // columns are freed
-    mlp_wait(mb, phase ^ 1u, MLP_WAIT_LIMIT);
+    // columns are freed (the full limit, whatever the main loop's)
+    if (mma_pending) mlp_wait(mb, phase ^ 1u, MLP_WAIT_LIMIT);
   }
   tc_fence_before();
   __syncthreads();

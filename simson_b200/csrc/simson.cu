@@ -101,6 +101,13 @@ struct sgpu_ctx {
   double* mlp_tau = nullptr;  // [6][nyp][nz][nx] physical tau
   int* mlp_err = nullptr;
   float mlp_s_in = 1.f, mlp_s_y = 1.f, mlp_s_out = 1.f;
+  // per-plane fallback of the learned model to the eddy-viscosity model
+  // (sgpu_set_sgs_fallback): plane switches [nyp] and the two backscatter sums
+  // per plane [2 nyp] of the last evaluation
+  bool sgs_fb = false;
+  double sgs_fb_bound = 0.0;
+  int* sgs_flags = nullptr;
+  double* sgs_bsums = nullptr;
   // mixed path: Chebyshev transform matrices for the tensor cores (cheb_tc.cuh)
   unsigned char* chb_fwd = nullptr;  // forward, scale 1/(nxp nzp)
   unsigned char* chb_inv = nullptr;  // inverse
@@ -134,6 +141,9 @@ struct sgpu_ctx {
   static constexpr int kbf = MIXED_KB, rbf = MIXED_RB, pbf = 8;  // FP32 tiles (mixed.h)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
+  // bounded waits of the tensor-core kernels (sgpu_set_wait_limit)
+  int wait_limit = 0;
+  int test_timeout = 0;
   // CUDA graph of one whole RK3 step (sgpu_step_rk), replayed while the step's
   // launch pattern stays the same
   cudaGraphExec_t step_exec = nullptr;
@@ -282,6 +292,7 @@ extern "C" const char* sgpu_error_string(int code) {
     case SGPU_E_STATE: return "call out of order";
     case SGPU_E_CFL: return "CFL*dt above 10";
     case SGPU_E_NAN: return "non-finite state";
+    case SGPU_E_TIMEOUT: return "a bounded device wait ran out";
     default: return "unknown error";
   }
 }
@@ -420,7 +431,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
                   c->sgs.spec9, c->sgs.phys10, c->sgs.filt21, c->sgs.numden, c->sgs.cxy, c->sgs.tauz6, c->sgs.tau,
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
                   c->xys_part, c->xys_u, c->box_out, c->press, c->press_wd, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
-                  c->mlp_err, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
+                  c->mlp_err, c->sgs_flags, c->sgs_bsums, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -547,6 +558,8 @@ static void launch_cheb_tc(sgpu_ctx* c, const float2* in, size_t in_fs, float2* 
   A.nx2 = g.nx2;
   A.zodd = g.zodd;
   A.err = c->chb_err;
+  A.wait_limit = c->wait_limit;
+  A.test_timeout = c->test_timeout;
   dim3 grid((A.ncol + CHB_TILE - 1) / CHB_TILE, nfields);
   k_cheb_tc<<<grid, CHB_THREADS, CHB_SMEM, c->stream>>>(A);
   c->launches++;
@@ -620,6 +633,9 @@ extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int 
                                int to_state, size_t* bytes) {
   if (c) c->press_valid = false;  // may write the state
   if (!c || !bytes) return SGPU_E_PARAM;
+  const bool nosync = (to_state & SGPU_BLOCK_NOSYNC) != 0;
+  to_state &= ~SGPU_BLOCK_NOSYNC;
+  if (to_state != 0 && to_state != 1) return SGPU_E_PARAM;
   const Dims& g = c->g;
   if (slot0 < 0 || nslots < 1 || slot0 + nslots > 7 || ylo < 0 || yhi > g.nyp || ylo >= yhi || zlo < 0 ||
       zhi > g.nz || zlo >= zhi)
@@ -644,7 +660,13 @@ extern "C" int sgpu_copy_block(sgpu_ctx* c, int slot0, int nslots, int ylo, int 
     off += width * height;
   }
   *bytes = off;
-  if (buf) CK(cudaStreamSynchronize(c->stream));
+  if (buf && !nosync) CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_stream(sgpu_ctx* c, void** stream) {
+  if (!c || !stream) return SGPU_E_PARAM;
+  *stream = static_cast<void*>(c->stream);
   return SGPU_OK;
 }
 
@@ -746,13 +768,35 @@ static void enqueue_sgs(sgpu_ctx* c) {
     A.s_y = c->mlp_s_y;
     A.s_out = c->mlp_s_out;
     A.err = c->mlp_err;
+    A.wait_limit = c->wait_limit;
+    A.test_timeout = c->test_timeout;
     const long long tiles = (A.n + MLP_ROWS - 1) / MLP_ROWS;
     const int blocks = (int)std::min<long long>(tiles, 148 * 4);
     k_sgs_mlp<<<blocks, 128, MLP_SMEM_LAUNCH, c->stream>>>(A);
-    k_sgs_tau_x<<<gx, 128, sx3, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, c->prm.re,
+    c->launches += 2;
+    SgsBufs F = c->sgs;
+    if (c->sgs_fb) {
+      // per-plane fallback: planes whose predicted backscatter exceeds the
+      // bound take the eddy-viscosity stress (its kernels skip the others)
+      k_sgs_backscatter<<<g.nyp, 256, 0, c->stream>>>(c->sgs, G, c->mlp_tau, c->sgs_fb_bound, c->sgs_flags,
+                                                       c->sgs_bsums);
+      F.plane_on = c->sgs_flags;
+      if (c->mixed)
+        k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, F, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                           c->beta, 0);
+      else
+        k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, F, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                            c->beta, 0);
+      k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+      k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(F, G, c->sgs_twz.plan, c->sgs_twz.d);
+      k_sgs_xpass2<<<gx, 128, sx11, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+      k_sgs_coef<<<dim3((g.nx + 127) / 128, g.nyp), 128, 0, c->stream>>>(F, G, c->les_cs, c->les_ineg);
+      c->launches += 6;
+    }
+    k_sgs_tau_x<<<gx, 128, sx3, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, c->prm.re,
                                              c->les_ineg, c->mlp_tau);
     k_sgs_zfwd<KB><<<gz, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
-    c->launches += 5;
+    c->launches += 3;
   } else {
   k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
   k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
@@ -940,6 +984,9 @@ static int enqueue_linear(sgpu_ctx* c) {
 
 static int collect_cfl(sgpu_ctx* c) {
   if (!c->cfl_pending) return SGPU_OK;
+  // a shard holds only its planes' partial maximum: the host all-reduces it
+  // (sgpu_cfl_partial, sgpu_cfl_set_global) before the stop test
+  if (sharded(c)) return SGPU_OK;
   unsigned long long bits = 0;
   CK(cudaMemcpyAsync(&bits, c->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -964,6 +1011,30 @@ extern "C" int sgpu_linear(sgpu_ctx* c) {
   if (!c) return SGPU_E_PARAM;
   if (!c->have_state) return SGPU_E_STATE;
   return enqueue_linear(c);
+}
+
+// Sharded runs: the partial maximum of this shard's planes, and the stop
+// test on the all-reduced one (bla/wcflbl.f:82-98 with MPI_Allreduce).  The
+// partial maximum is read only when a substep evaluated it.
+extern "C" int sgpu_cfl_partial(sgpu_ctx* c, double* cflp, int* pending) {
+  if (!c || !cflp || !pending) return SGPU_E_PARAM;
+  *pending = c->cfl_pending ? 1 : 0;
+  *cflp = 0.0;
+  if (!c->cfl_pending) return SGPU_OK;  // nothing to reduce: no wait
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  memcpy(cflp, &bits, sizeof(double));
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_cfl_set_global(sgpu_ctx* c, double cflp) {
+  if (!c) return SGPU_E_PARAM;
+  const double pi = 3.1415926535897932385;
+  c->cfl = (cflp * pi + 2. * fabs(c->prm.rot)) * c->dtn;  // bla/wcflbl.f:87
+  c->cfl_pending = false;
+  if (!(c->cfl <= 10.)) return std::isnan(c->cfl) ? SGPU_E_NAN : SGPU_E_CFL;
+  return SGPU_OK;
 }
 
 // Launch pattern of the RK3 step that starts now: bits 0-2 the substeps that
@@ -1164,21 +1235,36 @@ extern "C" int sgpu_get_scalars(sgpu_ctx* c, double* out, int n) {
   if (!c || !out) return SGPU_E_PARAM;
   int r = collect_cfl(c);
   double sc[4];
-  int tc_err = 0;
+  int tc_err = 0, mlp_err = 0;
   CK(cudaMemcpyAsync(sc, c->scal, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
   if (c->chb_err) CK(cudaMemcpyAsync(&tc_err, c->chb_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (c->mlp_err) CK(cudaMemcpyAsync(&mlp_err, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const double v[12] = {sc[0], sc[1], c->t, c->cfl, c->an, c->bn, c->anp1, c->bnp1, c->cnp1, (double)c->it, c->tc, c->dtn};
   for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
-  if (tc_err) {
-    fprintf(stderr, "simson_b200: tensor-core Chebyshev transform: a wait timed out\n");
-    return SGPU_E_CUDA;
+  if (tc_err || mlp_err) {
+    // reported once: the words are cleared, so a context whose state the
+    // host restores (upload, prhs) steps on normally
+    fprintf(stderr, "simson_b200: %s: a bounded wait ran out; the substep's result is not valid\n",
+            tc_err ? "tensor-core Chebyshev transform" : "learned SGS model");
+    if (c->chb_err) CK(cudaMemsetAsync(c->chb_err, 0, sizeof(int), c->stream));
+    if (c->mlp_err) CK(cudaMemsetAsync(c->mlp_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SGPU_E_TIMEOUT;
   }
   // a non-finite value anywhere in u, v, w reaches the kx = kz = 0 mode of H
   // through the forward transforms within one substep, and with it px
   // (constant flux) or the mass flux
   if (r == SGPU_OK && c->have_state && !(std::isfinite(sc[0]) && std::isfinite(sc[1]))) return SGPU_E_NAN;
   return r;
+}
+
+extern "C" int sgpu_set_wait_limit(sgpu_ctx* c, int limit, int test_timeout) {
+  if (c) c->step_valid = false;  // the limits are kernel arguments of the captured step
+  if (!c || limit < 0 || test_timeout < 0 || test_timeout > 1) return SGPU_E_PARAM;
+  c->wait_limit = limit;
+  c->test_timeout = test_timeout;
+  return SGPU_OK;
 }
 
 extern "C" int sgpu_event_record(sgpu_ctx* c, int slot_) {
@@ -1759,6 +1845,45 @@ extern "C" int sgpu_set_sgs_mlp(sgpu_ctx* c, const sgpu_sgs_mlp* p) {
   return SGPU_OK;
 }
 
+// Per-plane fallback of the learned model (no counterpart in the reference):
+// planes whose predicted backscatter exceeds the bound take the eddy-viscosity
+// stress of bla/les.f (dynamic when cs = 0, clipping ineg) for that substep.
+extern "C" int sgpu_set_sgs_fallback(sgpu_ctx* c, int enable, double bound, double cs, int ineg) {
+  if (c) c->step_valid = false;  // the captured step no longer matches
+  if (!c) return SGPU_E_PARAM;
+  if (!enable) {
+    c->sgs_fb = false;
+    return SGPU_OK;
+  }
+  if (!(bound == bound) || ineg < 0 || ineg > 2 || !(cs >= 0.0) || (cs != 0.0 && ineg != 1)) return SGPU_E_PARAM;
+  int rc = sgs_setup(c);
+  if (rc) return rc;
+  const int n = c->g.nyp;
+  if (!c->sgs_flags) {
+    if (cudaMalloc(&c->sgs_flags, n * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->sgs_bsums, 2 * (size_t)n * sizeof(double)) != cudaSuccess)
+      return SGPU_E_CUDA;
+    CK(cudaMemsetAsync(c->sgs_flags, 0, n * sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->sgs_bsums, 0, 2 * (size_t)n * sizeof(double), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->sgs_fb = true;
+  c->sgs_fb_bound = bound;
+  c->les_cs = cs;
+  c->les_ineg = ineg;
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_sgs_fallback_planes(sgpu_ctx* c, int* planes, double* sums) {
+  if (!c || !planes) return SGPU_E_PARAM;
+  if (!c->sgs_flags) return SGPU_E_STATE;
+  const int n = c->g.nyp;
+  CK(cudaMemcpyAsync(planes, c->sgs_flags, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (sums) CK(cudaMemcpyAsync(sums, c->sgs_bsums, 2 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
 // The MLP alone on n host feature rows x[n][10] -> y[n][6] (the kernel the
 // step uses, features given instead of formed from the velocity gradient).
 extern "C" int sgpu_sgs_mlp_eval(sgpu_ctx* c, const sgpu_sgs_mlp* p, const float* x, float* y, long long n) {
@@ -1782,6 +1907,8 @@ extern "C" int sgpu_sgs_mlp_eval(sgpu_ctx* c, const sgpu_sgs_mlp* p, const float
   A.s_y = p->s_y;
   A.s_out = p->s_out;
   A.err = c->mlp_err;
+  A.wait_limit = c->wait_limit;
+  A.test_timeout = c->test_timeout;
   int err = 0;
   rc = SGPU_OK;
   if (cudaMemcpyAsync(dx, x, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
@@ -1800,7 +1927,7 @@ extern "C" int sgpu_sgs_mlp_eval(sgpu_ctx* c, const sgpu_sgs_mlp* p, const float
   cudaFree(dy);
   if (!rc && err) {
     fprintf(stderr, "simson_b200: sgpu_sgs_mlp_eval: tensor-core wait timed out\n");
-    rc = SGPU_E_CUDA;
+    rc = SGPU_E_TIMEOUT;
   }
   return rc;
 }

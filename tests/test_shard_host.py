@@ -69,6 +69,51 @@ def _rank(rank, world, port, out):
         dist.destroy_process_group()
 
 
+class CflState:
+    """A shard's CFL bookkeeping as the library keeps it (sgpu_cfl_partial,
+    sgpu_cfl_set_global): a local partial maximum, the stop test on the
+    global one (bla/wcflbl.f:87-93, rot = 0)."""
+
+    def __init__(self, partial, dt, pending=True):
+        self.partial, self.dt, self.pending, self.cfl = partial, dt, pending, None
+
+    def cfl_partial(self):
+        return self.partial, self.pending
+
+    def cfl_set_global(self, g):
+        self.pending = False
+        self.cfl = g * np.pi * self.dt
+        if not self.cfl <= 10.0:
+            raise RuntimeError("CFL*dt above 10")
+
+
+def _cfl_rank(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        allreduce_max = shard.torch_allreduce_max("cpu")
+        # every shard below the limit: the stop test passes everywhere with
+        # the largest partial maximum
+        st = CflState(10.0 + rank, 0.01)
+        g = shard.reduce_cfl(st, allreduce_max)
+        ok_max = g == 10.0 + world - 1 and abs(st.cfl - g * np.pi * 0.01) < 1e-15
+        # nothing evaluated this substep: no collective, no test
+        ok_none = shard.reduce_cfl(CflState(1e9, 0.01, pending=False), allreduce_max) is None
+        # only rank 0's planes exceed the limit: every shard stops
+        st = CflState(1e6 if rank == 0 else 1.0, 0.01)
+        try:
+            shard.reduce_cfl(st, allreduce_max)
+            stopped = False
+        except RuntimeError:
+            stopped = True
+        # the ranks are still in step afterwards (the same collectives ran)
+        dist.barrier()
+        out[rank] = int(ok_max) + 2 * int(ok_none) + 4 * int(stopped)
+    finally:
+        dist.destroy_process_group()
+
+
 def free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -98,3 +143,20 @@ def test_block_all_to_alls_gloo(world):
         p.join(120)
         assert p.exitcode == 0
     assert all(out[r] == 3 for r in range(world)), dict(out)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_cfl_all_reduce_gloo(world):
+    """The sharded stop test: the shards' partial CFL maxima are all-reduced
+    before the test, so one shard over the limit stops every shard (the
+    reference all-reduces before wcflbl.f:93)."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = free_port()
+    procs = [ctx.Process(target=_cfl_rank, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert all(out[r] == 7 for r in range(world)), dict(out)
