@@ -441,7 +441,7 @@ __global__ void k_sgs_tau_x(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
 // plane switches to the eddy-viscosity model when sum P > bound * sum |P|
 // (bound in [-1, 1]: 1 never, below -1 always).  sums[2 y], sums[2 y + 1]
 // keep the two sums for diagnostics.
-__global__ void __launch_bounds__(256) k_sgs_backscatter(SgsBufs B, SgsGrid G, const double* __restrict__ tau,
+__global__ void __launch_bounds__(1024) k_sgs_backscatter(SgsBufs B, SgsGrid G, const double* __restrict__ tau,
                                                          double bound, int* __restrict__ plane_on,
                                                          double* __restrict__ sums) {
   const int y = blockIdx.x;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(256) k_sgs_backscatter(SgsBufs B, SgsGrid G, c
     pa += fabs(q);
   }
   // fixed-order reduction: warps by shuffles, then warp 0 over the warps
-  __shared__ double rp[8], ra[8];
+  __shared__ double rp[32], ra[32];
   for (int d = 16; d > 0; d >>= 1) {
     p += __shfl_down_sync(0xffffffffu, p, d);
     pa += __shfl_down_sync(0xffffffffu, pa, d);
@@ -516,42 +516,71 @@ __global__ void k_sgs_zfwd(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __
 }
 
 // sigma_i on Chebyshev coefficients (bla/sgs_stress.f): tc = Chebyshev
-// coefficients of tau [6][nyp][NP], sc = output [3][nyp][NP].
-__global__ void k_sgs_sigma(const double2* __restrict__ tc, double2* __restrict__ sc, SgsGrid G,
-                            const double* __restrict__ alfa, const double* __restrict__ beta) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= G.NP) return;
+// coefficients of tau [6][nyp][NP], sc = output [3][nyp][NP].  One warp per
+// pencil: the x and z derivatives row by row, and D tau_i2 -- the Chebyshev
+// derivative b_j = sum over k > j with k - j odd of 2 k a_k, b_0 halved (the
+// closed form of the bla/dcheb.f recurrence) -- as suffix sums: each lane
+// sums its block of rows by parity, the warp scans the block sums, and each
+// lane walks its rows down from its carry.
+__global__ void __launch_bounds__(128) k_sgs_sigma(const double2* __restrict__ tc, double2* __restrict__ sc,
+                                                   SgsGrid G, const double* __restrict__ alfa,
+                                                   const double* __restrict__ beta) {
+  const int lane = threadIdx.x & 31;
+  const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  if (p >= G.NP) return;  // the whole warp leaves together
   const int kx = p % G.nx2, iz = p / G.nx2;
   const double a = alfa[kx], b = beta[iz];
   const size_t fld = (size_t)G.nyp * G.NP;
+  const int n = G.nyp;
+  const int per = (n + 31) / 32;
+  const int j0 = min(n, lane * per), j1 = min(n, j0 + per);
   // sigma_1 = i a tau11 + i b tau13 + D tau12; sigma_2 = i a tau12 + i b tau23
   // + D tau22; sigma_3 = i a tau13 + i b tau33 + D tau23
   const int cx[3] = {0, 1, 2}, cz[3] = {2, 4, 5}, cy[3] = {1, 3, 4};
   for (int i = 0; i < 3; ++i) {
-    for (int y = 0; y < G.nyp; ++y) {
-      const double2 tx = tc[(size_t)cx[i] * fld + (size_t)y * G.NP + p];
-      const double2 tz = tc[(size_t)cz[i] * fld + (size_t)y * G.NP + p];
-      sc[(size_t)i * fld + (size_t)y * G.NP + p] = double2{-a * tx.y - b * tz.y, a * tx.x + b * tz.x};
+    const double2* ty = tc + (size_t)cy[i] * fld + p;
+    // this lane's block sums of 2 k a_k, k even / k odd
+    double2 se{0.0, 0.0}, so{0.0, 0.0};
+    for (int k = j0; k < j1; ++k) {
+      const double2 v = ty[(size_t)k * G.NP];
+      const double f = 2.0 * (double)k;
+      if (k & 1) {
+        so.x += f * v.x;
+        so.y += f * v.y;
+      } else {
+        se.x += f * v.x;
+        se.y += f * v.y;
+      }
     }
-    // + D tau_i2 (derivative in coefficient space, bla/dcheb.f), real and
-    // imaginary parts as separate columns; the result goes through a scratch
-    // column: the derivative of column cy[i] into sc's spare slot 3
-    double2* dst = const_cast<double2*>(sc) + 3 * fld;
-    cheb_deriv(Col{reinterpret_cast<double*>(dst) + 2 * (size_t)p, 2 * (size_t)G.NP},
-               Col{const_cast<double*>(reinterpret_cast<const double*>(tc + (size_t)cy[i] * fld)) + 2 * (size_t)p,
-                   2 * (size_t)G.NP},
-               G.nyp);
-    cheb_deriv(Col{reinterpret_cast<double*>(dst) + 2 * (size_t)p + 1, 2 * (size_t)G.NP},
-               Col{const_cast<double*>(reinterpret_cast<const double*>(tc + (size_t)cy[i] * fld)) + 2 * (size_t)p + 1,
-                   2 * (size_t)G.NP},
-               G.nyp);
-    for (int y = 0; y < G.nyp; ++y) {
-      const size_t o = (size_t)y * G.NP + p;
-      const double2 d = dst[o];
-      double2 s = sc[(size_t)i * fld + o];
-      s.x = s.x + d.x;
-      s.y = s.y + d.y;
-      sc[(size_t)i * fld + o] = s;
+    // carry = sums over the rows of the lanes above this one
+    double2 ce = se, co = so;  // inclusive suffix sums after the scan
+    for (int d = 1; d < 32; d <<= 1) {
+      const double ex = __shfl_down_sync(0xffffffffu, ce.x, d), ey = __shfl_down_sync(0xffffffffu, ce.y, d);
+      const double ox = __shfl_down_sync(0xffffffffu, co.x, d), oy = __shfl_down_sync(0xffffffffu, co.y, d);
+      if (lane + d < 32) {
+        ce.x += ex;
+        ce.y += ey;
+        co.x += ox;
+        co.y += oy;
+      }
+    }
+    double2 Se{ce.x - se.x, ce.y - se.y}, So{co.x - so.x, co.y - so.y};  // sums over k >= j1
+    for (int j = j1 - 1; j >= j0; --j) {
+      const size_t o = (size_t)j * G.NP + p;
+      const double2 v = ty[(size_t)j * G.NP];
+      double2 d = (j & 1) ? Se : So;  // k > j of the other parity
+      if (j == 0) d = double2{0.5 * d.x, 0.5 * d.y};
+      const double2 tx = tc[(size_t)cx[i] * fld + o];
+      const double2 tz = tc[(size_t)cz[i] * fld + o];
+      sc[(size_t)i * fld + o] = double2{-a * tx.y - b * tz.y + d.x, a * tx.x + b * tz.x + d.y};
+      const double f = 2.0 * (double)j;
+      if (j & 1) {
+        So.x += f * v.x;
+        So.y += f * v.y;
+      } else {
+        Se.x += f * v.x;
+        Se.y += f * v.y;
+      }
     }
   }
 }

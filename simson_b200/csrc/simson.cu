@@ -778,7 +778,7 @@ static void enqueue_sgs(sgpu_ctx* c) {
     if (c->sgs_fb) {
       // per-plane fallback: planes whose predicted backscatter exceeds the
       // bound take the eddy-viscosity stress (its kernels skip the others)
-      k_sgs_backscatter<<<g.nyp, 256, 0, c->stream>>>(c->sgs, G, c->mlp_tau, c->sgs_fb_bound, c->sgs_flags,
+      k_sgs_backscatter<<<g.nyp, 1024, 0, c->stream>>>(c->sgs, G, c->mlp_tau, c->sgs_fb_bound, c->sgs_flags,
                                                        c->sgs_bsums);
       F.plane_on = c->sgs_flags;
       if (c->mixed)
@@ -810,7 +810,8 @@ static void enqueue_sgs(sgpu_ctx* c) {
   // sigma on Chebyshev coefficients of tau (sgs_stress.f), back to physical y
   const size_t fld = (size_t)g.nyp * g.NP;
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, c->sgs.tau, fld, czf(c, 0), fld, 6, 0, 1.0, 0, c->twy.d);
-  k_sgs_sigma<<<(g.NP + 127) / 128, 128, 0, c->stream>>>(czf(c, 0), czf(c, 6), G, c->alfa, c->beta);
+  k_sgs_sigma<<<(unsigned)(((size_t)g.NP * 32 + 127) / 128), 128, 0, c->stream>>>(czf(c, 0), czf(c, 6), G, c->alfa,
+                                                                                c->beta);
   c->launches++;
   launch_cheb_t<double, sgpu_ctx::pb, double, double>(c, czf(c, 6), fld, c->les_gu, fld, 3, 1, 1.0, 0, c->twy.d);
 }
