@@ -44,8 +44,8 @@ typedef struct sgpu_params {
   int nx, ny, nz;   /* par.f nx, ny, nz (nfxd = nfzd = 1, nfyd = 0) */
   double re;        /* bla.i re (centreline Reynolds number) */
   double xl, zl;    /* box length in x and z */
-  double dt;        /* fixed time step (bla.i dt > 0) */
-  int nst;          /* RK stages: 3 (bla.i nst) */
+  double dt;        /* time step (bla.i dt > 0; a variable step: sgpu_set_dt) */
+  int nst;          /* RK stages: 3 or 4 (bla.i nst; bla/rkcoeff.f) */
   int cflux;        /* 1: constant mass flux (bla.i cflux); 0: fixed px */
   double mflux;     /* target flux under cflux (bla.f:1629 sets 4/3) */
   double px;        /* pressure gradient; first guess under cflux (-2/re) */
@@ -81,8 +81,22 @@ int sgpu_prhs(sgpu_ctx* ctx);
  * the constant-flux px correction, and advances it/t (bla/bla.f:2598-2607). */
 int sgpu_nonlin(sgpu_ctx* ctx);
 int sgpu_linear(sgpu_ctx* ctx);
-/* nsub consecutive substeps (nonlin + linear), enqueued without host syncs. */
+/* nsub consecutive substeps (nonlin + linear), enqueued without host syncs
+ * (nst substeps per full step). */
 int sgpu_step_rk(sgpu_ctx* ctx, int nsub);
+
+/* Variable time step (bla.i dt <= 0; the reference's vart).  sgpu_cfl_rate
+ * gives the CFL number per unit time step of the current state, as
+ * bla/getdt.f forms it (pi times the maximum over the planes of
+ * |u|/dx + |v|/dy + |w|/dz, bla/boxcfl.f, plus 2 |rot|; the first step's dt
+ * is cflmax over it); it synchronises and leaves the state unchanged.
+ * sgpu_set_dt sets the time step of the next full step (the reference's dtnp1,
+ * bla/bla.f:2358-2372): called before a step's last substep, it enters that
+ * substep's weights of the next stage (:2389-2397) and becomes the step's
+ * successor's dt (:2610); called before sgpu_prhs, it is the first step's
+ * dt.  Without it the step stays sgpu_params.dt.  Not on a shard. */
+int sgpu_cfl_rate(sgpu_ctx* ctx, double* rate);
+int sgpu_set_dt(sgpu_ctx* ctx, double dt);
 
 /* Scalars, in this order: px, mflux, t, cfl (CFL*dt of the last evaluated
  * substep, wcflbl.f), an, bn, anp1, bnp1, cnp1, it, tc, dt.  Synchronises.
@@ -295,6 +309,19 @@ int sgpu_stream(sgpu_ctx* ctx, void** stream);
  * (bla/wcflbl.f:87) and returns SGPU_E_CFL (above 10) or SGPU_E_NAN. */
 int sgpu_cfl_partial(sgpu_ctx* ctx, double* cflp, int* pending);
 int sgpu_cfl_set_global(sgpu_ctx* ctx, double cflp);
+
+/* Step 3's pencil kernel: warp = 1 solves each (kx, kz) pencil with one warp
+ * (every column of the pencil in registers across the warp: the tau solves
+ * by the partition method with a parallel cyclic reduction over the lanes,
+ * the Chebyshev derivatives as warp scans), warp = 0 with one thread per
+ * pencil sweeping its columns through memory in the reference's elimination
+ * order (bla/trid.f:120-200), warp = 2 chooses: the warp kernel up to 8192
+ * pencils (nz nx/2; grids such as the LES grid 64x97x64, where one thread
+ * per pencil leaves the GPU idle), the thread kernel above (the default,
+ * also set at sgpu_init; SIMSON_PENCIL_WARP=0/1 in the environment forces
+ * one for new contexts).  Both solve the same tau systems, to round-off.
+ * SGPU_E_PARAM for warp = 1 when ny > 256. */
+int sgpu_set_pencil_kernel(sgpu_ctx* ctx, int warp);
 
 /* Failure detection of the tensor-core kernels (the mixed path's Chebyshev
  * transforms and the learned SGS model): every wait of theirs on an mbarrier

@@ -13,15 +13,17 @@ outside ``oracle/_ref/`` (git-ignored).
 
 Translated units (reference file: what it contributes):
   bla/bla.f         declarations of the driver state + these statement ranges:
-                    849 rkcoeff call, 1080-1082 preprbl call, 1466-1478 first-step
+                    849 rkcoeff call, 1080-1082 preprbl call, 1407-1416 getdt (variable
+                    time step), 1466-1478 first-step
                     RK factors, 1562-1569 prhs call, 1622-1662 channel px/mflux init,
                     1796-1797 substep time, 1819-1826 box shift, 2251-2288 the
-                    nonlinbl plane loop (OpenMP), 2349-2351 wcflbl, 2384-2397 RK
+                    nonlinbl plane loop (OpenMP), 2349-2351 wcflbl, 2355-2380 the next
+                    step's time step of a variable-step run, 2384-2397 RK
                     weights, 2433-2475 the linearbl plane loop (OpenMP), 2598 it=it+1
   bla/nonlinbl.f advection.f boxcfl.f fft2db.f fft2df.f getxz.f putxz.f   (step 2)
   bla/linearbl.f getxy.f putxy.f setmacrhs.f trid.f dcheb.f evald.f evalbc.f
                  solvbc.f                                                  (step 3)
-  bla/prhs.f preprbl.f rkcoeff.f wcflbl.f cvecfft_acc.f                    (startup, CFL, FFTs)
+  bla/prhs.f preprbl.f rkcoeff.f wcflbl.f getdt.f cvecfft_acc.f            (startup, CFL, FFTs)
   bla/boxamp.f                                                             (plane statistics)
   bla/boxxys.f xzsh.f + bla.f 2069-2107                                    (xy statistics)
   bla/nonlinp.f linearp.f crhsc.f setmac.f tridc.f icheb.f + bla.f 2486-2527 (pressure)
@@ -56,12 +58,13 @@ UNIT_FILES = [
     "evalbc.f", "solvbc.f", "prhs.f", "preprbl.f", "rkcoeff.f", "wcflbl.f", "cvecfft_acc.f", "boxamp.f",
     "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
     "les.f", "sgs_stress.f", "filter_cutoff.f", "boxxys.f", "xzsh.f",
-    "nonlinp.f", "linearp.f", "crhsc.f", "setmac.f", "tridc.f", "icheb.f",
+    "nonlinp.f", "linearp.f", "crhsc.f", "setmac.f", "tridc.f", "icheb.f", "getdt.f",
 ]
 
 MAIN_RANGES = [
     ("bla_rkcoeff", 849, 849),
     ("bla_preprbl", 1080, 1082),
+    ("bla_getdt", 1407, 1416),
     ("bla_firststep", 1466, 1478),
     ("bla_lesinit", 1489, 1545),
     ("bla_prhs", 1562, 1569),
@@ -72,6 +75,7 @@ MAIN_RANGES = [
     ("bla_xys", 2069, 2107),
     ("bla_nonlin", 2251, 2288),
     ("bla_cfl", 2349, 2351),
+    ("bla_vart", 2355, 2380),
     ("bla_rkweights", 2384, 2397),
     ("bla_linear", 2433, 2475),
     ("bla_press", 2486, 2527),

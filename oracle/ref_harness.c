@@ -64,6 +64,29 @@ int sref_setup(double re, double xl, double zl, double dt, int cflux, int icfl, 
   return 0;
 }
 
+/* As sref_setup for a bla.i with nst = 3 or 4 stages and, when dt <= 0, the
+ * variable time step: what rparambl.f:1995-2017 leaves (vart = dt <= 0, dtmax
+ * = -dt for dt < 0, cflmax = cflmaxin sqrt(3) or sqrt(8)), the save time and
+ * tmax that bound the step (bla.f:2356-2380; here one far save time).  With
+ * vart the first step's dt comes from getdt when sref_start runs. */
+static int sref_defer_first = 0;
+int sref_setup_rk(double re, double xl, double zl, double dt, int cflux, int icfl, int nthreads, int nst,
+                  double cflmaxin, double tmax) {
+  sref_setup(re, xl, zl, dt > 0 ? dt : 1.0, cflux, icfl, nthreads);
+  v_nst = nst;
+  v_vart = dt <= 0.0;
+  v_dtmax = dt < 0.0 ? -dt : 1.0e30;
+  v_cflmax = cflmaxin * sqrt(nst == 3 ? 3.0 : 8.0);
+  v_tmax = tmax;
+  v_isave = 1;
+  v_tsave[0] = 1.0e30;
+  v_dtn = dt > 0 ? dt : 0.0;
+  bla_rkcoeff();
+  sref_defer_first = v_vart;
+  if (!v_vart) bla_firststep();
+  return 0;
+}
+
 static long slot_size(void) { return (long)v_memnx * v_memny * v_memnz; }
 
 void sref_set_slot(int slot, const double *re_part, const double *im_part) {
@@ -84,6 +107,11 @@ void sref_start(void) {
 #ifdef _OPENMP
   omp_set_num_threads(sref_threads);
 #endif
+  if (sref_defer_first) {
+    bla_getdt();
+    bla_firststep();
+    sref_defer_first = 0;
+  }
   bla_prhs();
   bla_pxinit();
   v_it = 1;
@@ -100,10 +128,14 @@ void sref_substep(void) {
   bla_les();
   bla_nonlin();
   bla_cfl();
+  bla_vart();
   bla_rkweights();
   bla_linear();
   bla_itinc();
-  if ((v_it - 1) % v_nst == 0) v_t = v_t + v_dtn;
+  if ((v_it - 1) % v_nst == 0) {
+    v_t = v_t + v_dtn;
+    if (v_vart) v_dtn = v_dtnp1; /* bla/bla.f:2610 */
+  }
 }
 
 /* Only step 2 or only step 3 (for per-kernel parity tests). */
@@ -115,10 +147,14 @@ void sref_nonlin_only(void) {
 }
 void sref_linear_only(void) {
   bla_cfl();
+  bla_vart();
   bla_rkweights();
   bla_linear();
   bla_itinc();
-  if ((v_it - 1) % v_nst == 0) v_t = v_t + v_dtn;
+  if ((v_it - 1) % v_nst == 0) {
+    v_t = v_t + v_dtn;
+    if (v_vart) v_dtn = v_dtnp1;
+  }
 }
 
 /* scalars: 0 px, 1 mflux, 2 t, 3 cfl, 4 an, 5 bn, 6 anp1, 7 bnp1, 8 cnp1, 9 it, 10 tc, 11 dtn */

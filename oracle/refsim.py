@@ -30,6 +30,7 @@ def _lib(nx, ny, nz, build=True, fma=False, pressure=False):
     lib = ctypes.CDLL(path)
     dp = ctypes.POINTER(ctypes.c_double)
     lib.sref_setup.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int] * 3
+    lib.sref_setup_rk.argtypes = [ctypes.c_double] * 4 + [ctypes.c_int] * 4 + [ctypes.c_double] * 2
     lib.sref_set_slot.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_get_slot.argtypes = [ctypes.c_int, dp, dp]
     lib.sref_scalars.argtypes = [dp]
@@ -55,15 +56,25 @@ def _dp(a):
 class RefSim:
     """The reference channel time stepper (temporal channel, RK3/CN, cflux)."""
 
-    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=3, threads=1, build=True, fma=False,
-                 pressure=False):
+    def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, icfl=None, threads=1, build=True, fma=False,
+                 pressure=False, nst=3, cflmaxin=0.8, tmax=0.0):
+        """dt <= 0: the variable time step of bla.i (first step from getdt,
+        then the CFL rule of bla/bla.f:2355-2380 with cflmax = cflmaxin
+        sqrt(3) or sqrt(8)); nst: 3 or 4 RK stages."""
         self.lib = _lib(nx, ny, nz, build, fma, pressure)
+        self.nst = nst
+        if icfl is None:
+            icfl = nst
         dims = (ctypes.c_int * 12)()
         self.lib.sref_dims(dims)
         self.dims = list(dims)
         self.nx, self.ny, self.nz = nx, ny, nz
         self.nyp = self.dims[4]
-        self.lib.sref_setup(re, xl, zl, dt, int(cflux), int(icfl), int(threads))
+        if nst == 3 and dt > 0:
+            self.lib.sref_setup(re, xl, zl, dt, int(cflux), int(icfl), int(threads))
+        else:
+            self.lib.sref_setup_rk(re, xl, zl, dt, int(cflux), int(icfl), int(threads), int(nst), float(cflmaxin),
+                                   float(tmax))
         self.shape = (nz, self.nyp, nx // 2)
 
     def set_slot(self, slot, field):
@@ -89,7 +100,7 @@ class RefSim:
         self.lib.sref_substep()
 
     def step(self, n=1):
-        for _ in range(3 * n):
+        for _ in range(self.nst * n):
             self.lib.sref_substep()
 
     def nonlin_only(self):

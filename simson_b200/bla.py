@@ -109,6 +109,9 @@ def load_library(build: bool = True):
     lib.sgpu_sgs_mlp_eval.argtypes = [vp, ctypes.POINTER(SgpuSgsMlp), fp, fp, ctypes.c_longlong]
     lib.sgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.sgpu_set_wait_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.sgpu_cfl_rate.argtypes = [vp, dp]
+    lib.sgpu_set_dt.argtypes = [vp, ctypes.c_double]
+    lib.sgpu_set_pencil_kernel.argtypes = [vp, ctypes.c_int]
     lib.sgpu_cfl_partial.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
     lib.sgpu_cfl_set_global.argtypes = [vp, ctypes.c_double]
     lib.sgpu_set_sgs_fallback.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int]
@@ -134,16 +137,19 @@ class Channel:
     """Temporal channel (fltype=1, RK3/CN, tau, ibc=0) resident on one GPU."""
 
     def __init__(self, nx, ny, nz, re, xl, zl, dt, cflux=True, mflux=4.0 / 3.0, px=None,
-                 rot=0.0, icfl=3, precision=FP64, device=0):
+                 rot=0.0, icfl=None, precision=FP64, device=0, nst=3):
         self.lib = load_library()
         self.nx, self.ny, self.nz = nx, ny, nz
         self.dt = dt
+        self.nst = nst
+        if icfl is None:
+            icfl = nst
         self.shape = (nz, ny, nx // 2)
         if px is None:
             px = -2.0 / re  # bla/bla.f:1630 first guess under cflux
         if isinstance(precision, str):
             precision = {"fp64": FP64, "mixed": MIXED}[precision.lower()]
-        prm = SgpuParams(nx, ny, nz, re, xl, zl, dt, 3, int(cflux), mflux, px, rot, icfl, precision, device)
+        prm = SgpuParams(nx, ny, nz, re, xl, zl, dt, nst, int(cflux), mflux, px, rot, icfl, precision, device)
         self._ctx = ctypes.c_void_p()
         self._check(self.lib.sgpu_init(ctypes.byref(prm), ctypes.byref(self._ctx)), "sgpu_init")
 
@@ -215,6 +221,13 @@ class Channel:
                                              ctypes.byref(n)), "copy_block")
         return n.value
 
+    def set_pencil_kernel(self, warp=True):
+        """Step 3 with one warp per pencil (True), one thread per pencil
+        (False) or the automatic choice by grid size ("auto");
+        sgpu_set_pencil_kernel."""
+        self._check(self.lib.sgpu_set_pencil_kernel(self._ctx, 2 if warp == "auto" else int(bool(warp))),
+                    "set_pencil_kernel")
+
     def set_wait_limit(self, limit=0, test_timeout=False):
         """Bounded waits of the tensor-core kernels: iterations per wait
         (0: default); test_timeout makes each launch's first wait run out
@@ -258,8 +271,19 @@ class Channel:
         self.linearbl()
 
     def step(self, n=1):
-        """n full RK3 steps (3 substeps each), no host synchronisation."""
-        self._check(self.lib.sgpu_step_rk(self._ctx, 3 * n), "step")
+        """n full RK steps (nst substeps each), no host synchronisation."""
+        self._check(self.lib.sgpu_step_rk(self._ctx, self.nst * n), "step")
+
+    def cfl_rate(self):
+        """CFL number per unit time step of the current state (bla/getdt.f)."""
+        r = ctypes.c_double()
+        self._check(self.lib.sgpu_cfl_rate(self._ctx, ctypes.byref(r)), "cfl_rate")
+        return r.value
+
+    def set_dt(self, dt):
+        """Time step of the next full step (before prhs: of the first step)."""
+        self.dt = dt
+        self._check(self.lib.sgpu_set_dt(self._ctx, float(dt)), "set_dt")
 
     def substeps(self, n):
         self._check(self.lib.sgpu_step_rk(self._ctx, n), "step")

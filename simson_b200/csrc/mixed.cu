@@ -3,6 +3,7 @@
 // homogeneous-solution and mean-flow kernels of step 3 with FP32 storage.
 #include "mixed.h"
 #include "step2_launch.cuh"
+#include "pencil_warp.cuh"
 
 namespace sb {
 
@@ -34,6 +35,11 @@ void mixed_pencil_hom(cudaStream_t s, const PencilBufs& B, const Dims& g, const 
 void mixed_pencil(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
                   double re, RKc rk, const double* vh, const double* hs, double* cf) {
   k_pencil<float2, double, float><<<(g.p1 - g.p0 + 127) / 128, 128, 0, s>>>(B, g, alfa, beta, re, rk, vh, hs, cf);
+}
+
+bool mixed_pencil_warp(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
+                       double re, RKc rk) {
+  return launch_pencil_warp<float2, float>(s, B, g, alfa, beta, re, rk);
 }
 
 void mixed_mean(cudaStream_t s, const MeanArgs& M, const Dims& g, double re, RKc rk) {

@@ -28,6 +28,9 @@ void mixed_pencil_hom(cudaStream_t s, const PencilBufs& B, const Dims& g, const 
                       double re, double anbn, double* vh, double* hs, double* cf);
 void mixed_pencil(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
                   double re, RKc rk, const double* vh, const double* hs, double* cf);
+// one warp per pencil (pencil_warp.cuh); false when ny is outside its range
+bool mixed_pencil_warp(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,
+                       double re, RKc rk);
 void mixed_mean(cudaStream_t s, const MeanArgs& M, const Dims& g, double re, RKc rk);
 
 }  // namespace sb

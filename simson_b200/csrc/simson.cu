@@ -28,14 +28,17 @@
 #include "mixed.h"
 #include "step2_launch.cuh"
 #include "cheb_tc.cuh"
+#include "pencil_warp.cuh"
 
 using namespace sb;
 
 namespace {
 
-const double ANRK[3] = {8. / 15., 5. / 12., 3. / 4.};
-const double BNRK[3] = {0., -17. / 60., -5. / 12.};
-const double CNRK[3] = {0., 8. / 15., 2. / 3.};
+// RK stage weights a_k, b_k, c_k of the 3-stage (Wray) and the 4-stage
+// scheme, the values of bla/rkcoeff.f:8-48 (row nst - 3)
+const double ANRK[2][4] = {{8. / 15., 5. / 12., 3. / 4., 0.}, {8. / 17., 17. / 60., 5. / 12., 3. / 4.}};
+const double BNRK[2][4] = {{0., -17. / 60., -5. / 12., 0.}, {0., -15. / 68., -17. / 60., -5. / 12.}};
+const double CNRK[2][4] = {{0., 8. / 15., 2. / 3., 0.}, {0., 8. / 17., 8. / 15., 2. / 3.}};
 
 struct Tw {
   double2* d = nullptr;
@@ -78,7 +81,7 @@ struct sgpu_ctx {
   double* hom_vh = nullptr;
   double* hom_s = nullptr;
   double* hom_cf = nullptr;  // coefficient columns [3][4][nyp][NP] (k_pencil_hom)
-  double hom_key[3] = {0.0, 0.0, 0.0};
+  double hom_key[4] = {0.0, 0.0, 0.0, 0.0};
   int hom_next = 0;
   double* mscr = nullptr;    // mean-flow scratch
   double* meanp = nullptr;   // [4][nyp] U, W, Omega_x, Omega_z for the mixed step 2
@@ -130,6 +133,9 @@ struct sgpu_ctx {
   size_t box_n = 0;          // coarse points box_out holds
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
+  // the next full step's time step (the reference's dtnp1, bla/bla.f:2358-2372),
+  // set by sgpu_set_dt; equal to dtn for a fixed time step
+  double dt_next = 0;
   int it = 1;
   double cfl = 0.0;
   bool cfl_pending = false;
@@ -141,6 +147,9 @@ struct sgpu_ctx {
   static constexpr int kbf = MIXED_KB, rbf = MIXED_RB, pbf = 8;  // FP32 tiles (mixed.h)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
+  // step 3 with one warp per pencil (pencil_warp.cuh) instead of one thread
+  // per pencil (k_pencil); SIMSON_PENCIL_WARP=0/1 overrides the default
+  bool pencil_warp = false;
   // bounded waits of the tensor-core kernels (sgpu_set_wait_limit)
   int wait_limit = 0;
   int test_timeout = 0;
@@ -148,13 +157,17 @@ struct sgpu_ctx {
   // launch pattern stays the same
   cudaGraphExec_t step_exec = nullptr;
   bool step_valid = false;
-  unsigned step_key = 0;         // CFL substep mask and LES mode of the captured step
+  unsigned step_key = 0;         // CFL substep mask, LES mode and pencil kernel of the captured step
+  double step_dt = 0.0;          // time step of the captured step
   long long step_launches = 0;   // kernels one captured step launches
   bool graphs = true;
   std::vector<cudaEvent_t> pev;
   std::vector<int> pid;
   int pnext = 0;
 };
+
+// the warp-per-pencil step 3 up to this many pencils (auto selection)
+constexpr int kPencilWarpMaxPencils = 8192;
 
 enum KernelId { K_ZINV = 0, K_XPASS, K_ZFWD, K_CHEB_FWD, K_PENCIL, K_MEAN, K_CHEB_INV, K_OTHER, K_COUNT };
 
@@ -303,7 +316,7 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   if (!prm || !out) return SGPU_E_PARAM;
   *out = nullptr;
   const sgpu_params& P = *prm;
-  if (P.nx < 4 || P.nz < 4 || P.nx % 4 || P.nz % 2 || P.ny < 9 || (P.ny % 2) == 0 || P.nst != 3 || !(P.dt > 0) ||
+  if (P.nx < 4 || P.nz < 4 || P.nx % 4 || P.nz % 2 || P.ny < 9 || (P.ny % 2) == 0 || (P.nst != 3 && P.nst != 4) || !(P.dt > 0) ||
       !(P.re > 0) || !(P.xl > 0) || !(P.zl > 0) || (P.precision != SGPU_FP64 && P.precision != SGPU_MIXED))
     return SGPU_E_PARAM;
   sgpu_ctx* c = new sgpu_ctx();
@@ -348,9 +361,9 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
       cudaMalloc(&c->cz, (size_t)c->ncz * fld * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&c->rz, (size_t)c->nrz * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->mscr, 16 * (size_t)g.nyp * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->hom_vh, 3 * fld * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->hom_s, 3 * 2 * (size_t)g.NP * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->hom_cf, 3 * 4 * fld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_vh, (size_t)P.nst * fld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_s, (size_t)P.nst * 2 * (size_t)g.NP * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->hom_cf, (size_t)P.nst * 4 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->stage, 2 * 7 * fld * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->ampd, 20 * (size_t)g.nyp * sizeof(double)) != cudaSuccess)
     return fail(SGPU_E_CUDA);
@@ -415,9 +428,18 @@ extern "C" int sgpu_init(const sgpu_params* prm, sgpu_ctx** out) {
   cudaFuncSetAttribute(k_cheb<float, sgpu_ctx::pbf, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)s_yf);
   c->dtn = P.dt;
+  c->dt_next = P.dt;
   // SIMSON_GRAPHS=0: launch every kernel directly (no CUDA-graph replay)
   const char* ge = getenv("SIMSON_GRAPHS");
   c->graphs = !(ge && ge[0] == '0');
+  // step 3's pencil kernel: one warp per pencil on grids with few pencils
+  // (its parallelism is per pencil: 0.11 against 0.42 ms at 64x97x64, 2 048
+  // pencils; 0.28 against 0.58 ms at 96x129x96, 4 608), one thread per
+  // pencil on large grids (0.58 against 0.85 ms at 192x129x160, 15 360; 1.3
+  // against 5.2 ms at 384x193x384, 73 728, where the thread kernel streams
+  // near the DRAM bandwidth); SIMSON_PENCIL_WARP=0/1 forces one of them
+  const char* pw = getenv("SIMSON_PENCIL_WARP");
+  c->pencil_warp = pencil_warp_rows(g.nyp) > 0 && (pw ? pw[0] == '1' : g.NP <= kPencilWarpMaxPencils);
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(SGPU_E_CUDA);
   *out = c;
   return SGPU_OK;
@@ -679,8 +701,8 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   const Dims& g = c->g;
   const size_t fld = (size_t)g.nyp * g.NP;
   // first-stage RK factors (bla/bla.f:1466-1478) and cflux px (:1622-1633)
-  c->dtn = c->prm.dt;
-  c->an = c->dtn * ANRK[0];
+  c->dtn = c->dt_next;
+  c->an = c->dtn * ANRK[c->prm.nst - 3][0];
   c->cnp1 = 0.0;
   c->anp1 = c->an;
   c->bnp1 = 0.0;
@@ -885,20 +907,28 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   return cuda_fail(cudaGetLastError(), "nonlin launch");
 }
 
-// RK weights of the coming linear step (bla/bla.f:2384-2397)
+// RK weights of the coming linear step (bla/bla.f:2384-2397); the weights of
+// the next step's first stage, formed in a step's last substep, take that
+// step's time step dtnp1 (:2358-2372)
 static void rk_advance(sgpu_ctx* c) {
+  const int nst = c->prm.nst;
   c->an = c->anp1;
   c->bn = c->bnp1;
-  const int k = c->it % 3;
-  c->anp1 = c->dtn * ANRK[k];
-  c->bnp1 = c->dtn * BNRK[k];
-  c->cnp1 = c->dtn * CNRK[k];
+  const int k = c->it % nst;
+  const double dtp = (k == 0) ? c->dt_next : c->dtn;
+  c->anp1 = dtp * ANRK[nst - 3][k];
+  c->bnp1 = dtp * BNRK[nst - 3][k];
+  c->cnp1 = dtp * CNRK[nst - 3][k];
 }
 
-// substep counter and time after a linear step (bla/bla.f:2598-2607)
+// substep counter, time and time step after a linear step
+// (bla/bla.f:2598-2610)
 static void it_advance(sgpu_ctx* c) {
   c->it += 1;
-  if ((c->it - 1) % 3 == 0) c->t = c->t + c->dtn;
+  if ((c->it - 1) % c->prm.nst == 0) {
+    c->t = c->t + c->dtn;
+    c->dtn = c->dt_next;
+  }
 }
 
 static int enqueue_linear(sgpu_ctx* c) {
@@ -925,32 +955,44 @@ static int enqueue_linear(sgpu_ctx* c) {
   M.cflux = P.cflux;
   // the mean flow belongs to the context that owns pencil 0 (kz = 0)
   const bool own_mean = g.p0 == 0;
+  // the warp kernels of step 3 come with the warp mean-flow solve
+  auto mean = [&](cudaStream_t st) {
+    if (c->pencil_warp && (c->mixed ? launch_mean_warp<float2>(st, M, g, P.re, rk)
+                                    : launch_mean_warp<double2>(st, M, g, P.re, rk)))
+      return;
+    if (c->mixed)
+      mixed_mean(st, M, g, P.re, rk);
+    else
+      k_mean<double2><<<1, 32, 0, st>>>(M, g, P.re, rk);
+  };
   if (!own_mean) {
   } else if (c->prof) {
     prof_mark(c, K_MEAN);
-    if (c->mixed)
-      mixed_mean(c->stream, M, g, P.re, rk);
-    else
-      k_mean<double2><<<1, 32, 0, c->stream>>>(M, g, P.re, rk);
+    mean(c->stream);
   } else {
     cudaEventRecord(c->fork, c->stream);
     cudaStreamWaitEvent(c->side, c->fork, 0);
-    if (c->mixed)
-      mixed_mean(c->side, M, g, P.re, rk);
-    else
-      k_mean<double2><<<1, 32, 0, c->side>>>(M, g, P.re, rk);
+    mean(c->side);
     cudaEventRecord(c->join, c->side);
   }
+  if (c->pencil_warp) {
+    // one warp per pencil: the homogeneous solutions are columns of its own
+    // solves, no per-stage cache
+    prof_mark(c, K_PENCIL);
+    const bool ok = c->mixed ? mixed_pencil_warp(c->stream, B, g, c->alfa, c->beta, P.re, rk)
+                             : launch_pencil_warp<double2, double>(c->stream, B, g, c->alfa, c->beta, P.re, rk);
+    if (!ok) return SGPU_E_PARAM;
+  } else {
   // this stage's homogeneous solutions, computed on its first use (a key of
   // 0 is never a valid a_n + b_n: dt > 0)
   const double anbn = rk.an + rk.bn;
   int hs = -1;
-  for (int s = 0; s < 3; ++s)
+  for (int s = 0; s < c->prm.nst; ++s)
     if (c->hom_key[s] == anbn) hs = s;
   const size_t fld = (size_t)g.nyp * g.NP;
   if (hs < 0) {
     hs = c->hom_next;
-    c->hom_next = (c->hom_next + 1) % 3;
+    c->hom_next = (c->hom_next + 1) % c->prm.nst;
     c->hom_key[hs] = anbn;
     prof_mark(c, K_OTHER);
     if (c->mixed)
@@ -971,6 +1013,7 @@ static int enqueue_linear(sgpu_ctx* c) {
   else
     k_pencil<double2, double, double><<<(g.p1 - g.p0 + 127) / 128, 128, 0, c->stream>>>(B, g, c->alfa, c->beta, P.re, rk,
                                                                                  vhc, hsc, cfc);
+  }
   if (!c->prof && own_mean) cudaStreamWaitEvent(c->stream, c->join, 0);
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
@@ -1014,6 +1057,60 @@ extern "C" int sgpu_linear(sgpu_ctx* c) {
   return enqueue_linear(c);
 }
 
+// The CFL number per unit time step of the current state (bla/getdt.f: the
+// step-2 transforms to physical space, bla/boxcfl.f's maximum of
+// |u|/dx + |v|/dy + |w|/dz over every plane, times pi, plus 2 |rot|): the
+// first time step of a variable-step run is cflmax over this.  The state is
+// not changed; the step-2 scratch is.
+extern "C" int sgpu_cfl_rate(sgpu_ctx* c, double* rate) {
+  if (!c || !rate) return SGPU_E_PARAM;
+  if (!c->have_state) return SGPU_E_STATE;
+  if (sharded(c) || c->cfl_pending) return SGPU_E_STATE;
+  const Dims& g = c->g;
+  const sgpu_params& P = c->prm;
+  k_cfl_reset<<<1, 1, 0, c->stream>>>(c->cfl_bits);
+  const int nyl = g.y1 - g.y0;
+  const double dxi = (double)(g.nx - 2) / P.xl;
+  const double dzi = (double)(g.nz - 2) / P.zl;
+  if (c->mixed) {
+    float2* zbf = reinterpret_cast<float2*>(c->zb);
+    float2* xbf = reinterpret_cast<float2*>(c->xb);
+    dim3 gzf((g.nx2 + sgpu_ctx::kbf - 1) / sgpu_ctx::kbf, nyl);
+    dim3 gxf((g.nzp + sgpu_ctx::rbf - 1) / sgpu_ctx::rbf, nyl);
+    mixed_mean_profiles(c->stream, c->stf, c->meanp, g);
+    mixed_zinv(c->stream, gzf, smem_fft(g.nzp, sgpu_ctx::kbf, sizeof(float2)), c->stf, zbf, g, c->twz.plan, c->twz.f,
+               c->alfa, c->beta);
+    mixed_xpass(c->stream, gxf, smem_fft(g.nxp, 3 * sgpu_ctx::rbf, sizeof(float2)), zbf, xbf, g, c->twx.plan,
+                c->twx.f, c->dyi, dxi, dzi, P.rot, c->cfl_bits, c->meanp);
+  } else {
+    dim3 gz((g.nx2 + c->kb - 1) / c->kb, nyl);
+    dim3 gx((g.nzp + c->rb - 1) / c->rb, nyl);
+    launch_zinv<double, sgpu_ctx::kb, double>(gz, smem_fft(g.nzp, c->kb, sizeof(double2)), c->stream, c->st, c->zb,
+                                              g, c->twz.plan, c->twz.d, c->alfa, c->beta, 0);
+    launch_xpass<double, sgpu_ctx::rb, sgpu_ctx::xpass64_threads>(gx, smem_fft(g.nxp, 3 * c->rb, sizeof(double2)),
+                                                                  c->stream, c->zb, c->xb, g, c->twx.plan, c->twx.d,
+                                                                  c->dyi, dxi, dzi, P.rot, c->cfl_bits, nullptr);
+  }
+  c->launches += c->mixed ? 4 : 3;
+  CK(cudaGetLastError());
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double m;
+  memcpy(&m, &bits, sizeof(m));
+  const double pi = 3.1415926535897932385;
+  *rate = m * pi + 2. * fabs(P.rot);
+  return SGPU_OK;
+}
+
+// The time step of the next full step (bla/bla.f:2358-2372 dtnp1, applied as
+// :2389-2397 and :2610 do).  Before sgpu_prhs: the first step's.
+extern "C" int sgpu_set_dt(sgpu_ctx* c, double dt) {
+  if (!c || !(dt > 0.0) || !std::isfinite(dt)) return SGPU_E_PARAM;
+  c->dt_next = dt;
+  return SGPU_OK;
+}
+
 // Sharded runs: the partial maximum of this shard's planes, and the stop
 // test on the all-reduced one (bla/wcflbl.f:82-98 with MPI_Allreduce).  The
 // partial maximum is read only when a substep evaluated it.
@@ -1038,46 +1135,49 @@ extern "C" int sgpu_cfl_set_global(sgpu_ctx* c, double cflp) {
   return SGPU_OK;
 }
 
-// Launch pattern of the RK3 step that starts now: bits 0-2 the substeps that
-// evaluate the CFL number, bits 3-5 the LES mode.  0xffffffff: the step cannot
-// be replayed (not at a step boundary, or a stage's homogeneous solutions not
-// yet cached: that substep launches k_pencil_hom).
+// Launch pattern of the RK step that starts now: bits 0-3 the substeps that
+// evaluate the CFL number, bits 4-7 the LES mode, bit 8 the pencil kernel.
+// 0xffffffff: the step cannot be replayed (not at a step boundary, its time
+// step changes at its end, or a stage's homogeneous solutions not yet
+// cached: that substep launches k_pencil_hom).
 static unsigned step_pattern(const sgpu_ctx* c) {
-  if ((c->it - 1) % 3 != 0) return 0xffffffffu;
-  unsigned key = (unsigned)c->iles << 3;
+  const int nst = c->prm.nst;
+  if ((c->it - 1) % nst != 0 || c->dt_next != c->dtn) return 0xffffffffu;
+  unsigned key = ((unsigned)c->iles << 4) | ((c->pencil_warp ? 1u : 0u) << 8);
   double anp1 = c->anp1, bnp1 = c->bnp1;
-  for (int s = 0; s < 3; ++s) {
+  for (int s = 0; s < nst; ++s) {
     const int it = c->it + s;
     if (c->prm.icfl > 0 && (it - 1) % c->prm.icfl == 0) key |= 1u << s;
     const double anbn = anp1 + bnp1;  // a_n + b_n of this substep's linear step
-    bool cached = false;
-    for (int h = 0; h < 3; ++h) cached = cached || c->hom_key[h] == anbn;
+    bool cached = c->pencil_warp;  // the warp kernel keeps no per-stage cache
+    for (int h = 0; h < nst; ++h) cached = cached || c->hom_key[h] == anbn;
     if (!cached) return 0xffffffffu;
-    anp1 = c->dtn * ANRK[it % 3];
-    bnp1 = c->dtn * BNRK[it % 3];
+    anp1 = c->dtn * ANRK[nst - 3][it % nst];
+    bnp1 = c->dtn * BNRK[nst - 3][it % nst];
   }
   return key;
 }
 
-// Capture the three substeps of this step into c->step_exec (launching
-// nothing); the host bookkeeping advances as in a direct launch.  On failure
-// the host state is restored and the caller launches directly.
+// Capture the substeps of this step into c->step_exec (launching nothing);
+// the host bookkeeping advances as in a direct launch.  On failure the host
+// state is restored and the caller launches directly.
 static int capture_step(sgpu_ctx* c, unsigned key) {
-  NvtxRange nv("capture RK3 step");
+  NvtxRange nv("capture RK step");
   const double an = c->an, bn = c->bn, anp1 = c->anp1, bnp1 = c->bnp1, cnp1 = c->cnp1, t = c->t, tc = c->tc;
+  const double dtn = c->dtn;
   const int it = c->it;
   const long long launches = c->launches;
   const bool cfl_pending = c->cfl_pending;
   auto restore = [&] {
     c->an = an; c->bn = bn; c->anp1 = anp1; c->bnp1 = bnp1; c->cnp1 = cnp1; c->t = t; c->tc = tc; c->it = it;
-    c->launches = launches; c->cfl_pending = cfl_pending;
+    c->dtn = dtn; c->launches = launches; c->cfl_pending = cfl_pending;
   };
   if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
     return SGPU_E_CUDA;
   }
   int r = SGPU_OK;
-  for (int s = 0; s < 3 && r == SGPU_OK; ++s) {
+  for (int s = 0; s < c->prm.nst && r == SGPU_OK; ++s) {
     r = enqueue_nonlin(c);
     if (r == SGPU_OK) r = enqueue_linear(c);
   }
@@ -1110,6 +1210,7 @@ static int capture_step(sgpu_ctx* c, unsigned key) {
   }
   c->step_valid = true;
   c->step_key = key;
+  c->step_dt = dtn;
   c->step_launches = c->launches - launches;
   return SGPU_OK;
 }
@@ -1117,12 +1218,12 @@ static int capture_step(sgpu_ctx* c, unsigned key) {
 // Host side of one replayed step: what enqueue_nonlin / enqueue_linear do to
 // the bookkeeping, without launching.
 static void replay_host(sgpu_ctx* c) {
-  for (int s = 0; s < 3; ++s) {
+  for (int s = 0; s < c->prm.nst; ++s) {
     c->tc = c->t + c->cnp1;
     rk_advance(c);
     it_advance(c);
   }
-  if (c->step_key & 7u) c->cfl_pending = true;
+  if (c->step_key & 15u) c->cfl_pending = true;
   c->launches += c->step_launches;
 }
 
@@ -1132,22 +1233,24 @@ extern "C" int sgpu_step_rk(sgpu_ctx* c, int nsub) {
   if (!c->have_state) return SGPU_E_STATE;
   // a shard needs the block exchanges between its two steps (host-driven)
   if (sharded(c)) return SGPU_E_STATE;
+  const int nst = c->prm.nst;
   int s = 0;
   while (s < nsub) {
-    // whole steps with an unchanged launch pattern replay one CUDA graph;
-    // the rest (first steps, profiling, partial steps) launch directly
-    const unsigned key = (c->graphs && !c->prof && nsub - s >= 3) ? step_pattern(c) : 0xffffffffu;
+    // whole steps with an unchanged launch pattern and time step replay one
+    // CUDA graph; the rest (first steps, profiling, partial steps, a step
+    // whose time step changes) launch directly
+    const unsigned key = (c->graphs && !c->prof && nsub - s >= nst) ? step_pattern(c) : 0xffffffffu;
     if (key != 0xffffffffu) {
-      if (c->step_valid && c->step_key == key) {
-        NvtxRange nv("RK3 step (graph)");
+      if (c->step_valid && c->step_key == key && c->step_dt == c->dtn) {
+        NvtxRange nv("RK step (graph)");
         CK(cudaGraphLaunch(c->step_exec, c->stream));
         replay_host(c);
-        s += 3;
+        s += nst;
         continue;
       }
       if (capture_step(c, key) == SGPU_OK) {
         CK(cudaGraphLaunch(c->step_exec, c->stream));
-        s += 3;
+        s += nst;
         continue;
       }
       c->graphs = false;  // capture not possible here: launch directly from now on
@@ -1185,7 +1288,7 @@ static int offload_enqueue(sgpu_ctx* c, double* ur, double* ui, int nsteps) {
       c->launches++;
     }
     c->have_state = true;
-    int r = sgpu_step_rk(c, 3);
+    int r = sgpu_step_rk(c, c->prm.nst);
     if (r) return r;
     // out: slot by slot, each copy as soon as its conversion is done
     for (int k = 0; k < 7; ++k) {
@@ -1258,6 +1361,15 @@ extern "C" int sgpu_get_scalars(sgpu_ctx* c, double* out, int n) {
   // (constant flux) or the mass flux
   if (r == SGPU_OK && c->have_state && !(std::isfinite(sc[0]) && std::isfinite(sc[1]))) return SGPU_E_NAN;
   return r;
+}
+
+extern "C" int sgpu_set_pencil_kernel(sgpu_ctx* c, int warp) {
+  if (c) c->step_valid = false;  // the captured step launches the other kernel
+  if (!c || warp < 0 || warp > 2) return SGPU_E_PARAM;
+  const bool fits = pencil_warp_rows(c->g.nyp) > 0;
+  if (warp == 1 && !fits) return SGPU_E_PARAM;
+  c->pencil_warp = warp == 2 ? (fits && c->g.NP <= kPencilWarpMaxPencils) : warp == 1;
+  return SGPU_OK;
 }
 
 extern "C" int sgpu_set_wait_limit(sgpu_ctx* c, int limit, int test_timeout) {

@@ -183,6 +183,7 @@ class ShardedChannel:
 
     def __init__(self, channel, rank, nranks, device, group=None):
         self.ch = channel
+        self.nst = getattr(channel, "nst", 3)
         self.rank, self.nranks = rank, nranks
         self.ranges = shard_ranges(channel.ny, channel.nz, nranks)
         channel.set_shard(*self.ranges[rank])
@@ -202,7 +203,7 @@ class ShardedChannel:
         self.bytes_moved += s1 + s2
 
     def step(self, n=1):
-        for _ in range(3 * n):
+        for _ in range(self.nst * n):
             self.substep()
 
 
@@ -214,6 +215,7 @@ class LocalShards:
 
     def __init__(self, make_channel, nranks, device):
         self.chs = [make_channel() for _ in range(nranks)]
+        self.nst = getattr(self.chs[0], "nst", 3)
         self.ranges = shard_ranges(self.chs[0].ny, self.chs[0].nz, nranks)
         for ch, rg in zip(self.chs, self.ranges):
             ch.set_shard(*rg)
@@ -245,7 +247,7 @@ class LocalShards:
             ch.linearbl()
 
     def step(self, n=1):
-        for _ in range(3 * n):
+        for _ in range(self.nst * n):
             self.substep()
 
     def state(self, nslots=7):

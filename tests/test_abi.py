@@ -51,7 +51,7 @@ def test_init_rejects_invalid_parameters():
     lib = _lib()
     good = dict(nx=48, ny=65, nz=48, re=4200.0, xl=12.566, zl=6.283, dt=0.01, nst=3, cflux=1, mflux=4.0 / 3.0,
                 px=-2.0 / 4200.0, rot=0.0, icfl=3, precision=0, device=0)
-    bad = [dict(nx=46), dict(nx=0), dict(nz=47), dict(ny=64), dict(ny=7), dict(nst=4), dict(dt=0.0), dict(dt=-1.0),
+    bad = [dict(nx=46), dict(nx=0), dict(nz=47), dict(ny=64), dict(ny=7), dict(nst=2), dict(nst=5), dict(dt=0.0), dict(dt=-1.0),
            dict(re=0.0), dict(xl=0.0), dict(zl=-1.0), dict(precision=2), dict(dt=float("nan"))]
     for change in bad:
         p = SgpuParams(**{**good, **change})

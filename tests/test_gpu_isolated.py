@@ -51,8 +51,17 @@ def test_step2_isolated(grid, need_ref):
 
 
 @pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
-def test_step3_isolated(grid, need_ref):
+@pytest.mark.parametrize("kernel", ["thread", "warp"])
+def test_step3_isolated(grid, kernel, need_ref):
+    """The thread-per-pencil kernel keeps the reference's elimination order
+    (1e-12); the warp-per-pencil kernel sums in another order, which the
+    stiff lam = k^2 + 2 Re/(a_n + b_n) solves amplify to a few 1e-12 on the
+    vorticities (5e-12), and its mean-flow solve sums U's flux once (puw
+    within 1e-11 of its largest value)."""
     ref, gpu = setup(grid, need_ref)
+    gpu.set_pencil_kernel(kernel == "warp")
+    tol = 1e-12 if kernel == "thread" else 5e-12
+    ptol = 1e-12 if kernel == "thread" else 1e-11
     for k in range(3):
         ref.nonlin_only()
         gpu.nonlinbl()
@@ -62,5 +71,5 @@ def test_step3_isolated(grid, need_ref):
         rs, gs = ref.state(), gpu.state()
         errs = [rel(gs[s], rs[s]) for s in range(7)]
         print("step3 substep", k, ["%.2e" % e for e in errs], "px", gpu.scalars()["px"] - ref.scalars()["px"])
-        np.testing.assert_allclose(gpu.puw(), ref.puw(), rtol=0, atol=1e-12 * np.abs(ref.puw()).max())
-        assert max(errs) < 1e-12, errs
+        np.testing.assert_allclose(gpu.puw(), ref.puw(), rtol=0, atol=ptol * np.abs(ref.puw()).max())
+        assert max(errs) < tol, errs
