@@ -127,6 +127,13 @@ def _cheb_regrid(q, nyp_out):
     return np.einsum("yk,zkx->zyx", np.cos(np.outer(theta_out, j)), a)
 
 
+def read_header(path, pressure_file=False):
+    """The header records of a .u (or .p) file as read_u returns them,
+    without the fields."""
+    head, _ = read_u(path, m=0, pressure_file=pressure_file)
+    return head
+
+
 def read_u(path, m=3, nx=None, nyp=None, nz=None, varsiz=True, pressure_file=False):
     """Read a .u file.  Returns (header dict, list of m fields (nz, nyp,
     nx/2)).  With a target size different from the file's, as rdiscbl does
@@ -196,6 +203,8 @@ def read_u(path, m=3, nx=None, nyp=None, nz=None, varsiz=True, pressure_file=Fal
             q[nz - nzcin // 2] = 0.0  # the file's -nzin/2 mode (rdiscbl.f:373-385)
         fields.append(q)
     # wall velocities of the mean mode, as read (rdiscbl.f:306-309)
+    if not walls:
+        return head, fields
     head["u0upp"], head["u0low"] = walls[0]
     if m >= 3:
         head["w0upp"], head["w0low"] = walls[2]

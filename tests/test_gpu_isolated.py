@@ -55,12 +55,14 @@ def test_step2_isolated(grid, need_ref):
 def test_step3_isolated(grid, kernel, need_ref):
     """The thread-per-pencil kernel keeps the reference's elimination order
     (1e-12); the warp-per-pencil kernel sums in another order, which the
-    stiff lam = k^2 + 2 Re/(a_n + b_n) solves amplify to a few 1e-12 on the
-    vorticities (5e-12), and its mean-flow solve sums U's flux once (puw
-    within 1e-11 of its largest value)."""
+    stiff lam = k^2 + 2 Re/(a_n + b_n) solves amplify on the vorticities to a
+    few 1e-12 at 48x65x48 and 3e-11 at 16x17x16 (the reference built with
+    fused multiply-add is 9e-12 from itself there after two steps): 5e-11;
+    its mean-flow solve sums U's flux once (puw within 1e-11 of its largest
+    value)."""
     ref, gpu = setup(grid, need_ref)
     gpu.set_pencil_kernel(kernel == "warp")
-    tol = 1e-12 if kernel == "thread" else 5e-12
+    tol = 1e-12 if kernel == "thread" else 5e-11
     ptol = 1e-12 if kernel == "thread" else 1e-11
     for k in range(3):
         ref.nonlin_only()
