@@ -364,6 +364,37 @@ int sgpu_sync(sgpu_ctx* ctx);
 int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in, void* h_out, double* cflp_max,
                         void* stream);
 
+/* Spatial simulation (bla.i spat = .true.) in the channel (ibc = 0; the
+ * spatially developing Poiseuille and Couette flows, fltype 4 and 5): the
+ * fringe forcing of bla/fring.f (no wave, streak or Orr-Sommerfeld forcing),
+ * H -= lambda(x) (u - U_b(x, y)) on the three components in physical space
+ * after the products of step 2 (bla/nonlinbl.f:681-691), and the same on the
+ * products of sgpu_pressure (bla/fringp.f).  The host computes the base flow
+ * (bla/bflow.f) and the pressure gradient (bla/bla.f:1655-1661: px = 0 and no
+ * constant flux outside the temporal channel). */
+typedef struct {
+  double fstart, fend; /* bla.i fstart, fend: the fringe's start and end in x */
+  double frise, ffall; /* bla.i frise, ffall: its rise and fall distances */
+  double fmax;         /* bla.i fmax: its strength (0: no fringe) */
+  double xsc;          /* x of the frame (bla/bla.f:1819 xs - cnp1 u0low; 0 without Galilean shift) */
+} sgpu_fringe;
+
+/* lambda at the nxp physical x points (x point 2k-2 and 2k-1 are the
+ * reference's fring1(k), fring2(k)), as bla/ffun.f:58-83 computes it with the
+ * smooth step of bla/step.f; zero outside the fringe.  Host only (no context,
+ * no GPU).  SGPU_E_PARAM when the fringe leaves the box. */
+int sgpu_fringe_function(const sgpu_fringe* f, int nxp, double xl, double* lambda);
+
+/* Fringe forcing from now on (f == NULL or fmax == 0: off), towards the base
+ * flow of sgpu_set_base_flow (zero until set).  Replaces bla/bla.f:2166-2175
+ * (ffun) and the fring call of bla/nonlinbl.f:681-691. */
+int sgpu_set_fringe(sgpu_ctx* ctx, const sgpu_fringe* f);
+
+/* The base flow bu1, bu2(nxp/2+1, nyp, 3) of bla/bflow.f (u, v, w in
+ * physical space at the even and odd x points, the reference's x pairs; the
+ * last x row is not read).  bu1 = bu2 = NULL: zero. */
+int sgpu_set_base_flow(sgpu_ctx* ctx, const double* bu1, const double* bu2);
+
 /* Per-kernel timing for profiling runs: enable, run substeps, read the
  * milliseconds and launch counts per kernel id (0 zinv, 1 xpass, 2 zfwd,
  * 3 Chebyshev forward, 4 pencil solve, 5 mean flow, 6 Chebyshev inverse,

@@ -29,6 +29,8 @@ Translated units (reference file: what it contributes):
   bla/nonlinp.f linearp.f crhsc.f setmac.f tridc.f icheb.f + bla.f 2486-2527 (pressure)
   bla/init_filter.f lpf_y.f hpf_y.f bandsolver.f + bla.f 1489-1545         (ADM-RT LES filters)
   bla/les.f sgs_stress.f filter_cutoff.f + bla.f 1945-2020                 (eddy-viscosity LES)
+  bla/fring.f fringp.f ffun.f step.f bflow.f cbflow.f + bla.f 1338-1374 (base flow),
+                 2166-2175 (fringe function)                               (spatial channel)
 For grids up to SMAG_MAX_POINTS the driver's compile-time switch iiles_smag
 (bla/bla.f:28) is set to 1, as the reference instructs for dynamic
 Smagorinsky runs, so that its SGS-stress arrays exist.
@@ -59,6 +61,7 @@ UNIT_FILES = [
     "init_filter.f", "lpf_y.f", "hpf_y.f", "bandsolver.f",
     "les.f", "sgs_stress.f", "filter_cutoff.f", "boxxys.f", "xzsh.f",
     "nonlinp.f", "linearp.f", "crhsc.f", "setmac.f", "tridc.f", "icheb.f", "getdt.f",
+    "fring.f", "fringp.f", "ffun.f", "step.f", "bflow.f", "cbflow.f",
 ]
 
 MAIN_RANGES = [
@@ -69,6 +72,8 @@ MAIN_RANGES = [
     ("bla_lesinit", 1489, 1545),
     ("bla_prhs", 1562, 1569),
     ("bla_pxinit", 1622, 1662),
+    ("bla_bflow", 1338, 1374),
+    ("bla_ffun", 2166, 2175),
     ("bla_substep_time", 1796, 1797),
     ("bla_les", 1945, 2020),
     ("bla_boxshift", 1819, 1826),

@@ -864,6 +864,11 @@ class Ctx:
                 return f"&({CTYPE[t]}){{{self.cname(a[1])}}}"
             if v is not None and v.dummy:
                 return self.cname(a[1])
+            if v is not None and v.char:
+                # program-level character variables (file names) are not
+                # declared: no translated unit processes characters, so they
+                # pass as null, like character literals
+                return "(char*)0"
             if v is not None and (v.external or a[1] in self.g.functions) and v.typ is None:
                 return f"(void*)f_{a[1]}"
             return f"&{self.cname(a[1])}"

@@ -117,6 +117,36 @@ void sref_start(void) {
   v_it = 1;
 }
 
+/* Spatial simulation in the channel (bla.i spat = .true., ibc = 0) with the
+ * flow type of the initial field (4 Poiseuille, 5 Couette): the fringe
+ * parameters of bla.i (rparambl.f leaves them as given; no wave, streak or
+ * OS forcing, rbfl = .false.), then the base-flow block of bla/bla.f:1338-1374
+ * (bflow, the boundary values for ibc = 0).  The pressure gradient follows
+ * from bla_pxinit in sref_start (px = 0, no constant flux for fltype != 1);
+ * each substep computes the fringe function (bla/bla.f:2166-2175) before
+ * step 2.  Call after sref_setup / sref_setup_rk, before sref_start. */
+void sref_set_spatial(int fltype, double fstart, double fend, double frise, double ffall, double fmax) {
+  v_spat = 1; v_fltype = fltype; v_rbfl = 0; v_tabfre = 0; v_pert = 0; v_bf3 = 0;
+  v_fstart = fstart; v_fend = fend; v_frise = frise; v_ffall = ffall; v_fmax = fmax;
+  v_ampob = 0.0; v_amp2d = 0.0; v_osmod = 0; v_streak = 0; v_waves = 0;
+  v_bstart = 0.0; v_blength = 0.0;
+  bla_bflow();
+}
+
+/* The fringe function fring1, fring2 (nxp/2 each) at the current substep's
+ * frame (bla/ffun.f), and the base flow bu1, bu2 (nxp/2+1, nyp, 3). */
+void sref_get_fringe(double *f1, double *f2) {
+  bla_boxshift();
+  bla_ffun();
+  memcpy(f1, v_fring1, (size_t)(v_nxp / 2) * sizeof(double));
+  memcpy(f2, v_fring2, (size_t)(v_nxp / 2) * sizeof(double));
+}
+void sref_get_base(double *b1, double *b2) {
+  const size_t n = (size_t)(v_nxp / 2 + 1) * v_nyp * 3;
+  memcpy(b1, v_bu1, n * sizeof(double));
+  memcpy(b2, v_bu2, n * sizeof(double));
+}
+
 /* One RK substep: step 2 (nonlinbl over xz-planes), CFL, RK weights, step 3
  * (linearbl over xy-planes), iteration counter and full-step time update. */
 void sref_substep(void) {
@@ -125,6 +155,7 @@ void sref_substep(void) {
 #endif
   bla_substep_time();
   bla_boxshift();
+  if (v_spat) bla_ffun();
   bla_les();
   bla_nonlin();
   bla_cfl();
@@ -142,6 +173,7 @@ void sref_substep(void) {
 void sref_nonlin_only(void) {
   bla_substep_time();
   bla_boxshift();
+  if (v_spat) bla_ffun();
   bla_les();
   bla_nonlin();
 }
@@ -185,6 +217,7 @@ void sref_get_amp(double *a) { memcpy(a, v_amp, (size_t)v_nyp * 20 * sizeof(doub
  * omega_x, omega_z in slots 4-5).  Returns -1 on a pressure = 0 build. */
 int sref_pressure(double *re_part, double *im_part) {
   if (v_pressure != 1) return -1;
+  if (v_spat) bla_ffun();
   v_do_press = 1;
   bla_press();
   v_do_press = 0;

@@ -46,6 +46,9 @@ def _lib(nx, ny, nz, build=True, fma=False, pressure=False):
     lib.sref_get_amp.argtypes = [dp]
     lib.sref_xys.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp]
     lib.sref_pressure.argtypes = [dp, dp]
+    lib.sref_set_spatial.argtypes = [ctypes.c_int] + [ctypes.c_double] * 5
+    lib.sref_get_fringe.argtypes = [dp, dp]
+    lib.sref_get_base.argtypes = [dp, dp]
     return lib
 
 
@@ -131,6 +134,29 @@ class RefSim:
         (cs = 0: dynamic Smagorinsky); filters set up as bla/bla.f:1489-1545."""
         self.lib.sref_set_les(int(iles), float(cutoff_inv), int(iord), float(chi), int(ihighorder),
                               float(cs), int(ineg))
+
+    def set_spatial(self, fltype=4, fstart=-13.0, fend=0.0, frise=7.0, ffall=3.0, fmax=1.0):
+        """Spatial simulation (spat = .true.) with the fringe of bla.i and the
+        base flow of flow type fltype (4 Poiseuille, 5 Couette) computed by
+        the reference's bflow; px = 0 and no constant flux follow at start()."""
+        self.lib.sref_set_spatial(int(fltype), float(fstart), float(fend), float(frise), float(ffall), float(fmax))
+
+    def fringe(self):
+        """fring1, fring2 of bla/ffun.f (x pairs) at the current frame."""
+        n = self.dims[3] // 2
+        f1 = np.empty(n)
+        f2 = np.empty(n)
+        self.lib.sref_get_fringe(_dp(f1), _dp(f2))
+        return f1, f2
+
+    def base_flow(self):
+        """bu1, bu2 of bla/bflow.f, shape (3, nyp, nxp/2+1) (the Fortran
+        (nxp/2+1, nyp, 3) array)."""
+        shape = (3, self.nyp, self.dims[3] // 2 + 1)
+        b1 = np.empty(shape)
+        b2 = np.empty(shape)
+        self.lib.sref_get_base(_dp(b1), _dp(b2))
+        return b1, b2
 
     def tau(self, comp):
         """SGS stress component comp (1..6 = 11 12 13 22 23 33), shape (nz, nyp, nx//2)."""

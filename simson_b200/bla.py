@@ -50,6 +50,12 @@ class SgpuSgsMlp(ctypes.Structure):
         ("s_in", ctypes.c_float), ("s_y", ctypes.c_float), ("s_out", ctypes.c_float)]
 
 
+class SgpuFringe(ctypes.Structure):
+    """The fringe of bla.i (fstart, fend, frise, ffall, fmax) and the frame's x."""
+    _fields_ = [("fstart", ctypes.c_double), ("fend", ctypes.c_double), ("frise", ctypes.c_double),
+                ("ffall", ctypes.c_double), ("fmax", ctypes.c_double), ("xsc", ctypes.c_double)]
+
+
 class SimsonError(RuntimeError):
     """A non-zero status of the C ABI; .code holds the SGPU_E_* value."""
 
@@ -120,6 +126,9 @@ def load_library(build: bool = True):
     lib.sgpu_set_shard.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.sgpu_copy_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+    lib.sgpu_fringe_function.argtypes = [ctypes.POINTER(SgpuFringe), ctypes.c_int, ctypes.c_double, dp]
+    lib.sgpu_set_fringe.argtypes = [vp, ctypes.POINTER(SgpuFringe)]
+    lib.sgpu_set_base_flow.argtypes = [vp, dp, dp]
     lib.sgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.sgpu_profile_read.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     _LIB = lib
@@ -131,6 +140,63 @@ def _dp(a):
 
 
 SCALARS = ("px", "mflux", "t", "cfl", "an", "bn", "anp1", "bnp1", "cnp1", "it", "tc", "dt")
+
+
+def fringe_function(nxp, xl, fstart, fend, frise, ffall, fmax, xsc=0.0):
+    """The fringe function lambda at the nxp physical x points (bla/ffun.f;
+    points 2k-2, 2k-1 are the reference's fring1(k), fring2(k)).  Host code of
+    the library (sgpu_fringe_function); needs no GPU."""
+    lib = load_library()
+    lam = np.empty(nxp)
+    f = SgpuFringe(fstart, fend, frise, ffall, fmax, xsc)
+    rc = lib.sgpu_fringe_function(ctypes.byref(f), int(nxp), float(xl), _dp(lam))
+    if rc != 0:
+        raise SimsonError(f"sgpu_fringe_function: {lib.sgpu_error_string(rc).decode()} ({rc})", rc)
+    return lam
+
+
+def base_flow(fltype, nyp, nxp):
+    """Base flow of a channel flow type as bla/cbflow.f:117-155 builds it:
+    Poiseuille 1 - y^2 (fltype 1, 4) or Couette y (2, 5) in u, zero v and w,
+    on the Gauss-Lobatto points y_j = cos(pi j/(nyp-1)).  Returns bu1, bu2 of
+    shape (3, nyp, nxp/2+1) (the reference's (nxp/2+1, nyp, 3) array); the
+    last x row is zero (bflow.f fills it with the periodic point)."""
+    eta = np.cos(np.pi * np.arange(nyp) / (nyp - 1))
+    if fltype in (1, 4):
+        prof = 1.0 - eta ** 2
+    elif fltype in (2, 5):
+        prof = eta.copy()
+    else:
+        raise ValueError(f"flow type {fltype}: only the channel base flows (1, 2, 4, 5)")
+    bu = np.zeros((3, nyp, nxp // 2 + 1))
+    bu[0, :, :nxp // 2] = prof[:, None]
+    return bu, bu.copy()
+
+
+def base_flow_from_fields(u, v, w, nxp, nyp=None, u0low=0.0, w0low=0.0):
+    """Base flow read from a velocity field, as bla/rbflow.f does for rbfl:
+    the kz = 0 plane of u, v, w (complex (nz, nyp, nx/2), e.g. from
+    simson_b200.ufile.read_u), the lower-wall values of u and w moved to
+    u0low, w0low (rbflow.f:157-160), synthesised in x on the nxp-point grid
+    (the spectrum zero-padded beyond nx/2; real part of kx = 0, as the real
+    inverse transform of bla/cvecfft_acc.f takes it).  Returns bu1, bu2 as
+    base_flow does."""
+    fields = [np.asarray(q)[0] for q in (u, v, w)]  # (nyp, nx/2)
+    nyp_f, nx2 = fields[0].shape
+    if nyp is not None and nyp != nyp_f:
+        raise ValueError("the base flow needs the field's y resolution (read it with varsiz)")
+    spec = np.zeros((3, nyp_f, nxp // 2 + 1), np.complex128)
+    for i, q in enumerate(fields):
+        spec[i, :, :nx2] = q
+    spec[0, :, 0] += u0low - spec[0, -1, 0].real
+    spec[2, :, 0] += w0low - spec[2, -1, 0].real
+    spec[:, :, 0] = spec[:, :, 0].real
+    phys = np.fft.irfft(spec, n=nxp, axis=2) * nxp  # sum over +-kx, unnormalised
+    bu1 = np.zeros((3, nyp_f, nxp // 2 + 1))
+    bu2 = np.zeros_like(bu1)
+    bu1[:, :, :nxp // 2] = phys[:, :, 0::2]
+    bu2[:, :, :nxp // 2] = phys[:, :, 1::2]
+    return bu1, bu2
 
 
 class Channel:
@@ -320,6 +386,24 @@ class Channel:
         the download run at full PCIe speed)."""
         dp = ctypes.POINTER(ctypes.c_double)
         self._check(self.lib.sgpu_pressure(self._ctx, ctypes.cast(re_ptr, dp), ctypes.cast(im_ptr, dp)), "pressure")
+
+    def set_fringe(self, fstart, fend, frise, ffall, fmax, xsc=0.0):
+        """Fringe forcing of a spatial run (bla/fring.f) from now on; fmax = 0
+        turns it off."""
+        f = SgpuFringe(fstart, fend, frise, ffall, fmax, xsc)
+        self._check(self.lib.sgpu_set_fringe(self._ctx, ctypes.byref(f)), "set_fringe")
+
+    def set_base_flow(self, bu1=None, bu2=None):
+        """Base flow the fringe damps towards: bu1, bu2 of shape (3, nyp,
+        nxp/2+1) as base_flow returns them; None: zero."""
+        if bu1 is None:
+            self._check(self.lib.sgpu_set_base_flow(self._ctx, None, None), "set_base_flow")
+            return
+        b1 = np.ascontiguousarray(bu1, np.float64)
+        b2 = np.ascontiguousarray(bu2, np.float64)
+        if b1.shape != b2.shape or b1.shape[0] != 3 or b1.shape[1] != self.ny:
+            raise ValueError("base flow arrays of shape (3, nyp, nxp/2+1)")
+        self._check(self.lib.sgpu_set_base_flow(self._ctx, _dp(b1), _dp(b2)), "set_base_flow")
 
     def set_les(self, cutoff_inv=1.5, iord=5, chi=0.2, ihighorder=2, iles=1, cs=0.0, ineg=1):
         """Large-eddy model (defaults of bla/rparamles.f): iles 1 ADM-RT, 2 eddy

@@ -19,7 +19,8 @@ Reading rules of the reference:
   ``dtmax``, ``cflmax``).
 
 Options whose physics this library does not implement (perturbation mode,
-spatial simulations, suction, localized forcing, trips, wall roughness or
+forcing in the fringe other than the damping to the base flow, tabulated
+free-stream velocities, suction, localized forcing, trips, wall roughness or
 jets, MHD, SFD, scalars, two-point correlations, time series) are reported by
 :func:`unsupported` or, where the records that follow them are not read
 here, stop the reading with DeckError naming the option.
@@ -129,6 +130,16 @@ class BlaInput:
     gall: bool = False
     suction: bool = False
     spat: bool = False
+    tabfre: bool = False
+    rbfl: bool = False
+    nambfl: str = ""
+    fmax: float = 0.0
+    fstart: float = 0.0
+    fend: float = 0.0
+    frise: float = 0.0
+    ffall: float = 0.0
+    ampob: float = 0.0
+    amp2d: float = 0.0
     cdev: float = 0.0
     sgs: bool = False
     isfd: int = 0
@@ -223,8 +234,31 @@ def read_bla_i(path, scalar=0, mxys=1) -> BlaInput:
             d.real()  # vsuc
     b.spat = d.logical()
     if b.spat:
-        raise DeckError("spatial simulations (spat): the fringe and the spatial base flow are not built")
-    if not b.suction:
+        # rparambl.f:547-686: base flow source, fringe, forcing in the fringe
+        b.tabfre = d.logical()
+        if b.tabfre:
+            raise DeckError("tabulated free-stream velocity (tabfre) is not built")
+        b.rbfl = d.logical()
+        if b.rbfl:
+            b.nambfl = d.text()
+        b.fmax = d.real()
+        b.fstart = d.real()
+        b.fend = d.real()
+        b.frise = d.real()
+        b.ffall = d.real()
+        b.ampob = d.real()
+        b.amp2d = d.real()
+        if d.logical():
+            raise DeckError("Orr-Sommerfeld forcing in the fringe (osmod) is not built")
+        if d.logical():
+            raise DeckError("streak forcing in the fringe (streak) is not built")
+        if d.logical():
+            raise DeckError("waves in the fringe (waves) is not built")
+        # rparambl.f:1898-1912
+        if (b.fstart >= b.fend or b.frise <= 0.0 or b.ffall <= 0.0 or b.fmax <= 0.0
+                or abs(b.fstart) > 0.5 * b.xl or abs(b.fend) > 0.5 * b.xl):
+            raise DeckError("fmax, frise, ffall must be positive and fstart < fend in -xl/2 to xl/2")
+    elif not b.suction:
         b.cdev = d.real()
     b.sgs = d.logical()
     b.isfd = d.int()
@@ -371,7 +405,9 @@ def unsupported(b: BlaInput):
               (b.isfd != 0, "selective frequency damping (isfd)"), (b.imhd != 0, "MHD (imhd)"),
               (b.loctyp != 0, f"localized forcing loctyp = {b.loctyp}"), (b.tripf, "trip forcing"),
               (b.wbci != 0, f"wall boundary condition wbci = {b.wbci}"),
-              (not b.cflux, "constant Re_tau (cflux false)"), (b.longli, "y-dependent amplitude file (longli)"),
+              (b.ampob != 0.0 or b.amp2d != 0.0, "wave forcing in the fringe (ampob, amp2d)"),
+              (b.gall and b.spat, "Galilean transformation of a spatial run"),
+              (b.longli, "y-dependent amplitude file (longli)"),
               (b.iext > 0, "extremum file (iext)"), (b.mwave > 0, "wavenumber output (mwave)"),
               (b.npl > 0, "plane output (npl)")]
     return [what for bad, what in checks if bad]

@@ -29,4 +29,15 @@ struct Dims {
   int p0, p1;
 };
 
+// Fringe forcing of a spatial simulation (bla/fring.f without wave or streak
+// forcing): H -= lambda(x) (u - U_b(x, y)) for the three components, in
+// physical space after the products.  lam[nxp]: the fringe function at every
+// x point (bla/ffun.f; zero outside the fringe, where the reference applies
+// nothing); base[3][nyp][nxp]: the base flow u, v, w in physical space.
+// lam == nullptr: no fringe.
+struct Fringe {
+  const double* lam;
+  const double* base;
+};
+
 }  // namespace sb

@@ -18,8 +18,9 @@ void mixed_zinv(cudaStream_t s, dim3 grid, size_t smem, const float2* stf, float
 
 void mixed_xpass(cudaStream_t s, dim3 grid, size_t smem, const float2* zb, float2* xb, const Dims& g,
                  const FFTPlan& plan, const float2* tw, const double* dyi, double dxi, double dzi, double rot,
-                 unsigned long long* cfl, const double* meanp) {
-  launch_xpass<float, MIXED_RB, SB_FFT_THREADS>(grid, smem, s, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, meanp);
+                 unsigned long long* cfl, const double* meanp, Fringe fr) {
+  launch_xpass<float, MIXED_RB, SB_FFT_THREADS>(grid, smem, s, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, meanp,
+                                                fr);
 }
 
 void mixed_zfwd(cudaStream_t s, dim3 grid, size_t smem, const float2* xb, float2* stf, const Dims& g,

@@ -21,7 +21,7 @@ void mixed_zinv(cudaStream_t s, dim3 grid, size_t smem, const float2* stf, float
                 const FFTPlan& plan, const float2* tw, const double* alfa, const double* beta);
 void mixed_xpass(cudaStream_t s, dim3 grid, size_t smem, const float2* zb, float2* xb, const Dims& g,
                  const FFTPlan& plan, const float2* tw, const double* dyi, double dxi, double dzi, double rot,
-                 unsigned long long* cfl, const double* meanp);
+                 unsigned long long* cfl, const double* meanp, Fringe fr);
 void mixed_zfwd(cudaStream_t s, dim3 grid, size_t smem, const float2* xb, float2* stf, const Dims& g,
                 const FFTPlan& plan, const float2* tw, const double* meanp, double rot);
 void mixed_pencil_hom(cudaStream_t s, const PencilBufs& B, const Dims& g, const double* alfa, const double* beta,

@@ -183,7 +183,8 @@ extern "C" int sgpu_nonlin_noalloc(const sgpu_params* prm, const void* fields_in
   dim3 gx((g.nzp + RB - 1) / RB, g.nyp);
   const double dxi = (double)(g.nx - 2) / P.xl;
   const double dzi = (double)(g.nz - 2) / P.zl;
-  k_xpass<double, RB><<<gx, TH, s_x, st>>>(zb, xb, g, px, twx, dyi, dxi, dzi, P.rot, cfl_bits, nullptr);
+  k_xpass<double, RB><<<gx, TH, s_x, st>>>(zb, xb, g, px, twx, dyi, dxi, dzi, P.rot, cfl_bits, nullptr,
+                                          Fringe{nullptr, nullptr});
   k_zfwd<double, KB, double><<<gz, TH, s_z, st>>>(xb, out, g, pz, twz, nullptr, 0.0);
   if (cudaGetLastError() != cudaSuccess) return SGPU_E_CUDA;
   if (cflp_max) {

@@ -24,6 +24,7 @@
 #pragma once
 #include "fft.cuh"
 #include "layout.cuh"
+#include "step2.cuh"
 #include "step3.cuh"
 
 namespace sb {
@@ -33,8 +34,10 @@ namespace sb {
 // 2E; forward x FFT of (H1 + i H2) and (H3 + i 2E); the kx < nx/2 spectra of
 // H1, H2, H3, 2E written to fields 0..3 of the same row of zb (this CTA's own
 // row: every read of it is done before the first barrier).
+// fr: the fringe forcing of a spatial run, which the reference's pressure
+// includes as well (bla/fringp.f, the forcing of bla/fring.f on H).
 __global__ void __launch_bounds__(256) k_xpass_p(double2* __restrict__ zb, Dims g, FFTPlan plan,
-                                                 const double2* __restrict__ tw, double rot) {
+                                                 const double2* __restrict__ tw, double rot, Fringe fr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* bA = reinterpret_cast<double2*>(smem_raw);
   const int n = g.nxp;
@@ -66,9 +69,10 @@ __global__ void __launch_bounds__(256) k_xpass_p(double2* __restrict__ zb, Dims 
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     const double2 z0 = res[j * 3 + 0], z1 = res[j * 3 + 1], z2 = res[j * 3 + 2];
     const double u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
-    const double h1 = v * (oz + r2) - w * oy;
-    const double h2 = w * ox - u * (oz + r2);
-    const double h3 = u * oy - v * ox;
+    double h1 = v * (oz + r2) - w * oy;
+    double h2 = w * ox - u * (oz + r2);
+    double h3 = u * oy - v * ox;
+    if (fr.lam != nullptr) fringe_apply<double>(fr, j, y, g.nyp, n, u, v, w, h1, h2, h3);
     const double e2 = u * u + v * v + w * w;
     oth[j * 2 + 0] = double2{h1, h2};
     oth[j * 2 + 1] = double2{h3, e2};

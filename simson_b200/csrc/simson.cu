@@ -4,6 +4,7 @@
 // (bla/bla.f:1464-1478 first stage, 2382-2397 weights, 2598-2607 time).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -131,6 +132,12 @@ struct sgpu_ctx {
   bool press_valid = false;     // press belongs to the current state
   double* press_wd = nullptr;   // [2][nyp] second-derivative weights at y = +1, -1
   size_t box_n = 0;          // coarse points box_out holds
+  // spatial simulation (sgpu_set_fringe, sgpu_set_base_flow): the fringe
+  // function at the nxp x points and the base flow [3][nyp][nxp] in physical
+  // space, which the fringe damps towards
+  double* fr_lam = nullptr;
+  double* fr_base = nullptr;
+  bool fringe = false;
   // RK bookkeeping (host mirror of the reference driver scalars)
   double an = 0, bn = 0, anp1 = 0, bnp1 = 0, cnp1 = 0, dtn = 0, t = 0, tc = 0;
   // the next full step's time step (the reference's dtnp1, bla/bla.f:2358-2372),
@@ -186,6 +193,11 @@ static void prof_mark(sgpu_ctx* c, int id) {
   cudaEventRecord(c->pev[c->pnext], c->stream);
   c->pid[c->pnext] = id;
   c->pnext++;
+}
+
+// the fringe arguments of the x passes (none unless sgpu_set_fringe enabled it)
+static Fringe ctx_fringe(const sgpu_ctx* c) {
+  return c->fringe ? Fringe{c->fr_lam, c->fr_base} : Fringe{nullptr, nullptr};
 }
 
 static int cuda_fail(cudaError_t e, const char* where) {
@@ -454,7 +466,8 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
                   c->sgs_delta2, c->sgs_twz.d, c->sgs_twz.f, c->sgs_twx.d, c->sgs_twx.f, c->xys, c->xys_spec,
                   c->xys_part, c->xys_u, c->box_out, c->press, c->press_wd, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->sgs_flags, c->sgs_bsums, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
-                  c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f};
+                  c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f,
+                  c->fr_lam, c->fr_base};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 16; ++i)
@@ -874,7 +887,8 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     mixed_mean_profiles(c->stream, c->stf, c->meanp, g);
     mixed_zinv(c->stream, gzf, s_zf, c->stf, zbf, g, c->twz.plan, c->twz.f, c->alfa, c->beta);
     prof_mark(c, K_XPASS);
-    mixed_xpass(c->stream, gxf, s_xf, zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp);
+    mixed_xpass(c->stream, gxf, s_xf, zbf, xbf, g, c->twx.plan, c->twx.f, c->dyi, dxi, dzi, P.rot, cflp, c->meanp,
+                ctx_fringe(c));
     prof_mark(c, K_ZFWD);
     mixed_zfwd(c->stream, gzf, s_zf, xbf, c->stf, g, c->twz.plan, c->twz.f, c->meanp, P.rot);
     c->launches++;
@@ -885,7 +899,8 @@ static int enqueue_nonlin(sgpu_ctx* c) {
     dim3 gx((g.nzp + c->rb - 1) / c->rb, nyl);
     prof_mark(c, K_XPASS);
     launch_xpass<double, sgpu_ctx::rb, sgpu_ctx::xpass64_threads>(gx, s_x, c->stream, c->zb, c->xb, g, c->twx.plan,
-                                                                  c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr);
+                                                                  c->twx.d, c->dyi, dxi, dzi, P.rot, cflp, nullptr,
+                                                                  ctx_fringe(c));
     prof_mark(c, K_ZFWD);
     launch_zfwd<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->xb, c->st, g, c->twz.plan, c->twz.d, nullptr,
                                               0.0);
@@ -1081,7 +1096,7 @@ extern "C" int sgpu_cfl_rate(sgpu_ctx* c, double* rate) {
     mixed_zinv(c->stream, gzf, smem_fft(g.nzp, sgpu_ctx::kbf, sizeof(float2)), c->stf, zbf, g, c->twz.plan, c->twz.f,
                c->alfa, c->beta);
     mixed_xpass(c->stream, gxf, smem_fft(g.nxp, 3 * sgpu_ctx::rbf, sizeof(float2)), zbf, xbf, g, c->twx.plan,
-                c->twx.f, c->dyi, dxi, dzi, P.rot, c->cfl_bits, c->meanp);
+                c->twx.f, c->dyi, dxi, dzi, P.rot, c->cfl_bits, c->meanp, Fringe{nullptr, nullptr});
   } else {
     dim3 gz((g.nx2 + c->kb - 1) / c->kb, nyl);
     dim3 gx((g.nzp + c->rb - 1) / c->rb, nyl);
@@ -1089,7 +1104,8 @@ extern "C" int sgpu_cfl_rate(sgpu_ctx* c, double* rate) {
                                               g, c->twz.plan, c->twz.d, c->alfa, c->beta, 0);
     launch_xpass<double, sgpu_ctx::rb, sgpu_ctx::xpass64_threads>(gx, smem_fft(g.nxp, 3 * c->rb, sizeof(double2)),
                                                                   c->stream, c->zb, c->xb, g, c->twx.plan, c->twx.d,
-                                                                  c->dyi, dxi, dzi, P.rot, c->cfl_bits, nullptr);
+                                                                  c->dyi, dxi, dzi, P.rot, c->cfl_bits, nullptr,
+                                                                  Fringe{nullptr, nullptr});
   }
   c->launches += c->mixed ? 4 : 3;
   CK(cudaGetLastError());
@@ -1136,14 +1152,15 @@ extern "C" int sgpu_cfl_set_global(sgpu_ctx* c, double cflp) {
 }
 
 // Launch pattern of the RK step that starts now: bits 0-3 the substeps that
-// evaluate the CFL number, bits 4-7 the LES mode, bit 8 the pencil kernel.
+// evaluate the CFL number, bits 4-7 the LES mode, bit 8 the pencil kernel,
+// bit 9 the fringe.
 // 0xffffffff: the step cannot be replayed (not at a step boundary, its time
 // step changes at its end, or a stage's homogeneous solutions not yet
 // cached: that substep launches k_pencil_hom).
 static unsigned step_pattern(const sgpu_ctx* c) {
   const int nst = c->prm.nst;
   if ((c->it - 1) % nst != 0 || c->dt_next != c->dtn) return 0xffffffffu;
-  unsigned key = ((unsigned)c->iles << 4) | ((c->pencil_warp ? 1u : 0u) << 8);
+  unsigned key = ((unsigned)c->iles << 4) | ((c->pencil_warp ? 1u : 0u) << 8) | ((c->fringe ? 1u : 0u) << 9);
   double anp1 = c->anp1, bnp1 = c->bnp1;
   for (int s = 0; s < nst; ++s) {
     const int it = c->it + s;
@@ -1626,7 +1643,7 @@ extern "C" int sgpu_pressure(sgpu_ctx* c, double* pr, double* pi) {
                                               c->alfa, c->beta, 0);
   const size_t s_xp = 2 * (size_t)g.nxp * 3 * sizeof(double2);
   cudaFuncSetAttribute(k_xpass_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_xp);
-  k_xpass_p<<<dim3(g.nzp, n), 256, s_xp, c->stream>>>(c->zb, g, c->twx.plan, c->twx.d, P.rot);
+  k_xpass_p<<<dim3(g.nzp, n), 256, s_xp, c->stream>>>(c->zb, g, c->twx.plan, c->twx.d, P.rot, ctx_fringe(c));
   const size_t fz = (size_t)n * g.nzp * g.nx2;  // one field of zb
   launch_zfwd<double, sgpu_ctx::kb, double>(gz, s_z, c->stream, c->zb, czf(c, 0), g, c->twz.plan, c->twz.d,
                                             nullptr, 0.0);  // H1, H2, H3
@@ -1841,6 +1858,123 @@ static int sgs_setup(sgpu_ctx* c) {
 
 // ADM-RT large-eddy model (bla/rparamles.f, bla/bla.f:1489-1518, 2212-2231):
 // filter tables on the host (les_filter.h), gu and the tables on the device.
+// ---------------------------------------------------------------------------
+// Spatial simulation: fringe forcing towards a base flow (bla/fring.f,
+// bla/ffun.f; the base flow of bla/bflow.f is computed by the caller)
+// ---------------------------------------------------------------------------
+// Smooth step of bla/step.f: 0 up to 0.02, 1 above 0.98,
+// 1 / (1 + exp(1/(x - 1) + 1/x)) between.
+static double fringe_step(double x) {
+  if (x <= 0.02) return 0.0;
+  if (x <= 0.98) return 1.0 / (1.0 + exp(1.0 / (x - 1.0) + 1.0 / x));
+  return 1.0;
+}
+
+// The fringe function of bla/ffun.f at the nxp physical x points (x pair k of
+// the reference, fring1(k) / fring2(k), is points 2k-2 and 2k-1 here): fmax
+// (S((x - fstart)/frise) - S((x - fend)/ffall + 1)) over the x range the
+// reference fills (the fringe start and end mapped into the box around xsc;
+// a fringe across the box end is filled in two parts with fmax added), zero
+// elsewhere.
+extern "C" int sgpu_fringe_function(const sgpu_fringe* f, int nxp, double xl, double* lam) {
+  if (!f || !lam || nxp < 2 || (nxp & 1) || !(xl > 0.0) || !(f->frise > 0.0) || !(f->ffall > 0.0))
+    return SGPU_E_PARAM;
+  for (int j = 0; j < nxp; ++j) lam[j] = 0.0;
+  const double r = 0.499999999999999999;  // rounding offset of the int() below, as bla/ffun.f declares it
+  const double dnx = xl / (double)nxp;
+  const double fstc = f->fstart + (double)(long long)((f->xsc - f->fstart) / xl + r) * xl;
+  const double fenc = f->fend + (double)(long long)((f->xsc - f->fend) / xl + r) * xl;
+  const int nh = nxp / 2;
+  const int xstart = (int)((double)nh * (fstc - f->xsc + xl / 2.0) / xl) + 1;
+  const int xend = (int)((double)nh * (fenc - f->xsc + xl / 2.0) / xl) + 1;
+  const bool wrap = xstart > xend;  // the fringe crosses the box end: two ranges
+  for (int i = wrap ? 0 : 1; i <= 1; ++i) {
+    const int xst = (i == 0) ? 1 : xstart;
+    const int xen = std::max(xend, (i == 0) ? 1 : (wrap ? nh : 1));
+    if (xst < 1 || xen > nh) return SGPU_E_PARAM;  // outside the box: the reference would index past fring1
+    for (int x = xst; x <= xen; ++x) {
+      const double xc1 = (double)(2 * x - 1 - nh - 1) * dnx + f->xsc;
+      double f1 = f->fmax * (fringe_step((xc1 - fstc) / f->frise) - fringe_step((xc1 - fenc) / f->ffall + 1.0));
+      const double xc2 = xc1 + dnx;
+      double f2 = f->fmax * (fringe_step((xc2 - fstc) / f->frise) - fringe_step((xc2 - fenc) / f->ffall + 1.0));
+      if (wrap) {
+        f1 = f1 + f->fmax;
+        f2 = f2 + f->fmax;
+      }
+      lam[2 * (x - 1)] = f1;
+      lam[2 * (x - 1) + 1] = f2;
+    }
+  }
+  return SGPU_OK;
+}
+
+static int fringe_alloc(sgpu_ctx* c) {
+  const Dims& g = c->g;
+  const size_t nb = 3 * (size_t)g.nyp * g.nxp;
+  if (!c->fr_lam && cudaMalloc(&c->fr_lam, (size_t)g.nxp * sizeof(double)) != cudaSuccess) {
+    c->fr_lam = nullptr;
+    return SGPU_E_CUDA;
+  }
+  if (!c->fr_base) {
+    if (cudaMalloc(&c->fr_base, nb * sizeof(double)) != cudaSuccess) {
+      c->fr_base = nullptr;
+      return SGPU_E_CUDA;
+    }
+    CK(cudaMemsetAsync(c->fr_base, 0, nb * sizeof(double), c->stream));
+  }
+  return SGPU_OK;
+}
+
+extern "C" int sgpu_set_fringe(sgpu_ctx* c, const sgpu_fringe* f) {
+  if (!c) return SGPU_E_PARAM;
+  c->step_valid = false;   // the captured step no longer matches
+  c->press_valid = false;  // the pressure includes the fringe force
+  if (!f || f->fmax == 0.0) {
+    c->fringe = false;
+    return SGPU_OK;
+  }
+  if (!(f->fmax > 0.0)) return SGPU_E_PARAM;
+  const Dims& g = c->g;
+  std::vector<double> lam((size_t)g.nxp);
+  int r = sgpu_fringe_function(f, g.nxp, c->prm.xl, lam.data());
+  if (r) return r;
+  r = fringe_alloc(c);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->fr_lam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->fringe = true;
+  return SGPU_OK;
+}
+
+// bu1, bu2(nxp/2+1, nyp, 3) of the reference (bla/bflow.f): the base flow
+// u, v, w in physical space at the even (bu1) and odd (bu2) x points.
+extern "C" int sgpu_set_base_flow(sgpu_ctx* c, const double* bu1, const double* bu2) {
+  if (!c || (bu1 == nullptr) != (bu2 == nullptr)) return SGPU_E_PARAM;
+  c->press_valid = false;
+  const Dims& g = c->g;
+  int r = fringe_alloc(c);
+  if (r) return r;
+  const size_t nb = 3 * (size_t)g.nyp * g.nxp;
+  if (!bu1) {
+    CK(cudaMemsetAsync(c->fr_base, 0, nb * sizeof(double), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SGPU_OK;
+  }
+  const int nh = g.nxp / 2, ld = nh + 1;  // leading dimension nxp/2+1
+  std::vector<double> b(nb);
+  for (int i = 0; i < 3; ++i)
+    for (int y = 0; y < g.nyp; ++y)
+      for (int x = 0; x < nh; ++x) {
+        const size_t src = (size_t)x + (size_t)ld * ((size_t)y + (size_t)g.nyp * i);
+        double* row = b.data() + ((size_t)i * g.nyp + y) * g.nxp;
+        row[2 * x] = bu1[src];
+        row[2 * x + 1] = bu2[src];
+      }
+  CK(cudaMemcpyAsync(c->fr_base, b.data(), nb * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SGPU_OK;
+}
+
 extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
   if (c) c->step_valid = false;  // the captured step no longer matches
   if (c && sharded(c) && p && p->iles != 0) return SGPU_E_PARAM;  // LES needs the whole domain

@@ -104,12 +104,27 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// H -= lambda (u - U_b) at x point j of plane y; u, v, w are totals.
+template <class T>
+__device__ __forceinline__ void fringe_apply(const Fringe& fr, int j, int y, int nyp, int n, T u, T v, T w, T& h1,
+                                             T& h2, T& h3) {
+  const double lm = fr.lam[j];
+  if (lm == 0.0) return;
+  const size_t cs = (size_t)nyp * n;  // one component of the base flow
+  const double* b = fr.base + (size_t)y * n + j;
+  const T l = (T)lm;
+  h1 = h1 - l * (u - (T)b[0]);
+  h2 = h2 - l * (v - (T)b[cs]);
+  h3 = h3 - l * (w - (T)b[2 * cs]);
+}
+
 // N > 0: the x length g.nxp is N (compile-time plan, NT threads per CTA).
 template <class T, int RB, int N = 0, int NT = 0>
 __global__ void __launch_bounds__(NT > 0 ? NT : 256)
     k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb, Dims g,
             FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ dyi, double dxi,
-            double dzi, double rot, unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean) {
+            double dzi, double rot, unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean,
+            Fringe fr) {
   typedef typename C2<T>::type V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int B = 3 * RB;
@@ -191,6 +206,8 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
       h2 = (W * ox + w * Ox - U * oz - u * Oz) + (w * ox - u * oz);
       h3 = U * oy - v * Ox + (u * oy - v * ox);
     }
+    // fringe on the total velocity (U = W = 0 on the FP64 path, so u + U = u)
+    if (fr.lam != nullptr) fringe_apply<T>(fr, j, y, g.nyp, n, u + U, v, w + W, h1, h2, h3);
     if constexpr (RB % 2 == 0) {
       oth[j * B2 + r] = V{h1, h2};
       T* h3p = reinterpret_cast<T*>(&oth[j * B2 + RB + r / 2]);

@@ -78,25 +78,25 @@ template <class T, int RB, int N, int NT>
 inline void xpass_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
                     typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan, const typename C2<T>::type* tw,
                     const double* dyi, double dxi, double dzi, double rot, unsigned long long* cfl,
-                    const double* mean) {
+                    const double* mean, Fringe fr) {
   cudaFuncSetAttribute(k_xpass<T, RB, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_xpass<T, RB, N, NT><<<grid, NT, smem, st>>>(zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
+  k_xpass<T, RB, N, NT><<<grid, NT, smem, st>>>(zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean, fr);
 }
 template <class T, int RB, int NT0>
 inline void launch_xpass(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T>::type* zb,
                          typename C2<T>::type* xb, const Dims& g, const FFTPlan& plan,
                          const typename C2<T>::type* tw, const double* dyi, double dxi, double dzi, double rot,
-                         unsigned long long* cfl, const double* mean) {
+                         unsigned long long* cfl, const double* mean, Fringe fr) {
   switch (g.nxp) {
 #define SB_CASE(n)                                                                                        \
   case n:                                                                                                 \
     xpass_n<T, RB, n, fixed_threads(n, 3 * RB)>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, \
-                                                mean);                                                    \
+                                                mean, fr);                                                \
     return;
     SB_FIXED_LENGTHS(SB_CASE)
 #undef SB_CASE
     default:
-      xpass_n<T, RB, 0, NT0>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean);
+      xpass_n<T, RB, 0, NT0>(grid, smem, st, zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean, fr);
   }
 }
 

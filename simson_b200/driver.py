@@ -5,9 +5,15 @@ writes what the reference writes for such a run:
 
 * start (bla/bla.f:960-1082, 1405-1478, 1562-1662): the field of namnin
   (bla/rdiscbl.f through simson_b200.ufile; re, xl, zl and t come from the
-  file, as they do for a temporal run), the first time step (dt > 0 as
-  given; dt <= 0: cflmax over the field's CFL rate, bla/getdt.f, bounded by
-  dtmax), the LES model of sgs.i, prhs;
+  file, as they do for a temporal run), the pressure gradient of the flow
+  type (bla/bla.f:1622-1661: fltype 1 drives with the constant flux 4/3 or
+  px = -(Re_tau/Re)^2, every other flow type has px = 0), for a spatial run
+  (spat) the base flow (bla/bflow.f: bla/cbflow.f's Poiseuille or Couette
+  profile, or the field of nambfl read as bla/rbflow.f does), the fringe
+  (bla/ffun.f, bla/fring.f) and its time-step bound (bla/bla.f:1418-1431),
+  the first time step (dt > 0 as given; dt <= 0: cflmax over the field's CFL
+  rate, bla/getdt.f; either bounded by dtmax, bla/bla.f:1467), the LES model
+  of sgs.i, prhs;
 * every full step (nst substeps): with a variable time step, the next step's
   dt after the step's CFL evaluation, by the rule of bla/bla.f:2355-2380
   (cfl/cflmax above 10/9: dt cflmax/cfl, else dt (0.8 + 0.2 cflmax/cfl);
@@ -36,7 +42,7 @@ import os
 import time
 
 from . import blai, ufile
-from .bla import FP64, MIXED, Channel
+from .bla import FP64, MIXED, Channel, base_flow, base_flow_from_fields
 
 
 def fortran_e(v, w=25, d=16, e=3):
@@ -91,13 +97,22 @@ def run(deck_dir, grid=None, precision="fp64", device=0, max_steps=None, log=pri
         raise blai.DeckError(f"iamp = {b.iamp} is not a multiple of nst = {b.nst}")
     init = blai.deck_path(deck_dir, b.namnin)
     head = ufile.read_header(init)
-    if head["fltype"] not in (1, 2):
-        raise blai.DeckError(f"flow type {head['fltype']}: this library steps the channel (fltype 1)")
+    fltype = head["fltype"]
+    if fltype not in (1, 2, 4, 5) or (b.spat and fltype not in (4, 5)):
+        raise blai.DeckError(f"flow type {fltype}" + (" in a spatial run" if b.spat else "") +
+                             ": this library steps the channel (fltype 1, 2; spatial 4, 5)")
     nx, ny, nz = grid or (head["nx"], head["nyp"], head["nzc"])
     _, fields = ufile.read_u(init, m=3, nx=nx, nyp=ny, nz=nz, varsiz=b.varsiz)
     re, xl, zl, t0 = head["re"], head["xl"], head["zl"], head["t"]
     nst = b.nst
-    ch = Channel(nx, ny, nz, re, xl, zl, b.dt if b.dt > 0 else 1.0, cflux=b.cflux, icfl=b.icfl, nst=nst,
+    # pressure gradient (bla/bla.f:1622-1661)
+    cflux = b.cflux and fltype == 1
+    px = (-2.0 / re) if cflux else (-(b.retau / re) ** 2 if fltype == 1 else 0.0)
+    dtmax = b.dtmax
+    if b.spat:  # the fringe's bound on the time step (bla/bla.f:1418-1431)
+        dtmax = min(dtmax, (1.75 if nst == 3 else 1.96) / b.fmax)
+    dt0 = min(b.dt, dtmax) if b.dt > 0 else 1.0
+    ch = Channel(nx, ny, nz, re, xl, zl, dt0, cflux=cflux, px=px, icfl=b.icfl, nst=nst,
                  rot=b.rot, precision=MIXED if precision == "mixed" else FP64, device=device)
     written = []
     wall0, cpu0 = time.time(), time.process_time()
@@ -105,10 +120,18 @@ def run(deck_dir, grid=None, precision="fp64", device=0, max_steps=None, log=pri
         if les is not None and les.iles:
             ch.set_les(iles=les.iles, cutoff_inv=les.cutoff_inv, iord=les.iord, chi=les.chi, cs=les.cs,
                        ineg=les.ineg)
+        if b.spat:
+            nxp = 3 * nx // 2
+            if b.rbfl:
+                _, bf = ufile.read_u(blai.deck_path(deck_dir, b.nambfl), m=3, nx=nx, nyp=ny, nz=nz, varsiz=True)
+                ch.set_base_flow(*base_flow_from_fields(*bf, nxp=nxp))
+            else:
+                ch.set_base_flow(*base_flow(fltype, ny, nxp))
+            ch.set_fringe(b.fstart, b.fend, b.frise, b.ffall, b.fmax)
         ch.set_velocity(*fields)
-        dtn = b.dt
+        dtn = dt0
         if b.vart:
-            dtn = min(b.cflmax / ch.cfl_rate(), b.dtmax)  # getdt, then bla/bla.f:1467
+            dtn = min(b.cflmax / ch.cfl_rate(), dtmax)  # getdt, then bla/bla.f:1467
             ch.set_dt(dtn)
             log(f"First time step      : {dtn}")
         ch.prhs()
@@ -132,7 +155,7 @@ def run(deck_dir, grid=None, precision="fp64", device=0, max_steps=None, log=pri
                 if b.vart:
                     ch.substeps(nst - 1)
                     sc = ch.scalars()  # the CFL of this step's first substep; stops as wcflbl.f:93
-                    dtnp1 = next_dt(dtn, sc["cfl"], b.cflmax, b.dtmax, t, tsave[isave], b.tmax)
+                    dtnp1 = next_dt(dtn, sc["cfl"], b.cflmax, dtmax, t, tsave[isave], b.tmax)
                     ch.set_dt(dtnp1)
                     ch.substeps(1)
                     dtn = dtnp1

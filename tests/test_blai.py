@@ -52,7 +52,22 @@ def test_fixed_and_bounded_time_steps(tmp_path):
 def test_constant_re_tau_branch_reads_retau(tmp_path):
     b = blai.read_bla_i(write(tmp_path, "bla.i", bla_i(cflux=False, retau=395.0)))
     assert not b.cflux and b.retau == 395.0
-    assert "constant Re_tau (cflux false)" in blai.unsupported(b)
+    assert blai.unsupported(b) == []  # px = -(Re_tau/Re)^2 (bla/bla.f:1645)
+
+
+def test_spatial_deck_records(tmp_path):
+    b = blai.read_bla_i(write(tmp_path, "bla.i", bla_i(spat=True, cflux=False, retau=0.0, rbfl="baseflow.u",
+                                                       xl=48.0, fringe=(2.0, -10.0, -1.0, 5.0, 2.0))))
+    assert b.spat and b.rbfl and b.nambfl == "baseflow.u" and not b.tabfre
+    assert (b.fmax, b.fstart, b.fend, b.frise, b.ffall) == (2.0, -10.0, -1.0, 5.0, 2.0)
+    assert b.cdev == 0.0 and blai.unsupported(b) == []
+    b = blai.read_bla_i(write(tmp_path, "w.i", bla_i(spat=True, xl=48.0, ampob=0.1)))
+    assert "wave forcing in the fringe (ampob, amp2d)" in blai.unsupported(b)
+    # rparambl.f:1898-1912: fstart < fend inside the box, positive distances and strength
+    for bad in ((1.0, 0.0, -13.0, 7.0, 3.0), (0.0, -13.0, 0.0, 7.0, 3.0), (1.0, -13.0, 0.0, -7.0, 3.0),
+                (1.0, -13.0, 7.0, 7.0, 3.0)):
+        with pytest.raises(blai.DeckError, match="fstart < fend"):
+            blai.read_bla_i(write(tmp_path, "f.i", bla_i(spat=True, xl=12.0, fringe=bad)))
 
 
 def test_rejected_decks(tmp_path):
@@ -85,6 +100,18 @@ def test_reference_example_decks(example):
     assert blai.unsupported(b) == []
     s = blai.read_sgs_i(os.path.join(REF, "examples", "spatial-blasius-les", "sgs.i"))
     assert (s.iles, s.cutoff_inv, s.iord, s.chi) == (1, 1.5, 5, 0.2)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "examples")), reason="reference sources not present")
+def test_reference_spatial_example_decks():
+    b = blai.read_bla_i(os.path.join(REF, "examples", "spatial-channel-couette", "bla.i"))
+    assert b.spat and b.rbfl and b.nambfl == "baseflow.u" and not b.cflux and b.nst == 4
+    assert (b.fmax, b.fstart, b.fend, b.frise, b.ffall) == (1.0, -13.0, 0.0, 7.0, 3.0)
+    assert blai.unsupported(b) == []
+    b = blai.read_bla_i(os.path.join(REF, "examples", "spatial-blasius-les", "bla.i"))
+    assert b.spat and b.fstart == -70.0 and b.sgs
+    bad = blai.unsupported(b)
+    assert "boundary condition ibc = 110" in bad and "trip forcing" in bad
 
 
 def test_amp_stat_number_format():

@@ -60,3 +60,44 @@ def test_driver_four_stage_channel_deck(tmp_path, need_ref, dt):
     lines = (tmp_path / "amp.stat").read_text().splitlines()
     assert len(lines) == steps // 2 and all(len(ln.split()) == 19 for ln in lines)
     assert os.path.exists(tmp_path / "t1.u")
+
+
+SX, SY, SZ, SXL, SRE = 32, 33, 16, 48.0, 2000.0
+FR = (1.0, -13.0, 0.0, 7.0, 3.0)  # fmax, fstart, fend, frise, ffall
+
+
+@pytest.mark.parametrize("rbfl", [False, True])
+def test_driver_spatial_channel_deck(tmp_path, need_ref, rbfl):
+    """A spatial deck (spat, the fringe of the reference's spatial-channel
+    example, fltype 4 in the initial field, cflux off, RK4 with the variable
+    time step under the fringe's bound 1.96/fmax), the base flow computed or
+    read from a file (rbfl), against the reference run with its own bflow and
+    ffun."""
+    from refsim import RefSim
+    from simson_b200 import driver, ufile
+    need_ref(SX, SY, SZ)
+    steps = 6
+    u, v, w = channel_field(SX, SY, SZ, SXL, ZL, 0.05, 31)
+    ufile.write_u(str(tmp_path / "init.u"), [u, v, w], SRE, SXL, ZL, 0.0, fltype=4)
+    if rbfl:  # the Poiseuille base flow as a field file
+        y = np.cos(np.pi * np.arange(SY) / (SY - 1))
+        b = np.zeros((SZ, SY, SX // 2), complex)
+        b[0, :, 0] = 1.0 - y ** 2
+        ufile.write_u(str(tmp_path / "baseflow.u"), [b, 0 * b, 0 * b], SRE, SXL, ZL, 0.0, fltype=4)
+    (tmp_path / "bla.i").write_text(bla_i(xl=SXL, dt=0.0, nst=4, maxit=4 * steps, icfl=4, cflux=False, retau=0.0,
+                                          spat=True, rbfl="baseflow.u" if rbfl else None, fringe=FR))
+    res = driver.run(str(tmp_path), log=lambda *a: None)
+    assert res["steps"] == steps and res["px"] == 0.0
+    head, got = ufile.read_u(str(tmp_path / "end.u"))
+    ref = RefSim(SX, SY, SZ, SRE, SXL, ZL, -1.96 / FR[0], cflux=False, nst=4, cflmaxin=0.8)
+    ref.set_spatial(4, FR[1], FR[2], FR[3], FR[4], FR[0])
+    ref.set_velocity(u, v, w)
+    ref.start()
+    ref.step(steps)
+    want, sc = ref.state()[:3], ref.scalars()
+    errs = [rel(got[k], want[k]) for k in range(3)]
+    print("spatial driver (rbfl %s) vs reference:" % rbfl, ["%.2e" % e for e in errs],
+          "t %.15f / %.15f" % (head["t"], sc["t"]))
+    assert max(errs) <= 1e-10, errs
+    assert abs(head["t"] - sc["t"]) <= 1e-12 * max(1.0, sc["t"])
+    assert abs(res["dt"] - sc["dtn"]) <= 1e-12 * sc["dtn"]
