@@ -110,7 +110,8 @@ int sgpu_get_scalars(sgpu_ctx* ctx, double* out, int n);
 
 /* Large-eddy model, the reference's sgs.i (bla/rparamles.f:31-60):
  *   iles        0 none, 1 ADM-RT (approximate deconvolution, relaxation term),
- *               2 eddy viscosity (Smagorinsky; dynamic when cs = 0)
+ *               2 eddy viscosity (Smagorinsky; dynamic when cs = 0),
+ *               3 HPF eddy viscosity (Smagorinsky on the high-pass filtered field)
  *   cutoff_inv  1 / cut-off wavenumber fraction of the primary filter (1.5)
  *   iord        order N of the deconvolution, 0..5 (5)
  *   chi         relaxation coefficient (0.2)
@@ -135,11 +136,18 @@ typedef struct {
  * iles = 2: every substep starts with the SGS stress of bla/les.f and its
  *   divergence (bla/sgs_stress.f, the loops of bla/bla.f:1945-2020); step 2
  *   adds -sigma (bla/nonlinbl.f:1011-1048).  Needs nx, nz divisible by 4.
- * iles = 3 (HPF eddy viscosity) is rejected with SGPU_E_PARAM. */
+ * iles = 3: the high-pass filter of iles = 1 applied to u, v, w, omega_x,
+ *   omega_z after prhs and every step 3 (bla/prhs.f, bla/linearbl.f:
+ *   1871-2060), and every substep the eddy-viscosity stress of iles = 2
+ *   formed with the strain of the filtered field (bla/les.f:404-450,
+ *   883-966), cs > 0 fixed (ineg = 1).  The dynamic HPF procedure (cs = 0,
+ *   bla/les.f:968-1383 with the secondary filter of bla/bla.f:1520-1545)
+ *   is rejected with SGPU_E_PARAM. */
 int sgpu_set_les(sgpu_ctx* ctx, const sgpu_les_params* p);
 
-/* gur, gui(memnx, memny, memnz, 1..3): the filtered velocities (iles = 1) or
- * the SGS force sigma (iles = 2). */
+/* gur, gui(memnx, memny, memnz, 1..3): the filtered velocities (iles = 1, and
+ * iles = 3 after sgpu_prhs or a step 3) or the SGS force sigma (iles = 2, 3
+ * after a step 2). */
 int sgpu_download_les(sgpu_ctx* ctx, double* gr, double* gi);
 
 /* taur, taui(memnx, memny, memnz, 1..6) (iles = 2): the SGS stress of the

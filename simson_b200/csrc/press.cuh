@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) k_xpass_p(double2* __restrict__ zb, Dims 
     double h1 = v * (oz + r2) - w * oy;
     double h2 = w * ox - u * (oz + r2);
     double h3 = u * oy - v * ox;
-    if (fr.lam != nullptr) fringe_apply<double>(fr, j, y, g.nyp, n, u, v, w, h1, h2, h3);
+    if (fr.lam != nullptr) fringe_apply<double>(fr, j, y, g.nyp, n, u, v, w, 0.0, 0.0, h1, h2, h3);
     const double e2 = u * u + v * v + w * w;
     oth[j * 2 + 0] = double2{h1, h2};
     oth[j * 2 + 1] = double2{h3, e2};

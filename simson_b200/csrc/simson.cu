@@ -91,6 +91,7 @@ struct sgpu_ctx {
   int iles = 0, les_mode = 2, les_iord = 5;
   double les_chi = 0.0;
   double2* les_gu = nullptr;
+  int les_gu_n = 0;            // fields les_gu holds: 3, or 5 for the HPF model (u, v, w, omega_x, omega_z)
   double* les_coef = nullptr;  // [nyp][LES_ROW]
   double* les_lpf = nullptr;   // [NP] L_xz
   double* les_filt = nullptr;  // [NP] F_xz
@@ -739,7 +740,7 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
   // omega_x, omega_z back to physical y into slots 3, 4
   cheb_to_phys(c, czf(c, 4), 3, 2, 0);
   // ADM-RT: high-pass filtered start-up velocities (bla/prhs.f:95-193)
-  if (c->iles == 1) les_filter_velocity(c, 0);
+  if (c->iles == 1 || c->iles == 3) les_filter_velocity(c, 0);
   (void)fld;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
@@ -752,7 +753,7 @@ extern "C" int sgpu_prhs(sgpu_ctx* c) {
 static void les_filter_velocity(sgpu_ctx* c, int skip_oddball) {
   const Dims& g = c->g;
   YFilter F{c->les_coef, c->les_fact2, c->les_factm2, g.nyp};
-  dim3 grid((g.NP + 127) / 128, 3);
+  dim3 grid((g.NP + 127) / 128, c->iles == 3 ? 5 : 3);
   prof_mark(c, K_OTHER);
   if (c->mixed)
     k_les_hpf<float2><<<grid, 128, 0, c->stream>>>(c->stf, c->les_gu, czf(c, 0), F, c->les_lpf, c->les_filt, g,
@@ -780,7 +781,10 @@ static void enqueue_sgs(sgpu_ctx* c) {
   prof_mark(c, K_OTHER);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp), gz4((G.nx4 + KB - 1) / KB, g.nyp), gx(g.nz, g.nyp);
   const int set = (c->iles == 4) ? 1 : 0;
-  if (c->mixed)
+  if (c->iles == 3)  // HPF model: the strain of the high-pass filtered fields (bla/les.f:404-450, 883-966)
+    k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->les_gu, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d,
+                                                        c->alfa, c->beta, 0);
+  else if (c->mixed)
     k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
                                                        c->beta, set);
   else
@@ -857,7 +861,7 @@ static int enqueue_nonlin(sgpu_ctx* c) {
   const Dims& g = c->g;
   const sgpu_params& P = c->prm;
   c->tc = c->t + c->cnp1;
-  if (c->iles == 2 || c->iles == 4) enqueue_sgs(c);
+  if (c->iles >= 2) enqueue_sgs(c);
   // CFL partial maxima only on the substeps the reference evaluates them
   // (nonlinbl.f: mod(it-1,icfl) == 0); the device word keeps the last one.
   const bool do_cfl = (P.icfl > 0) && ((c->it - 1) % P.icfl == 0);
@@ -1033,8 +1037,8 @@ static int enqueue_linear(sgpu_ctx* c) {
   // u, v, w, omega_x, omega_z back to physical y (slots 0-4), oddball plane untouched
   prof_mark(c, K_CHEB_INV);
   cheb_to_phys(c, B.OU, 0, 5, 1, /*fp32_input=*/c->mixed);
-  // ADM-RT: high-pass filtered new velocities (bla/linearbl.f:1871-1960)
-  if (c->iles == 1) les_filter_velocity(c, 1);
+  // ADM-RT and HPF: high-pass filtered new velocities (bla/linearbl.f:1871-2060)
+  if (c->iles == 1 || c->iles == 3) les_filter_velocity(c, 1);
   prof_mark(c, K_OTHER);
   c->launches += 2;
   it_advance(c);
@@ -1806,6 +1810,21 @@ extern "C" int sgpu_amplitudes(sgpu_ctx* c, double* amp, double* row) {
 }
 
 // Buffers, transforms and Delta^2 of the eddy-viscosity and learned models.
+// les_gu with at least n fields (zeroed when (re)allocated)
+static int les_gu_ensure(sgpu_ctx* c, int n) {
+  if (c->les_gu_n >= n) return SGPU_OK;
+  const size_t fld = (size_t)c->g.nyp * c->g.NP;
+  if (c->les_gu) cudaFree(c->les_gu);
+  c->les_gu_n = 0;
+  if (cudaMalloc(&c->les_gu, n * fld * sizeof(double2)) != cudaSuccess) {
+    c->les_gu = nullptr;
+    return SGPU_E_CUDA;
+  }
+  CK(cudaMemsetAsync(c->les_gu, 0, n * fld * sizeof(double2), c->stream));
+  c->les_gu_n = n;
+  return SGPU_OK;
+}
+
 static int sgs_setup(sgpu_ctx* c) {
   const Dims& g = c->g;
   const size_t fld = (size_t)g.nyp * g.NP;
@@ -1827,10 +1846,8 @@ static int sgs_setup(sgpu_ctx* c) {
         cudaMalloc(&c->sgs.tau, 6 * fld * sizeof(double2)) != cudaSuccess ||
         cudaMalloc(&c->sgs_delta2, (size_t)g.nyp * sizeof(double)) != cudaSuccess)
       return SGPU_E_CUDA;
-    if (!c->les_gu) {
-      if (cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) return SGPU_E_CUDA;
-      CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
-    }
+    int rg = les_gu_ensure(c, 3);
+    if (rg) return rg;
     const int sm[4] = {(int)sz, (int)sx11, (int)(2 * (size_t)g.nx * 3 * sizeof(double2)),
                        (int)(2 * (size_t)g.nx * 5 * sizeof(double2))};
     cudaFuncSetAttribute(k_sgs_zinv<double2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm[0]);
@@ -1984,7 +2001,6 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
     return SGPU_OK;
   }
   const Dims& g = c->g;
-  const size_t fld = (size_t)g.nyp * g.NP;
   if (p->iles == 2) {
     // eddy viscosity: cs = 0 dynamic (Germano/Lilly), else fixed C = cs^2
     if (p->ineg < 0 || p->ineg > 2 || (p->cs != 0.0 && p->ineg != 1) || !(p->cs >= 0.0)) return SGPU_E_PARAM;
@@ -1995,10 +2011,17 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
     c->iles = 2;
     return SGPU_OK;
   }
-  if (p->iles != 1) {
-    fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0, 1 or 2)\n", p->iles);
+  if (p->iles != 1 && p->iles != 3) {
+    fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0, 1, 2 or 3)\n", p->iles);
     return SGPU_E_PARAM;
   }
+  if (p->iles == 3 && p->cs == 0.0) {
+    // the dynamic HPF procedure (bla/les.f:968-1383 with the secondary
+    // filter of bla/bla.f:1520-1545) is not built
+    fprintf(stderr, "simson_b200: sgpu_set_les: iles=3 with cs=0 (dynamic HPF model) not supported\n");
+    return SGPU_E_PARAM;
+  }
+  if (p->iles == 3 && (!(p->cs > 0.0) || p->ineg != 1)) return SGPU_E_PARAM;
   if (!(p->cutoff_inv >= 1.0) || p->iord < 0 || p->iord > 5 || p->ihighorder < 0 || p->ihighorder > 2 ||
       !(p->chi >= 0.0))
     return SGPU_E_PARAM;
@@ -2008,12 +2031,22 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
   std::vector<double> rows;
   les_filter_rows(F, rows);
   if (!c->les_coef) {
-    if ((!c->les_gu && cudaMalloc(&c->les_gu, 3 * fld * sizeof(double2)) != cudaSuccess) ||
-        cudaMalloc(&c->les_coef, rows.size() * sizeof(double)) != cudaSuccess ||
+    if (cudaMalloc(&c->les_coef, rows.size() * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->les_lpf, (size_t)g.NP * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->les_filt, (size_t)g.NP * sizeof(double)) != cudaSuccess)
       return SGPU_E_CUDA;
-    CK(cudaMemsetAsync(c->les_gu, 0, 3 * fld * sizeof(double2), c->stream));
+  }
+  {
+    // ADM-RT filters u, v, w; the HPF model also omega_x, omega_z
+    // (bla/linearbl.f:1965-2060), from which it forms the filtered gradients
+    const int rg = les_gu_ensure(c, p->iles == 3 ? 5 : 3);
+    if (rg) return rg;
+  }
+  if (p->iles == 3) {
+    const int rs = sgs_setup(c);
+    if (rs) return rs;
+    c->les_cs = p->cs;
+    c->les_ineg = 1;
   }
   CK(cudaMemcpyAsync(c->les_coef, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->les_lpf, F.lpfxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -2025,7 +2058,7 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
   c->les_mode = p->ihighorder;
   c->les_iord = p->iord;
   c->les_chi = p->chi;  // chi_scaled = chi / dstar, dstar = 1
-  c->iles = 1;
+  c->iles = p->iles;
   return SGPU_OK;
 }
 
@@ -2048,7 +2081,7 @@ extern "C" int sgpu_download_les(sgpu_ctx* c, double* gr, double* gi) {
 // 11 12 13 22 23 33) in the reference layout.
 extern "C" int sgpu_download_sgs_stress(sgpu_ctx* c, double* tr, double* ti) {
   if (!c || !tr || !ti) return SGPU_E_PARAM;
-  if (c->iles != 2 && c->iles != 4) return SGPU_E_STATE;
+  if (c->iles < 2) return SGPU_E_STATE;
   const size_t n = 6 * (size_t)c->g.nyp * c->g.NP;  // the staging area holds 7 slots
   k_to_ref<<<592, 256, 0, c->stream>>>(c->sgs.tau, c->stage, c->stage + n, c->g, 6);
   c->launches++;

@@ -104,18 +104,22 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
-// H -= lambda (u - U_b) at x point j of plane y; u, v, w are totals.
+// H -= lambda (u - U_b) at x point j of plane y.  u, v, w are the velocities
+// the products used; um, wm the plane means they leave out (the mixed path's
+// perturbation form, 0 on the FP64 path), which enter as U - U_b in FP64 so
+// that no O(1) difference is rounded to FP32.  FP64 path: u + (-U_b) is the
+// reference's u - U_b exactly.
 template <class T>
-__device__ __forceinline__ void fringe_apply(const Fringe& fr, int j, int y, int nyp, int n, T u, T v, T w, T& h1,
-                                             T& h2, T& h3) {
+__device__ __forceinline__ void fringe_apply(const Fringe& fr, int j, int y, int nyp, int n, T u, T v, T w,
+                                             double um, double wm, T& h1, T& h2, T& h3) {
   const double lm = fr.lam[j];
   if (lm == 0.0) return;
   const size_t cs = (size_t)nyp * n;  // one component of the base flow
   const double* b = fr.base + (size_t)y * n + j;
   const T l = (T)lm;
-  h1 = h1 - l * (u - (T)b[0]);
-  h2 = h2 - l * (v - (T)b[cs]);
-  h3 = h3 - l * (w - (T)b[2 * cs]);
+  h1 = h1 - l * (u + (T)(um - b[0]));
+  h2 = h2 - l * (v + (T)(0.0 - b[cs]));
+  h3 = h3 - l * (w + (T)(wm - b[2 * cs]));
 }
 
 // N > 0: the x length g.nxp is N (compile-time plan, NT threads per CTA).
@@ -206,8 +210,10 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
       h2 = (W * ox + w * Ox - U * oz - u * Oz) + (w * ox - u * oz);
       h3 = U * oy - v * Ox + (u * oy - v * ox);
     }
-    // fringe on the total velocity (U = W = 0 on the FP64 path, so u + U = u)
-    if (fr.lam != nullptr) fringe_apply<T>(fr, j, y, g.nyp, n, u + U, v, w + W, h1, h2, h3);
+    // fringe on the total velocity (no plane means on the FP64 path)
+    if (fr.lam != nullptr)
+      fringe_apply<T>(fr, j, y, g.nyp, n, u, v, w, mean != nullptr ? mean[0 * g.nyp + y] : 0.0,
+                      mean != nullptr ? mean[1 * g.nyp + y] : 0.0, h1, h2, h3);
     if constexpr (RB % 2 == 0) {
       oth[j * B2 + r] = V{h1, h2};
       T* h3p = reinterpret_cast<T*>(&oth[j * B2 + RB + r / 2]);

@@ -188,3 +188,58 @@ def test_smagorinsky_variants(cs, ineg, need_ref):
     assert max(_tau_errors(ref, gpu, nz)) < 1e-10
     e = _state_errors(ref, gpu)
     assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+# --- HPF eddy-viscosity model (iles = 3, fixed constant) --------------------
+
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_hpf_smagorinsky_matches_reference(grid, need_ref):
+    """tau_ij = -2 cs^2 Delta^2 |S(H u)| S(H u) of bla/les.f:883-966, 1515 on
+    the high-pass filtered velocities and vorticities of bla/linearbl.f:
+    1871-2060 (prhs.f at the start), its divergence sigma, the state."""
+    nx, ny, nz = grid
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 9, need_ref, iles=3, cs=0.12)
+    assert max(_gu_errors(ref, gpu, nz)) < 1e-12  # H u, v, w after the start-up
+    ref.substep()
+    gpu.substep()
+    te = _tau_errors(ref, gpu, nz)
+    assert max(te) < 1e-11, te
+    se = _gu_errors(ref, gpu, nz)  # sigma
+    assert max(se) < 1e-11, se
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+@pytest.mark.parametrize("ihighorder", [0, 1, 2])
+def test_hpf_smagorinsky_substeps(ihighorder, need_ref):
+    nx, ny, nz = 16, 17, 16
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 10, need_ref, iles=3, cs=0.1,
+                     ihighorder=ihighorder)
+    for _ in range(6):
+        ref.substep()
+        gpu.substep()
+        e = _state_errors(ref, gpu)
+        assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+    assert max(_tau_errors(ref, gpu, nz)) < 1e-10
+
+
+def test_hpf_smagorinsky_config_d(need_ref):
+    """The LES configuration 64x97x64, ten RK3 steps."""
+    nx, ny, nz = 64, 97, 64
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 11, need_ref, iles=3, cs=0.1)
+    for _ in range(30):
+        ref.substep()
+        gpu.substep()
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+def test_hpf_dynamic_is_rejected():
+    """The dynamic HPF procedure (cs = 0) is not built: SGPU_E_PARAM."""
+    from simson_b200.bla import Channel, SimsonError
+    ch = Channel(16, 17, 16, 4200.0, 2 * np.pi, np.pi, 0.005)
+    try:
+        with pytest.raises(SimsonError):
+            ch.set_les(iles=3, cs=0.0)
+    finally:
+        ch.close()
