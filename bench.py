@@ -240,6 +240,10 @@ def setup_les(ch, model):
         ch.set_les(iles=1)
     elif model == "dyn":
         ch.set_les(iles=2)
+    elif model == "hpf":
+        ch.set_les(iles=3, cs=0.1)
+    elif model == "hpf_dyn":
+        ch.set_les(iles=3, cs=0.0)
     elif model in ("mlp", "mlp_fb"):
         w, (s_in, s_y, s_out), _ = learned_model()
         ch.set_sgs_mlp(w, s_in=s_in, s_y=s_y, s_out=s_out)
@@ -250,24 +254,26 @@ def setup_les(ch, model):
 def les_arm(steps, warmup):
     """RK3 steps/s of the LES configuration 64x97x64 (Re_cl 9000, the box of
     the 384x193x384 workload) with each SGS model: ADM-RT and dynamic
-    Smagorinsky with the reference's sgs.i defaults, the learned model alone
-    and with its per-plane fallback to dynamic Smagorinsky."""
+    Smagorinsky with the reference's sgs.i defaults, the HPF eddy viscosity
+    (fixed cs = 0.1 and dynamic), the learned model alone and with its
+    per-plane fallback to dynamic Smagorinsky."""
     from simson_b200.bla import Channel, FP64, MIXED
     from simson_b200.fields import channel_field
     w = LES_WORKLOAD
     u, v, wv = channel_field(w["nx"], w["ny"], w["nz"], w["xl"], w["zl"], w["rms"], w["seed"])
     out = {}
     variants = [("no_model_fp64", FP64, None), ("adm_rt_fp64", FP64, "adm"), ("dyn_smagorinsky_fp64", FP64, "dyn"),
+                ("hpf_fixed_fp64", FP64, "hpf"), ("hpf_dynamic_fp64", FP64, "hpf_dyn"),
                 ("learned_mlp_fp64", FP64, "mlp"), ("learned_mlp_fallback_fp64", FP64, "mlp_fb"),
                 ("dyn_smagorinsky_mixed", MIXED, "dyn"), ("learned_mlp_mixed", MIXED, "mlp"),
                 ("learned_mlp_fallback_mixed", MIXED, "mlp_fb"), ("no_model_mixed", MIXED, None)]
     for tag, prec, model in variants:
         ch = Channel(w["nx"], w["ny"], w["nz"], w["re"], w["xl"], w["zl"], w["dt"], precision=prec)
         ch.set_velocity(u, v, wv)
-        if model == "adm":
+        if model in ("adm", "hpf", "hpf_dyn"):
             setup_les(ch, model)  # before prhs: it filters the start-up velocities
         ch.prhs()
-        if model != "adm":
+        if model not in ("adm", "hpf", "hpf_dyn"):
             setup_les(ch, model)
         for _ in range(warmup):
             ch.step(1)

@@ -140,9 +140,12 @@ typedef struct {
  *   omega_z after prhs and every step 3 (bla/prhs.f, bla/linearbl.f:
  *   1871-2060), and every substep the eddy-viscosity stress of iles = 2
  *   formed with the strain of the filtered field (bla/les.f:404-450,
- *   883-966), cs > 0 fixed (ineg = 1).  The dynamic HPF procedure (cs = 0,
- *   bla/les.f:968-1383 with the secondary filter of bla/bla.f:1520-1545)
- *   is rejected with SGPU_E_PARAM. */
+ *   883-966): cs > 0 fixed (ineg = 1), or cs = 0 the dynamic HPF
+ *   procedure (bla/les.f:968-1383): a secondary filter with the x/z transfer
+ *   functions over a quarter of the wavenumbers (bla/bla.f:1520-1545) on the
+ *   same five fields, L_ij from the resolved velocity, M_ij from the strain
+ *   of the primary filtered field and the test-filtered strain of the
+ *   secondary one, the coefficient as for iles = 2 (ineg 0, 1, 2). */
 int sgpu_set_les(sgpu_ctx* ctx, const sgpu_les_params* p);
 
 /* gur, gui(memnx, memny, memnz, 1..3): the filtered velocities (iles = 1, and

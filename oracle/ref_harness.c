@@ -276,6 +276,17 @@ void sref_get_filter(double *g1, double *g2, double *dg, double *sx, double *sz,
   memcpy(lpf, v_lpfxz, (size_t)(v_nx / 2) * v_nz * sizeof(double));
 }
 
+/* Secondary filter of the dynamic HPF model (bla/bla.f:1520-1545, after
+ * sref_set_les with iles = 3, cs = 0): gewy12, gewy22, diags2 (nyp,5 each),
+ * lpfxz2 and filtxz2 (nx/2,nz). */
+void sref_get_filter2(double *g1, double *g2, double *dg, double *lpf, double *filt) {
+  memcpy(g1, v_gewy12, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(g2, v_gewy22, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(dg, v_diags2, (size_t)v_nyp * 5 * sizeof(double));
+  memcpy(lpf, v_lpfxz2, (size_t)(v_nx / 2) * v_nz * sizeof(double));
+  memcpy(filt, v_filtxz2, (size_t)(v_nx / 2) * v_nz * sizeof(double));
+}
+
 /* High-pass filtered velocity gur,gui(memnx,memny,memnz,5), component 1..3. */
 void sref_get_gu(int comp, double *re_part, double *im_part) {
   long n = slot_size();

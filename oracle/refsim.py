@@ -46,6 +46,7 @@ def _lib(nx, ny, nz, build=True, fma=False, pressure=False):
     lib.sref_get_amp.argtypes = [dp]
     lib.sref_xys.argtypes = [ctypes.c_double, ctypes.c_int, dp, dp]
     lib.sref_pressure.argtypes = [dp, dp]
+    lib.sref_get_filter2.argtypes = [dp] * 5
     lib.sref_set_spatial.argtypes = [ctypes.c_int] + [ctypes.c_double] * 5
     lib.sref_get_fringe.argtypes = [dp, dp]
     lib.sref_get_base.argtypes = [dp, dp]
@@ -172,6 +173,15 @@ class RefSim:
         sx = np.empty(nx // 2 + 2); sz = np.empty(nz // 2 + 2); lpf = np.empty((nz, nx // 2))
         self.lib.sref_get_filter(_dp(g1), _dp(g2), _dp(dg), _dp(sx), _dp(sz), _dp(lpf))
         return g1, g2, dg, sx, sz, lpf
+
+    def filter2_tables(self):
+        """The dynamic HPF model's secondary filter (bla/bla.f:1520-1545):
+        gewy12, gewy22, diags2 as (5, nyp); lpfxz2, filtxz2 as (nz, nx/2)."""
+        g1, g2, dg = (np.empty((5, self.nyp)) for _ in range(3))
+        lpf = np.empty((self.nz, self.nx // 2))
+        filt = np.empty((self.nz, self.nx // 2))
+        self.lib.sref_get_filter2(_dp(g1), _dp(g2), _dp(dg), _dp(lpf), _dp(filt))
+        return g1, g2, dg, lpf, filt
 
     def gu(self, comp):
         """High-pass filtered velocity component comp (1..3), shape (nz, nyp, nx//2)."""

@@ -80,6 +80,19 @@ extern "C" int sbh_les_filter(int nyp, int nx, int nz, double cutoff, int iord, 
   return 0;
 }
 
+// The secondary filter of the dynamic HPF model (les_filter_build with
+// secondary = true): g1, g2 [nyp][5], lpfxz, filtxz [nz][nx/2].
+extern "C" int sbh_les_filter2(int nyp, int nx, int nz, double cutoff, int iord, double* g1, double* g2,
+                               double* lpfxz, double* filtxz) {
+  LesFilter F;
+  if (!les_filter_build(nyp, nx, nz, cutoff, iord, F, true)) return -1;
+  memcpy(g1, F.g1.data(), F.g1.size() * sizeof(double));
+  memcpy(g2, F.g2.data(), F.g2.size() * sizeof(double));
+  memcpy(lpfxz, F.lpfxz.data(), F.lpfxz.size() * sizeof(double));
+  memcpy(filtxz, F.filtxz.data(), F.filtxz.size() * sizeof(double));
+  return 0;
+}
+
 // One high-pass filtered column (the device routine run on the host):
 // in/out complex interleaved, nyp values; mode = ihighorder.
 extern "C" int sbh_les_hpf_column(int nyp, int nx, int nz, double cutoff, int iord, int mode, int kx, int iz,

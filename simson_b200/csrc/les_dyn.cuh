@@ -1,4 +1,5 @@
-// Eddy-viscosity large-eddy model on the device (iles = 2): the Smagorinsky
+// Eddy-viscosity large-eddy model on the device (iles = 2; iles = 3 feeds it
+// the high-pass filtered fields, see k_sgs_zinv and k_sgs_xpass1): the Smagorinsky
 // stress tau_ij = -2 C Delta^2 |S| S_ij with the dynamic (Germano/Lilly)
 // coefficient C, its divergence sigma_i = d tau_ij / dx_j, and -sigma added
 // to H in step 2.  The reference computes tau plane by plane in bla/les.f
@@ -120,10 +121,13 @@ __device__ __forceinline__ double2 sgs_spec_field(const V* st, size_t slot, size
   }
 }
 
+// sf != nullptr (field set 0): the strain-rate fields 3..8 from the fields
+// of sf (the dynamic HPF model: u from the state, S_ij of the high-pass
+// filtered field), u, v, w from st.
 template <class V, int KB>
 __global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPlan plan,
                            const double2* __restrict__ tw, const double* __restrict__ alfa,
-                           const double* __restrict__ beta, int set) {
+                           const double* __restrict__ beta, int set, const double2* __restrict__ sf) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* b0 = reinterpret_cast<double2*>(smem_raw);
   double2* b1 = b0 + (size_t)G.nz * KB;
@@ -136,8 +140,11 @@ __global__ void k_sgs_zinv(const V* __restrict__ st, SgsBufs B, SgsGrid G, FFTPl
       const int iz = t / KB;
       const int kx = kx0 + t - iz * KB;
       double2 val{0.0, 0.0};
-      if (kx < G.nx2 && iz != G.zodd)
-        val = sgs_spec_field(st, slot, (size_t)y * G.NP + (size_t)iz * G.nx2 + kx, f, alfa[kx], beta[iz], set);
+      if (kx < G.nx2 && iz != G.zodd) {
+        const size_t off = (size_t)y * G.NP + (size_t)iz * G.nx2 + kx;
+        val = (sf != nullptr && f >= 3) ? sgs_spec_field(sf, slot, off, f, alfa[kx], beta[iz], set)
+                                        : sgs_spec_field(st, slot, off, f, alfa[kx], beta[iz], set);
+      }
       b0[t] = val;
     }
     __syncthreads();
@@ -173,8 +180,11 @@ __device__ __forceinline__ double sgs_sabs(const double* s) {
 }
 
 // One z row per CTA.  Shared memory: two buffers of 11 columns x nx.
+// s2 != nullptr: the test filter's B_ij parts are these six physical fields
+// (the dynamic HPF model: the strain of the secondary high-pass filtered
+// field, bla/les.f:1031-1250) instead of S_ij.
 __global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
-                             const double* __restrict__ delta2) {
+                             const double* __restrict__ delta2, const double* __restrict__ s2) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NC = 11;
   double2* bA = reinterpret_cast<double2*>(smem_raw);
@@ -220,7 +230,7 @@ __global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
     r[9] = -v * v;
     r[10] = -w * v;
     r[11] = -w * w;
-    for (int l = 0; l < 6; ++l) r[12 + l] = s[l];  // B = S
+    for (int l = 0; l < 6; ++l) r[12 + l] = s2 ? s2[(size_t)l * fs10 + prow + j] : s[l];  // B = S (or S of H2 u)
     r[18] = u;
     r[19] = v;
     r[20] = w;
@@ -242,9 +252,11 @@ __global__ void k_sgs_xpass1(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* 
   }
 }
 
-// The nine gradient rows of one z row back to physical x (learned model):
-// phys10 fields 0..8.
-__global__ void k_sgs_xinv9(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw) {
+// The nine spec9 rows of one z row back to physical x: fields f0..8 into
+// out[f - f0] (the learned model's gradients: out = phys10, f0 = 0; the
+// dynamic HPF model's secondary strain: f0 = 3).
+__global__ void k_sgs_xinv9(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* __restrict__ tw,
+                            double* __restrict__ out, int f0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* bA = reinterpret_cast<double2*>(smem_raw);
   double2* bB = bA + (size_t)G.nx * 5;
@@ -265,8 +277,8 @@ __global__ void k_sgs_xinv9(SgsBufs B, SgsGrid G, FFTPlan plan, const double2* _
   for (int t = threadIdx.x; t < n * 5; t += blockDim.x) {
     const int j = t / 5, c = t - 5 * (t / 5);
     const double2 z = res[j * 5 + c];
-    B.phys10[(size_t)(2 * c) * fs10 + prow + j] = z.x;
-    if (2 * c + 1 < 9) B.phys10[(size_t)(2 * c + 1) * fs10 + prow + j] = z.y;
+    if (2 * c >= f0) out[(size_t)(2 * c - f0) * fs10 + prow + j] = z.x;
+    if (2 * c + 1 < 9 && 2 * c + 1 >= f0) out[(size_t)(2 * c + 1 - f0) * fs10 + prow + j] = z.y;
   }
 }
 

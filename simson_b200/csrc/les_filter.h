@@ -224,7 +224,12 @@ inline bool les_filter_factor(LesFilter& F) {
 // (the reference's gridy with dstar = 1), nx/2 x nz stored modes, cut-off
 // wavenumber fraction cutoff = 1/cutoff_inv and order N = iord.  Returns
 // false on a singular condition system (not reached for nyp >= 7).
-inline bool les_filter_build(int nyp, int nx, int nz, double cutoff, int iord, LesFilter& F) {
+// secondary: the filter of the dynamic HPF model (bla/bla.f:1520-1545): the
+// x and z transfer functions span kx = 0..nx/4 and kz = 0..nz/4 (the
+// reference's init_filter called with nx/4+1, nz/4+1 points) and are zero
+// above; the wall-normal stencils do not depend on it.
+inline bool les_filter_build(int nyp, int nx, int nz, double cutoff, int iord, LesFilter& F,
+                             bool secondary = false) {
   using namespace les_detail;
   if (nyp < 7 || (nyp % 2) == 0 || nx < 2 || nz < 2 || iord < 0) return false;
   F.nyp = nyp;
@@ -243,9 +248,9 @@ inline bool les_filter_build(int nyp, int nx, int nz, double cutoff, int iord, L
     long double bx[5], ax[5];
     if (!explicit_mindisp(x, s, bx)) return false;
     implicit_from(bx, s, 2, cutoff, ax);
-    const int nxs = nx / 2 + 1, nzs = nz / 2 + 1;
-    F.specx.resize(nxs);
-    F.specz.resize(nzs);
+    const int nxs = (secondary ? nx / 4 : nx / 2) + 1, nzs = (secondary ? nz / 4 : nz / 2) + 1;
+    F.specx.assign(nx / 2 + 1, 0.0);
+    F.specz.assign(nz / 2 + 1, 0.0);
     for (int i = 0; i < nxs; ++i) F.specx[i] = transfer(bx, ax, (long double)i * pi / (long double)(nxs - 1));
     for (int i = 0; i < nzs; ++i) F.specz[i] = transfer(bx, ax, (long double)i * pi / (long double)(nzs - 1));
   }

@@ -92,6 +92,14 @@ struct sgpu_ctx {
   double les_chi = 0.0;
   double2* les_gu = nullptr;
   int les_gu_n = 0;            // fields les_gu holds: 3, or 5 for the HPF model (u, v, w, omega_x, omega_z)
+  // dynamic HPF model (iles = 3, cs = 0): the secondary filter's x/z tables,
+  // the five secondary high-pass filtered fields, and the physical strain of
+  // those [6][nyp][nz][nx]
+  bool hpf_dyn = false;
+  double* les_lpf2 = nullptr;
+  double* les_filt2 = nullptr;
+  double2* les_gu2 = nullptr;
+  double* hpf_s2 = nullptr;
   double* les_coef = nullptr;  // [nyp][LES_ROW]
   double* les_lpf = nullptr;   // [NP] L_xz
   double* les_filt = nullptr;  // [NP] F_xz
@@ -468,7 +476,7 @@ extern "C" int sgpu_finalize(sgpu_ctx* c) {
                   c->xys_part, c->xys_u, c->box_out, c->press, c->press_wd, c->xys_twz.d, c->xys_twz.f, c->xys_twx.d, c->xys_twx.f, c->mlp_image, c->mlp_tau,
                   c->mlp_err, c->sgs_flags, c->sgs_bsums, c->chb_fwd, c->chb_inv, c->chb_err, c->puw, c->scal, c->cfl_bits, c->alfa, c->beta, c->dyi, c->zb, c->xb, c->cz, c->rz,
                   c->mscr, c->hom_vh, c->hom_s, c->hom_cf, c->stage, c->twz.d, c->twz.f, c->twx.d, c->twx.f, c->twy.d, c->twy.f,
-                  c->fr_lam, c->fr_base};
+                  c->fr_lam, c->fr_base, c->les_lpf2, c->les_filt2, c->les_gu2, c->hpf_s2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < 16; ++i)
@@ -762,6 +770,17 @@ static void les_filter_velocity(sgpu_ctx* c, int skip_oddball) {
     k_les_hpf<double2><<<grid, 128, 0, c->stream>>>(c->st, c->les_gu, czf(c, 0), F, c->les_lpf, c->les_filt, g,
                                                     c->les_mode, c->les_iord, skip_oddball);
   c->launches++;
+  if (c->iles == 3 && c->hpf_dyn) {
+    // the secondary filter (bla/linearbl.f:2067-2250, the same wall-normal
+    // filter, the x/z tables of the quarter cut-off) for the dynamic procedure
+    if (c->mixed)
+      k_les_hpf<float2><<<grid, 128, 0, c->stream>>>(c->stf, c->les_gu2, czf(c, 0), F, c->les_lpf2, c->les_filt2, g,
+                                                     c->les_mode, c->les_iord, skip_oddball);
+    else
+      k_les_hpf<double2><<<grid, 128, 0, c->stream>>>(c->st, c->les_gu2, czf(c, 0), F, c->les_lpf2, c->les_filt2,
+                                                      g, c->les_mode, c->les_iord, skip_oddball);
+    c->launches++;
+  }
 }
 
 static SgsGrid sgs_grid(const sgpu_ctx* c) {
@@ -781,20 +800,40 @@ static void enqueue_sgs(sgpu_ctx* c) {
   prof_mark(c, K_OTHER);
   dim3 gz((g.nx2 + KB - 1) / KB, g.nyp), gz4((G.nx4 + KB - 1) / KB, g.nyp), gx(g.nz, g.nyp);
   const int set = (c->iles == 4) ? 1 : 0;
-  if (c->iles == 3)  // HPF model: the strain of the high-pass filtered fields (bla/les.f:404-450, 883-966)
+  const double* s2 = nullptr;
+  if (c->iles == 3 && c->hpf_dyn) {
+    // dynamic HPF (bla/les.f:968-1383): first the strain of the secondary
+    // filtered field in physical space (test-filtered below in place of S),
+    // then u of the state with the strain of the primary filtered field
+    k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->les_gu2, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d,
+                                                        c->alfa, c->beta, 0, nullptr);
+    k_sgs_xinv9<<<gx, 128, 2 * (size_t)g.nx * 5 * sizeof(double2), c->stream>>>(c->sgs, G, c->sgs_twx.plan,
+                                                                                 c->sgs_twx.d, c->hpf_s2, 3);
+    s2 = c->hpf_s2;
+    c->launches += 2;
+    if (c->mixed)
+      k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                         c->beta, 0, c->les_gu);
+    else
+      k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
+                                                          c->beta, 0, c->les_gu);
+  } else if (c->iles == 3) {
+    // HPF model, fixed constant: the strain of the high-pass filtered fields
+    // (bla/les.f:404-450, 883-966)
     k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->les_gu, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d,
-                                                        c->alfa, c->beta, 0);
-  else if (c->mixed)
+                                                        c->alfa, c->beta, 0, nullptr);
+  } else if (c->mixed) {
     k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                       c->beta, set);
-  else
+                                                       c->beta, set, nullptr);
+  } else {
     k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                        c->beta, set);
+                                                        c->beta, set, nullptr);
+  }
   if (c->iles == 4) {
     // learned model: gradients to physical space, MLP on the tensor cores,
     // tau / (nx nz) back to Fourier space
     k_sgs_xinv9<<<gx, 128, 2 * (size_t)g.nx * 5 * sizeof(double2), c->stream>>>(c->sgs, G, c->sgs_twx.plan,
-                                                                                 c->sgs_twx.d);
+                                                                                 c->sgs_twx.d, c->sgs.phys10, 0);
     MlpArgs A{};
     A.image = c->mlp_image;
     A.mode = 1;
@@ -822,11 +861,11 @@ static void enqueue_sgs(sgpu_ctx* c) {
       F.plane_on = c->sgs_flags;
       if (c->mixed)
         k_sgs_zinv<float2, KB><<<gz, 256, sz, c->stream>>>(c->stf, F, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                           c->beta, 0);
+                                                           c->beta, 0, nullptr);
       else
         k_sgs_zinv<double2, KB><<<gz, 256, sz, c->stream>>>(c->st, F, G, c->sgs_twz.plan, c->sgs_twz.d, c->alfa,
-                                                            c->beta, 0);
-      k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+                                                            c->beta, 0, nullptr);
+      k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, nullptr);
       k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(F, G, c->sgs_twz.plan, c->sgs_twz.d);
       k_sgs_xpass2<<<gx, 128, sx11, c->stream>>>(F, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
       k_sgs_coef<<<dim3((g.nx + 127) / 128, g.nyp), 128, 0, c->stream>>>(F, G, c->les_cs, c->les_ineg);
@@ -837,7 +876,7 @@ static void enqueue_sgs(sgpu_ctx* c) {
     k_sgs_zfwd<KB><<<gz, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
     c->launches += 3;
   } else {
-  k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
+  k_sgs_xpass1<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2, s2);
   k_sgs_zfilt<KB><<<gz4, 256, sz, c->stream>>>(c->sgs, G, c->sgs_twz.plan, c->sgs_twz.d);
   k_sgs_xpass2<<<gx, 128, sx11, c->stream>>>(c->sgs, G, c->sgs_twx.plan, c->sgs_twx.d, c->sgs_delta2);
   k_sgs_coef<<<dim3((g.nx + 127) / 128, g.nyp), 128, 0, c->stream>>>(c->sgs, G, c->les_cs, c->les_ineg);
@@ -2015,13 +2054,8 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
     fprintf(stderr, "simson_b200: sgpu_set_les: iles=%d not supported (0, 1, 2 or 3)\n", p->iles);
     return SGPU_E_PARAM;
   }
-  if (p->iles == 3 && p->cs == 0.0) {
-    // the dynamic HPF procedure (bla/les.f:968-1383 with the secondary
-    // filter of bla/bla.f:1520-1545) is not built
-    fprintf(stderr, "simson_b200: sgpu_set_les: iles=3 with cs=0 (dynamic HPF model) not supported\n");
+  if (p->iles == 3 && (p->ineg < 0 || p->ineg > 2 || (p->cs != 0.0 && p->ineg != 1) || !(p->cs >= 0.0)))
     return SGPU_E_PARAM;
-  }
-  if (p->iles == 3 && (!(p->cs > 0.0) || p->ineg != 1)) return SGPU_E_PARAM;
   if (!(p->cutoff_inv >= 1.0) || p->iord < 0 || p->iord > 5 || p->ihighorder < 0 || p->ihighorder > 2 ||
       !(p->chi >= 0.0))
     return SGPU_E_PARAM;
@@ -2046,7 +2080,28 @@ extern "C" int sgpu_set_les(sgpu_ctx* c, const sgpu_les_params* p) {
     const int rs = sgs_setup(c);
     if (rs) return rs;
     c->les_cs = p->cs;
-    c->les_ineg = 1;
+    c->les_ineg = p->ineg;
+    c->hpf_dyn = (p->cs == 0.0);
+    if (c->hpf_dyn) {
+      // the secondary filter of the dynamic procedure (bla/bla.f:1520-1545)
+      LesFilter F2;
+      if (!les_filter_build(g.nyp, g.nx, g.nz, 1.0 / p->cutoff_inv, p->iord, F2, true)) return SGPU_E_PARAM;
+      const size_t fld = (size_t)g.nyp * g.NP;
+      const size_t pl = (size_t)g.nyp * g.nz * g.nx;
+      if (!c->les_lpf2) {
+        if (cudaMalloc(&c->les_lpf2, (size_t)g.NP * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&c->les_filt2, (size_t)g.NP * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&c->les_gu2, 5 * fld * sizeof(double2)) != cudaSuccess ||
+            cudaMalloc(&c->hpf_s2, 6 * pl * sizeof(double)) != cudaSuccess)
+          return SGPU_E_CUDA;
+        CK(cudaMemsetAsync(c->les_gu2, 0, 5 * fld * sizeof(double2), c->stream));
+      }
+      CK(cudaMemcpyAsync(c->les_lpf2, F2.lpfxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaMemcpyAsync(c->les_filt2, F2.filtxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
   }
   CK(cudaMemcpyAsync(c->les_coef, rows.data(), rows.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->les_lpf, F.lpfxz.data(), (size_t)g.NP * sizeof(double), cudaMemcpyHostToDevice, c->stream));

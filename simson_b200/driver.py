@@ -89,8 +89,6 @@ def run(deck_dir, grid=None, precision="fp64", device=0, max_steps=None, log=pri
     if bad:
         raise blai.DeckError("options this library does not run: " + ", ".join(bad))
     les = blai.read_sgs_i(os.path.join(deck_dir, "sgs.i")) if b.sgs else None
-    if les is not None and les.iles == 3 and les.cs == 0.0:
-        raise blai.DeckError("sgs.i iles = 3 with cs = 0 (the dynamic HPF model) is not built")
     if b.iamp > 0 and b.iamp % b.nst:
         # nonlinbl samples at any substep with mod(it-1-nst, iamp) = 0; this
         # driver samples at step boundaries only

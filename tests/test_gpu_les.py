@@ -234,12 +234,59 @@ def test_hpf_smagorinsky_config_d(need_ref):
     assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
 
 
-def test_hpf_dynamic_is_rejected():
-    """The dynamic HPF procedure (cs = 0) is not built: SGPU_E_PARAM."""
-    from simson_b200.bla import Channel, SimsonError
-    ch = Channel(16, 17, 16, 4200.0, 2 * np.pi, np.pi, 0.005)
-    try:
-        with pytest.raises(SimsonError):
+@pytest.mark.parametrize("grid,ineg", [((16, 17, 16), 1), ((48, 65, 48), 1), ((16, 17, 16), 0), ((16, 17, 16), 2)])
+def test_dynamic_hpf_matches_reference(grid, ineg, need_ref):
+    """The dynamic HPF procedure (cs = 0): L_ij of the resolved velocity, M_ij
+    of the primary and the test-filtered secondary high-pass strain, the
+    clipped coefficient, tau = -2 C Delta^2 |S(H u)| S(H u).  tau and sigma
+    are compared after the step-2 half of the first substep: the reference's
+    step 3 then writes the secondary filtered fields into taur slots 1-5
+    (bla/linearbl.f:2067-2250); the state after six substeps."""
+    nx, ny, nz = grid
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 12, need_ref, iles=3, cs=0.0, ineg=ineg)
+    ref.nonlin_only()
+    gpu.nonlinbl()
+    te = _tau_errors(ref, gpu, nz)
+    assert max(te) < 1e-11, te
+    assert max(_gu_errors(ref, gpu, nz)) < 1e-11
+    ref.linear_only()
+    gpu.linearbl()
+    for _ in range(5):
+        ref.substep()
+        gpu.substep()
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+
+
+def test_dynamic_hpf_config_d(need_ref):
+    """The LES configuration 64x97x64, ten RK3 steps of the dynamic HPF model."""
+    nx, ny, nz = 64, 97, 64
+    ref, gpu = _pair(nx, ny, nz, 2 * np.pi, np.pi, 4200.0, 0.005, 0.1, 13, need_ref, iles=3, cs=0.0)
+    for _ in range(30):
+        ref.substep()
+        gpu.substep()
+    e = _state_errors(ref, gpu)
+    assert max(e[:3]) < 1e-11 and max(e) < 1e-10, e
+    # taur slot 6 (tau_33) is the only one the reference's step 3 leaves
+    assert _tau_errors(ref, gpu, nz)[5] < 1e-10
+
+
+def test_dynamic_hpf_mixed_close_to_fp64():
+    from simson_b200.bla import Channel
+    nx, ny, nz = 48, 65, 48
+    u, v, w = channel_field(nx, ny, nz, 2 * np.pi, np.pi, 0.1, 14, kmax=min(nx, nz) // 2 - 2)
+    out = []
+    for prec in ("fp64", "mixed"):
+        ch = Channel(nx, ny, nz, 4200.0, 2 * np.pi, np.pi, 0.005, precision=prec)
+        try:
             ch.set_les(iles=3, cs=0.0)
-    finally:
-        ch.close()
+            ch.set_velocity(u, v, w)
+            ch.start()
+            ch.step(10)
+            out.append(ch.state(3))
+        finally:
+            ch.close()
+    keep = np.ones(nz, bool)
+    keep[nz // 2] = False
+    errs = [rel_l2(out[1][k][keep], out[0][k][keep]) for k in range(3)]
+    assert max(errs) < 1e-5, errs

@@ -53,6 +53,29 @@ def test_filter_tables_match_reference(grid, host, need_ref):
     assert np.abs(lpf - rl).max() < 1e-14
 
 
+@pytest.mark.parametrize("grid", [(16, 17, 16), (48, 65, 48)])
+def test_secondary_filter_tables_match_reference(grid, host, need_ref):
+    """The dynamic HPF model's second filter (x/z transfer functions over a
+    quarter of the wavenumbers, the same wall-normal stencils) against the
+    reference's set-up of bla/bla.f:1520-1545."""
+    from refsim import RefSim
+    nx, ny, nz = grid
+    need_ref(nx, ny, nz)
+    host.sbh_les_filter2.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_int] + [dp] * 4
+    ref = RefSim(nx, ny, nz, 4200.0, 4 * np.pi, 2 * np.pi, 0.01)
+    ref.set_les(iles=3, cs=0.0)
+    r1, r2, _, rl, rf = ref.filter2_tables()
+    p1, p2 = ref.filter_tables()[:2]
+    assert np.array_equal(r1, p1) and np.array_equal(r2, p2)  # the wall-normal filter is the primary's
+    g1 = np.empty((ny, 5)); g2 = np.empty((ny, 5))
+    lpf = np.empty((nz, nx // 2)); filt = np.empty((nz, nx // 2))
+    assert host.sbh_les_filter2(ny, nx, nz, 1 / 1.5, 5, _p(g1), _p(g2), _p(lpf), _p(filt)) == 0
+    assert np.abs(g1.T - r1).max() < 1e-14 and np.abs(g2.T - r2).max() < 1e-14
+    assert np.abs(filt - rf).max() < 1e-14
+    assert np.abs(lpf - rl).max() < 1e-14
+    assert filt[0, nx // 4 + 1:].max() == 0.0  # nothing passes above kx = nx/4
+
+
 @pytest.mark.parametrize("mode", [2, 1, 0])
 def test_filtered_columns_match_reference(mode, host, need_ref):
     """The column routine the kernel runs, on the host, against the
