@@ -157,3 +157,50 @@ def test_spatial_pressure_vs_reference(need_ref):
     print("spatial pressure vs reference: %.2e (without the fringe term %.2e)" % (e, rel(gp0[keep], rp[keep])))
     assert e <= 1e-10
     assert rel(gp0[keep], rp[keep]) > 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_spatial_shards_and_graphs_equal_one_direct_context(precision):
+    """The fringe under the multi-GPU decomposition (two shard contexts,
+    emulated on one device: each applies the fringe on its own xz-planes) and
+    under CUDA-graph replay (the fringe is part of the captured launch
+    pattern) gives the state of one context launching directly, bit for bit."""
+    import os
+    from simson_b200.shard import LocalShards
+    u, v, w = channel_field(NX, NY, NZ, XL, ZL, 0.05, 24)
+
+    def make():
+        ch = _gpu(NX, NY, NZ, precision)
+        ch.set_velocity(u, v, w)
+        ch.prhs()
+        return ch
+
+    old = os.environ.get("SIMSON_GRAPHS")
+    os.environ["SIMSON_GRAPHS"] = "0"
+    try:
+        one = make()
+    finally:
+        if old is None:
+            os.environ.pop("SIMSON_GRAPHS")
+        else:
+            os.environ["SIMSON_GRAPHS"] = old
+    try:
+        one.step(3)
+        ref = one.state(7)
+    finally:
+        one.close()
+    graph = make()
+    try:
+        graph.step(3)
+        got_graph = graph.state(7)
+    finally:
+        graph.close()
+    sh = LocalShards(make, 2, "cuda:0")
+    try:
+        sh.step(3)
+        got_sh = sh.state(7)
+    finally:
+        sh.close()
+    for k in range(7):
+        assert np.array_equal(got_graph[k], ref[k]), k
+        assert np.array_equal(got_sh[k], ref[k]), k
