@@ -76,18 +76,63 @@ SB_HD inline void cheb_deriv(Col b, Col a, int n) {
   bp[(size_t)(n - 1) * sb] = 0.0;
 }
 
+// The lam-independent factors of the tau rows (bla/setmacrhs.f) and of the
+// tau right-hand side, per 1-based row index i, as FP64 tables: IEEE
+// division is correctly rounded, so an entry equals the quotient computed in
+// place and the solves keep their arithmetic bit for bit, without the FP64
+// divisions in their serial sweeps.  Rows from TAU_TAB_N on are computed.
+constexpr int TAU_TAB_N = 640;
+struct TauTab {
+  double c[TAU_TAB_N];   // -0.25 (i = 1), -0.25 / (i (i + 1))
+  double d[TAU_TAB_N];   // 0.5 / (i (i + 2))
+  double e[TAU_TAB_N];   // -0.25 / ((i + 1)(i + 2))
+  double ra[TAU_TAB_N];  // 0.25 / ((i - 2)(i - 1)), i >= 4 (0 below)
+  double rb[TAU_TAB_N];  // -0.5 / ((i - 2) i), i >= 3
+  double rc[TAU_TAB_N];  // 0.25 / ((i - 1) i), i >= 2
+};
+constexpr TauTab tau_tab_make() {
+  TauTab t{};
+  for (int i = 1; i < TAU_TAB_N; ++i) {
+    const double di = (double)i;
+    t.c[i] = (i == 1) ? -0.25 : -0.25 / (di * (di + 1.0));
+    t.d[i] = 0.5 / (di * (di + 2.0));
+    t.e[i] = -0.25 / ((di + 1.0) * (di + 2.0));
+    t.ra[i] = (i >= 4) ? 0.25 / ((di - 2.0) * (di - 1.0)) : 0.0;
+    t.rb[i] = (i >= 3) ? -0.5 / ((di - 2.0) * di) : 0.0;
+    t.rc[i] = (i >= 2) ? 0.25 / ((di - 1.0) * di) : 0.0;
+  }
+  return t;
+}
+inline constexpr TauTab kTauHost = tau_tab_make();
+#ifdef __CUDACC__
+// read with one row index per warp at a time (the thread-per-pencil sweeps):
+// constant-cache broadcasts
+__constant__ const TauTab kTauConst = tau_tab_make();
+#endif
+#ifdef __CUDA_ARCH__
+#define SB_TAUTAB kTauConst
+#else
+#define SB_TAUTAB kTauHost
+#endif
+
 // Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
 // (1-based row index i as in bla/setmacrhs.f).
 template <class S>
 SB_HD __forceinline__ S tau_c(int i, S lam) {
+  if constexpr (std::is_same<S, double>::value)
+    if (i < TAU_TAB_N) return SB_TAUTAB.c[i] * lam;
   return (i == 1) ? (S)-0.25 * lam : ((S)-0.25 / ((S)i * ((S)i + (S)1.0))) * lam;
 }
 template <class S>
 SB_HD __forceinline__ S tau_d(int i, S lam) {
+  if constexpr (std::is_same<S, double>::value)
+    if (i < TAU_TAB_N) return 1.0 + SB_TAUTAB.d[i] * lam;
   return (S)1.0 + ((S)0.5 / ((S)i * ((S)i + (S)2.0))) * lam;
 }
 template <class S>
 SB_HD __forceinline__ S tau_e(int i, S lam) {
+  if constexpr (std::is_same<S, double>::value)
+    if (i < TAU_TAB_N) return SB_TAUTAB.e[i] * lam;
   return ((S)-0.25 / (((S)i + (S)1.0) * ((S)i + (S)2.0))) * lam;
 }
 
@@ -184,9 +229,16 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       if (!FAST && !CPC) wtp[(size_t)(i - 1) * ws] = wnew;
     }
     const S di = (S)i;
-    const S ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
-    const S cb = (S)-0.5 / ((di - (S)2.0) * di);
-    const S cc = (S)0.25 / ((di - (S)1.0) * di);
+    S ca, cb, cc;
+    if (std::is_same<S, double>::value && i < TAU_TAB_N) {
+      ca = (S)SB_TAUTAB.ra[i];  // 0 at i = 3
+      cb = (S)SB_TAUTAB.rb[i];
+      cc = (S)SB_TAUTAB.rc[i];
+    } else {
+      ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
+      cb = (S)-0.5 / ((di - (S)2.0) * di);
+      cc = (S)0.25 / ((di - (S)1.0) * di);
+    }
     const S e2 = (i <= n - 4) ? tau_e(i - 2, lam) : (S)0.0;
 #pragma unroll
     for (int q = 0; q < M; ++q) {
