@@ -103,11 +103,20 @@ __device__ __forceinline__ void wderiv(const double2 (&a)[R], double2 (&b)[R], i
 // Tau-system row of Chebyshev coefficient j >= 2 (1-based row i = j + 1):
 // c x_{j-2} + d x_j + e x_{j+2} = rhs (tau_c/d/e of bla/setmacrhs.f with the
 // truncation of the last rows, as tau_solve eliminates them).
+// The lam-independent factors come from the global table (each lane reads
+// its own rows; rows beyond it are computed).
 __device__ __forceinline__ void wtau_row(int j, int n, double lam, double& c, double& d, double& e) {
   const int i = j + 1;
-  c = tau_c(i - 2, lam);
-  d = (i <= n - 2) ? tau_d(i - 2, lam) : 1.0;
-  e = (i <= n - 4) ? tau_e(i - 2, lam) : 0.0;
+  const int m = i - 2;
+  if (m >= 1 && m < TAU_TAB_N) {
+    c = __ldg(&kTauGlobal.c[m]) * lam;
+    d = (i <= n - 2) ? 1.0 + __ldg(&kTauGlobal.d[m]) * lam : 1.0;
+    e = (i <= n - 4) ? __ldg(&kTauGlobal.e[m]) * lam : 0.0;
+    return;
+  }
+  c = tau_c(m, lam);
+  d = (i <= n - 2) ? tau_d(m, lam) : 1.0;
+  e = (i <= n - 4) ? tau_e(m, lam) : 0.0;
 }
 
 // Solves (D^2 - lam) x_q = f_q, q < NC, with the boundary rows
@@ -140,6 +149,10 @@ __device__ __forceinline__ void wtau(double lam, int n, double (&w)[NC + 1][R], 
         const double fm2 = fr[r], f0 = fr[r + 2], fp2 = fr[r + 4];
         if (i == 3) {
           v = 0.25 * fm2 + fp2 / 24.0 - f0 / 6.0;
+        } else if (i < TAU_TAB_N) {
+          v = __ldg(&kTauGlobal.ra[i]) * fm2;
+          if (i <= n - 2) v += __ldg(&kTauGlobal.rb[i]) * f0;
+          if (i <= n - 4) v += __ldg(&kTauGlobal.rc[i]) * fp2;
         } else {
           const double di = (double)i;
           v = (0.25 / ((di - 2.0) * (di - 1.0))) * fm2;

@@ -82,57 +82,72 @@ SB_HD inline void cheb_deriv(Col b, Col a, int n) {
 // place and the solves keep their arithmetic bit for bit, without the FP64
 // divisions in their serial sweeps.  Rows from TAU_TAB_N on are computed.
 constexpr int TAU_TAB_N = 640;
+// The FP32 instance (the mixed path's omega_y / phi solve) takes its own
+// table of the same quotients evaluated in FP32.
+template <class S>
 struct TauTab {
-  double c[TAU_TAB_N];   // -0.25 (i = 1), -0.25 / (i (i + 1))
-  double d[TAU_TAB_N];   // 0.5 / (i (i + 2))
-  double e[TAU_TAB_N];   // -0.25 / ((i + 1)(i + 2))
-  double ra[TAU_TAB_N];  // 0.25 / ((i - 2)(i - 1)), i >= 4 (0 below)
-  double rb[TAU_TAB_N];  // -0.5 / ((i - 2) i), i >= 3
-  double rc[TAU_TAB_N];  // 0.25 / ((i - 1) i), i >= 2
+  S c[TAU_TAB_N];   // -0.25 (i = 1), -0.25 / (i (i + 1))
+  S d[TAU_TAB_N];   // 0.5 / (i (i + 2))
+  S e[TAU_TAB_N];   // -0.25 / ((i + 1)(i + 2))
+  S ra[TAU_TAB_N];  // 0.25 / ((i - 2)(i - 1)), i >= 4 (0 below)
+  S rb[TAU_TAB_N];  // -0.5 / ((i - 2) i), i >= 3
+  S rc[TAU_TAB_N];  // 0.25 / ((i - 1) i), i >= 2
 };
-constexpr TauTab tau_tab_make() {
-  TauTab t{};
+template <class S>
+constexpr TauTab<S> tau_tab_make() {
+  TauTab<S> t{};
   for (int i = 1; i < TAU_TAB_N; ++i) {
-    const double di = (double)i;
-    t.c[i] = (i == 1) ? -0.25 : -0.25 / (di * (di + 1.0));
-    t.d[i] = 0.5 / (di * (di + 2.0));
-    t.e[i] = -0.25 / ((di + 1.0) * (di + 2.0));
-    t.ra[i] = (i >= 4) ? 0.25 / ((di - 2.0) * (di - 1.0)) : 0.0;
-    t.rb[i] = (i >= 3) ? -0.5 / ((di - 2.0) * di) : 0.0;
-    t.rc[i] = (i >= 2) ? 0.25 / ((di - 1.0) * di) : 0.0;
+    const S di = (S)i;
+    t.c[i] = (i == 1) ? (S)-0.25 : (S)-0.25 / (di * (di + (S)1.0));
+    t.d[i] = (S)0.5 / (di * (di + (S)2.0));
+    t.e[i] = (S)-0.25 / ((di + (S)1.0) * (di + (S)2.0));
+    t.ra[i] = (i >= 4) ? (S)0.25 / ((di - (S)2.0) * (di - (S)1.0)) : (S)0.0;
+    t.rb[i] = (i >= 3) ? (S)-0.5 / ((di - (S)2.0) * di) : (S)0.0;
+    t.rc[i] = (i >= 2) ? (S)0.25 / ((di - (S)1.0) * di) : (S)0.0;
   }
   return t;
 }
-inline constexpr TauTab kTauHost = tau_tab_make();
+inline constexpr TauTab<double> kTauHost = tau_tab_make<double>();
+inline constexpr TauTab<float> kTauHostF = tau_tab_make<float>();
 #ifdef __CUDACC__
 // read with one row index per warp at a time (the thread-per-pencil sweeps):
 // constant-cache broadcasts
-__constant__ const TauTab kTauConst = tau_tab_make();
+__constant__ const TauTab<double> kTauConst = tau_tab_make<double>();
+__constant__ const TauTab<float> kTauConstF = tau_tab_make<float>();
+// the same in global memory, for reads whose row index differs across a
+// warp (the warp-per-pencil kernels: the constant cache would serialise them)
+__device__ const TauTab<double> kTauGlobal = tau_tab_make<double>();
 #endif
 #ifdef __CUDA_ARCH__
 #define SB_TAUTAB kTauConst
+#define SB_TAUTAB_F kTauConstF
 #else
 #define SB_TAUTAB kTauHost
+#define SB_TAUTAB_F kTauHostF
 #endif
+// the table of the solve's scalar type
+template <class S>
+SB_HD __forceinline__ const TauTab<S>& tau_tab();
+template <>
+SB_HD __forceinline__ const TauTab<double>& tau_tab<double>() { return SB_TAUTAB; }
+template <>
+SB_HD __forceinline__ const TauTab<float>& tau_tab<float>() { return SB_TAUTAB_F; }
 
 // Tau-method coefficients of (D^2 - lam) for the quasi-tridiagonal rows
 // (1-based row index i as in bla/setmacrhs.f).
 template <class S>
 SB_HD __forceinline__ S tau_c(int i, S lam) {
-  if constexpr (std::is_same<S, double>::value)
-    if (i < TAU_TAB_N) return SB_TAUTAB.c[i] * lam;
+  if (i < TAU_TAB_N) return tau_tab<S>().c[i] * lam;
   return (i == 1) ? (S)-0.25 * lam : ((S)-0.25 / ((S)i * ((S)i + (S)1.0))) * lam;
 }
 template <class S>
 SB_HD __forceinline__ S tau_d(int i, S lam) {
-  if constexpr (std::is_same<S, double>::value)
-    if (i < TAU_TAB_N) return 1.0 + SB_TAUTAB.d[i] * lam;
+  if (i < TAU_TAB_N) return (S)1.0 + tau_tab<S>().d[i] * lam;
   return (S)1.0 + ((S)0.5 / ((S)i * ((S)i + (S)2.0))) * lam;
 }
 template <class S>
 SB_HD __forceinline__ S tau_e(int i, S lam) {
-  if constexpr (std::is_same<S, double>::value)
-    if (i < TAU_TAB_N) return SB_TAUTAB.e[i] * lam;
+  if (i < TAU_TAB_N) return tau_tab<S>().e[i] * lam;
   return ((S)-0.25 / (((S)i + (S)1.0) * ((S)i + (S)2.0))) * lam;
 }
 
@@ -230,10 +245,10 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     }
     const S di = (S)i;
     S ca, cb, cc;
-    if (std::is_same<S, double>::value && i < TAU_TAB_N) {
-      ca = (S)SB_TAUTAB.ra[i];  // 0 at i = 3
-      cb = (S)SB_TAUTAB.rb[i];
-      cc = (S)SB_TAUTAB.rc[i];
+    if (i < TAU_TAB_N) {
+      ca = tau_tab<S>().ra[i];  // 0 at i = 3
+      cb = tau_tab<S>().rb[i];
+      cc = tau_tab<S>().rc[i];
     } else {
       ca = (i == 3) ? (S)0.0 : (S)0.25 / ((di - (S)2.0) * (di - (S)1.0));
       cb = (S)-0.5 / ((di - (S)2.0) * di);
@@ -536,8 +551,12 @@ __global__ void __launch_bounds__(128) k_pencil_hom(PencilBufs B, Dims g, const 
 // the forcing in float.  The fourth-order v solve, the superposition and every
 // derivative are FP64 in both.  VHc, HS: this stage's homogeneous solution
 // (k_pencil_hom).
+// resident CTAs of 128 threads per SM the register budget is sized for
+#ifndef SB_PENCIL_MINB
+#define SB_PENCIL_MINB 4
+#endif
 template <class IO, class SC, class FC>
-__global__ void __launch_bounds__(128, 4) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
+__global__ void __launch_bounds__(128, SB_PENCIL_MINB) k_pencil(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                 const double* __restrict__ beta, double re, RKc rk,
                                                 const double* __restrict__ VHc, const double* __restrict__ HS,
                                                 double* __restrict__ CF) {
