@@ -10,7 +10,9 @@
 //   tau_ij = s_out * (W3 h2 + b3)   (6: 11 12 13 22 23 33)
 //
 // Arithmetic: weights, x, h1, h2 rounded to BF16 (round to nearest even),
-// products accumulated in FP32 in tensor memory, biases and tanh in FP32.
+// products accumulated in FP32 in tensor memory, biases in FP32, tanh by the
+// hardware approximation (tanh.approx.f32, relative error ~2^-11, below the
+// BF16 rounding of the activations that follows it).
 //
 // One CTA of 128 threads takes 128 points at a time (thread t = row t):
 // each layer is tcgen05.mma kind::f16 with M = 128 (K = 16 steps; N = 64, 64,
@@ -147,6 +149,16 @@ constexpr int MLP_SMEM_USED = MLP_SMEM_BAR + 16;
 constexpr int MLP_SMEM_LAUNCH = 56 * 1024;
 constexpr int MLP_WAIT_LIMIT = 1 << 20;
 
+__device__ __forceinline__ float mlp_tanh(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// planes whose wall-distance feature is tabulated per CTA (larger grids
+// compute it per point)
+constexpr int MLP_YTAB = 512;
+
 __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* A1 = sm + MLP_SMEM_A1;
@@ -159,7 +171,14 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(sm + MLP_SMEM_BAR);
   unsigned* tslot = reinterpret_cast<unsigned*>(sm + MLP_SMEM_BAR + 8);
   __shared__ int s_fail;
+  __shared__ float s_ywall[MLP_YTAB];  // x_9 = s_y (1 - |y|) of each plane
   const int t = threadIdx.x, warp = t >> 5;
+  const bool ytab = a.mode == 1 && a.nyp <= MLP_YTAB;
+  if (ytab)
+    for (int y = t; y < a.nyp; y += blockDim.x) {
+      const double eta = cos(3.1415926535897932385 * (double)y / (double)(a.nyp - 1));
+      s_ywall[y] = a.s_y * (float)(1.0 - fabs(eta));
+    }
 
   // weights and biases into shared memory
   for (int i = t; i < MLP_IMAGE_BYTES / 16; i += blockDim.x)
@@ -209,8 +228,12 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) x[k] = a.s_in * (float)a.grad[(long long)k * a.n + i];
         const int y = (int)(i / a.plane);
-        const double eta = cos(3.1415926535897932385 * (double)y / (double)(a.nyp - 1));
-        x[9] = a.s_y * (float)(1.0 - fabs(eta));
+        if (ytab) {
+          x[9] = s_ywall[y];
+        } else {
+          const double eta = cos(3.1415926535897932385 * (double)y / (double)(a.nyp - 1));
+          x[9] = a.s_y * (float)(1.0 - fabs(eta));
+        }
       }
     }
     mlp_store8(A1, t, 0, 16, x);
@@ -245,7 +268,7 @@ __global__ void __launch_bounds__(128) k_sgs_mlp(MlpArgs a) {
           mlp_ld16(tmem + lane_base + dcol + 16 * c, v);
           mlp_ld_wait();
 #pragma unroll
-          for (int q = 0; q < 16; ++q) v[q] = tanhf(v[q] + b[16 * c + q]);
+          for (int q = 0; q < 16; ++q) v[q] = mlp_tanh(v[q] + b[16 * c + q]);
           mlp_store8(A, t, 2 * c, MLP_H, v);
           mlp_store8(A, t, 2 * c + 1, MLP_H, v + 8);
         }
