@@ -29,8 +29,20 @@ namespace sb {
 // NT threads per CTA; N = 0: runtime plan, any block size.
 // (the FP64 fixed-length variant is held to three CTAs per SM: unbounded it
 // takes ~130 registers and one CTA per SM)
+// SB_ZINV_MINB, SB_ZFWD_MINB: the same for the FP32 variants of the long
+// transforms (N >= 288).  Four CTAs per SM (z-inverse 62 -> 55 registers,
+// z-forward 94 -> 52, no spills) measured faster than the compiler's choice
+// of three and two at 384x193x384: 0.547 -> 0.510 and 0.328 -> 0.269 ms;
+// five measured slower, and at N = 96 the cap cost 2 %.
+#ifndef SB_ZINV_MINB
+#define SB_ZINV_MINB 4
+#endif
+#ifndef SB_ZFWD_MINB
+#define SB_ZFWD_MINB 4
+#endif
 template <class T, int KB, class S, int N = 0, int NT = 0>
-__global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) ? 3 : 0)
+__global__ void __launch_bounds__(NT > 0 ? NT : 256,
+                                  (NT > 0 && sizeof(T) == 8) ? 3 : (NT > 0 && N >= 288 ? SB_ZINV_MINB : 0))
     k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
            FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ alfa,
            const double* __restrict__ beta, int drop_mean) {
@@ -123,8 +135,14 @@ __device__ __forceinline__ void fringe_apply(const Fringe& fr, int j, int y, int
 }
 
 // N > 0: the x length g.nxp is N (compile-time plan, NT threads per CTA).
+// SB_XPASS_MINB: resident CTAs per SM the FP32 fixed-length variant's
+// register budget is sized for (0: the compiler's choice, three CTAs of 448
+// threads at 40 registers; four at 32 registers measured the same)
+#ifndef SB_XPASS_MINB
+#define SB_XPASS_MINB 0
+#endif
 template <class T, int RB, int N = 0, int NT = 0>
-__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+__global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 4) ? SB_XPASS_MINB : 0)
     k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb, Dims g,
             FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ dyi, double dxi,
             double dzi, double rot, unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean,
@@ -270,8 +288,12 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256)
 
 // mean != nullptr: add nxp*nzp*(W Omega_x - U (Omega_z + 2 rot)) to the
 // kx = kz = 0 mode of H2 in FP64 (the mean-mean product left out by k_xpass).
+#ifndef SB_ZFWD64_MINB
+#define SB_ZFWD64_MINB 0
+#endif
 template <class T, int KB, class S, int N = 0, int NT = 0>
-__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+__global__ void __launch_bounds__(NT > 0 ? NT : 256,
+                                  NT > 0 ? (sizeof(T) == 4 ? (N >= 288 ? SB_ZFWD_MINB : 0) : SB_ZFWD64_MINB) : 0)
     k_zfwd(const typename C2<T>::type* __restrict__ xb, typename C2<S>::type* __restrict__ st, Dims g,
            FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ mean, double rot) {
   typedef typename C2<T>::type V;

@@ -80,6 +80,9 @@ inline void xpass_n(dim3 grid, size_t smem, cudaStream_t st, const typename C2<T
                     const double* dyi, double dxi, double dzi, double rot, unsigned long long* cfl,
                     const double* mean, Fringe fr) {
   cudaFuncSetAttribute(k_xpass<T, RB, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+#ifdef SB_XPASS_CARVEOUT
+  cudaFuncSetAttribute(k_xpass<T, RB, N, NT>, cudaFuncAttributePreferredSharedMemoryCarveout, SB_XPASS_CARVEOUT);
+#endif
   k_xpass<T, RB, N, NT><<<grid, NT, smem, st>>>(zb, xb, g, plan, tw, dyi, dxi, dzi, rot, cfl, mean, fr);
 }
 template <class T, int RB, int NT0>
