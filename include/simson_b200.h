@@ -271,10 +271,10 @@ int sgpu_box_filter_sample(sgpu_ctx* ctx, int factor, float* features, float* ta
  * uploading all 7 slots from ur, ui (reference layout, as sgpu_upload_state;
  * pinned host memory for full speed) and downloading the result into them
  * (as sgpu_download_state), so the host arrays are current after every step.
- * The copies of consecutive steps are pipelined per slot: the upload of slot
- * k for step n+1 waits only for slot k of step n to be back on the host and
- * overlaps the download of the other slots (PCIe is full duplex).  Returns
- * after the last download.  Not on a shard. */
+ * The copies of consecutive steps are pipelined: each slot moves in eight
+ * pieces, and a piece of step n+1's upload waits only for the same piece of
+ * step n to be back on the host, overlapping the rest of the download (PCIe
+ * is full duplex).  Returns after the last download.  Not on a shard. */
 int sgpu_offload_steps(sgpu_ctx* ctx, double* ur, double* ui, int nsteps);
 
 /* Multi-GPU runs (one context per GPU, the reference's MPI decomposition of

@@ -384,8 +384,20 @@ __device__ __forceinline__ void wtau(double lam, int n, double (&w)[NC + 1][R], 
 // plane excluded).  IO: storage of H and of the outputs (float2 on the
 // mixed path); FC: rounding of the forcing columns h_v, h_omega and of the
 // right-hand sides (float on the mixed path, as k_pencil stores them).
+// SB_PWARP_MINB4/8: resident CTAs per SM the register budget is sized for,
+// by rows per lane (0: the compiler's choice).  R = 4 (ny <= 127): four CTAs
+// at 128 registers (a 64-byte spill) keep every pencil of the 64x97x64 LES
+// grid resident at once, where the compiler's 166-174 registers left two or
+// three: its step 0.648 -> 0.553 ms (FP64), 0.487 -> 0.401 ms (mixed).
+#ifndef SB_PWARP_MINB4
+#define SB_PWARP_MINB4 4
+#endif
+#ifndef SB_PWARP_MINB8
+#define SB_PWARP_MINB8 0
+#endif
 template <class IO, class FC, int R>
-__global__ void __launch_bounds__(128) k_pencil_w(PencilBufs B, Dims g, const double* __restrict__ alfa,
+__global__ void __launch_bounds__(128, R <= 4 ? SB_PWARP_MINB4 : SB_PWARP_MINB8)
+    k_pencil_w(PencilBufs B, Dims g, const double* __restrict__ alfa,
                                                   const double* __restrict__ beta, double re, RKc rk) {
   const int lane = threadIdx.x & 31;
   const int p = g.p0 + (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);

@@ -40,9 +40,15 @@ namespace sb {
 #ifndef SB_ZFWD_MINB
 #define SB_ZFWD_MINB 4
 #endif
+// SB_ZINV64_MINB: the FP64 variant (three CTAs of 288 threads at 72
+// registers; four, at 56, measured 1.116 -> 1.148 ms at 384x193x384)
+#ifndef SB_ZINV64_MINB
+#define SB_ZINV64_MINB 3
+#endif
 template <class T, int KB, class S, int N = 0, int NT = 0>
 __global__ void __launch_bounds__(NT > 0 ? NT : 256,
-                                  (NT > 0 && sizeof(T) == 8) ? 3 : (NT > 0 && N >= 288 ? SB_ZINV_MINB : 0))
+                                  (NT > 0 && sizeof(T) == 8) ? SB_ZINV64_MINB
+                                                             : (NT > 0 && N >= 288 ? SB_ZINV_MINB : 0))
     k_zinv(const typename C2<S>::type* __restrict__ st, typename C2<T>::type* __restrict__ zb, Dims g,
            FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ alfa,
            const double* __restrict__ beta, int drop_mean) {
@@ -141,8 +147,15 @@ __device__ __forceinline__ void fringe_apply(const Fringe& fr, int j, int y, int
 #ifndef SB_XPASS_MINB
 #define SB_XPASS_MINB 0
 #endif
+// SB_XPASS64_MINB: the same for the FP64 fixed-length variant (0: the
+// compiler's choice, four CTAs of 224 threads at 66 registers; five, at 56
+// registers and a 20-byte spill, measured 2.24 -> 2.34 ms at 384x193x384)
+#ifndef SB_XPASS64_MINB
+#define SB_XPASS64_MINB 0
+#endif
 template <class T, int RB, int N = 0, int NT = 0>
-__global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 4) ? SB_XPASS_MINB : 0)
+__global__ void __launch_bounds__(NT > 0 ? NT : 256,
+                                  NT > 0 ? (sizeof(T) == 4 ? SB_XPASS_MINB : SB_XPASS64_MINB) : 0)
     k_xpass(const typename C2<T>::type* __restrict__ zb, typename C2<T>::type* __restrict__ xb, Dims g,
             FFTPlan plan, const typename C2<T>::type* __restrict__ tw, const double* __restrict__ dyi, double dxi,
             double dzi, double rot, unsigned long long* __restrict__ cfl_bits, const double* __restrict__ mean,
@@ -288,8 +301,10 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 4) 
 
 // mean != nullptr: add nxp*nzp*(W Omega_x - U (Omega_z + 2 rot)) to the
 // kx = kz = 0 mode of H2 in FP64 (the mean-mean product left out by k_xpass).
+// FP64 z-forward: three CTAs per SM (102 -> 72 registers, an 8-byte spill)
+// measured 0.710 -> 0.633 ms at 384x193x384 against the compiler's two
 #ifndef SB_ZFWD64_MINB
-#define SB_ZFWD64_MINB 0
+#define SB_ZFWD64_MINB 3
 #endif
 template <class T, int KB, class S, int N = 0, int NT = 0>
 __global__ void __launch_bounds__(NT > 0 ? NT : 256,

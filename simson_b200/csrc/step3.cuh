@@ -406,8 +406,15 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
 // N > 0: the transform length 2(ny-1) is N, with the compile-time plan and
 // NT threads per CTA; its first pass reads the columns (even extension
 // folded into the index) and its last pass writes the n kept coefficients.
+// SB_CHEB64_MINB: resident CTAs per SM the FP64 fixed-length variant's
+// register budget is sized for (0: the compiler's choice, 56 registers at
+// 256 threads; five CTAs, at 48 registers and a 16-byte spill, measured
+// 0.82 -> 0.95 ms for the five-field inverse at 384x193x384)
+#ifndef SB_CHEB64_MINB
+#define SB_CHEB64_MINB 0
+#endif
 template <class T, int PB, class SI, class SO, int N = 0, int NT = 0>
-__global__ void __launch_bounds__(NT > 0 ? NT : 256)
+__global__ void __launch_bounds__(NT > 0 ? NT : 256, (NT > 0 && sizeof(T) == 8) ? SB_CHEB64_MINB : 0)
     k_cheb(const typename C2<SI>::type* __restrict__ in, size_t in_fs, typename C2<SO>::type* __restrict__ out,
            size_t out_fs, Dims g, int inverse, double scale, FFTPlan plan, const typename C2<T>::type* __restrict__ tw,
            int skip_oddball) {
