@@ -274,7 +274,9 @@ int sgpu_box_filter_sample(sgpu_ctx* ctx, int factor, float* features, float* ta
  * The copies of consecutive steps are pipelined: each slot moves in eight
  * pieces, and a piece of step n+1's upload waits only for the same piece of
  * step n to be back on the host, overlapping the rest of the download (PCIe
- * is full duplex).  Returns after the last download.  Not on a shard. */
+ * is full duplex).  Without LES, the first substep's nonlinear step starts
+ * once slots 0-4 are on the device, while p_v and p_omega still upload.
+ * Returns after the last download.  Not on a shard. */
 int sgpu_offload_steps(sgpu_ctx* ctx, double* ur, double* ui, int nsteps);
 
 /* Multi-GPU runs (one context per GPU, the reference's MPI decomposition of
