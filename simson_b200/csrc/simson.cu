@@ -166,7 +166,13 @@ struct sgpu_ctx {
   long long launches = 0;
   // threads per CTA of the FFT kernels (measured on B200: 256 everywhere but
   // the FP64 x-pass, whose register use prefers 128)
-  static constexpr int kb = 4, rb = 1, pb = 4, fft_threads = 256, xpass64_threads = 128;
+  // rb: z rows per CTA of the FP64 x pass; two (the H3 of both rows paired in
+  // one complex FFT, 72 registers, two CTAs of 448 threads per SM) measured
+  // 2.24 -> 2.43 ms at 384x193x384
+#ifndef SB_XPASS64_RB
+#define SB_XPASS64_RB 1
+#endif
+  static constexpr int kb = 4, rb = SB_XPASS64_RB, pb = 4, fft_threads = 256, xpass64_threads = 128;
   static constexpr int kbf = MIXED_KB, rbf = MIXED_RB, pbf = 8;  // FP32 tiles (mixed.h)
   // optional per-kernel timing (sgpu_profile): event pairs around each launch
   bool prof = false;
