@@ -88,6 +88,19 @@ SB_HD __forceinline__ void dft3(V& a, V& b, V& c, int s) {
   c = csub(m, r);
 }
 
+// dft3 of (a, 0, c): the same operations as dft3 with b = 0 and the terms
+// that add or subtract that zero left out (equal results up to the sign of
+// an exact zero)
+template <class T, class V>
+SB_HD __forceinline__ void dft3_zmid(V& a, V& b, V& c, int s) {
+  const V dif = V{-c.x, -c.y};
+  const V m = V{a.x - (T)0.5 * c.x, a.y - (T)0.5 * c.y};
+  const V r = cmuli(V{(T)SB_S3 * dif.x, (T)SB_S3 * dif.y}, s);
+  a = cadd(a, c);
+  b = cadd(m, r);
+  c = csub(m, r);
+}
+
 template <class T, class V>
 SB_HD __forceinline__ void dft4(V& a, V& b, V& c, V& d, int s) {
   V a0 = cadd(a, c), a1 = csub(a, c);
@@ -192,6 +205,38 @@ SB_HD __forceinline__ void dft_small(V* v, int R, int s) {
     v[2] = cadd(p2, q2);
     v[3] = csub(p2, q2);
   }
+}
+
+// dft_small with the inputs of mask ZM (bit r: v[r]) known to be zero: the
+// radix-9 butterfly of a first pass whose middle third is the zero band
+// skips the additions of those zeros; other radices use dft_small (the zeros
+// are still not loaded)
+template <class T, class V, unsigned ZM>
+SB_HD __forceinline__ void dft_small_z(V* v, int R, int s) {
+  if constexpr ((ZM & 0x38u) == 0x38u) {
+    if (R == 9) {
+      V a0 = v[0], a1 = v[3], a2 = v[6];
+      V b0 = v[1], b1 = v[4], b2 = v[7];
+      V c0 = v[2], c1 = v[5], c2 = v[8];
+      dft3_zmid<T, V>(a0, a1, a2, s);
+      dft3_zmid<T, V>(b0, b1, b2, s);
+      dft3_zmid<T, V>(c0, c1, c2, s);
+      const V w1 = V{(T)SB_C9_1, (T)(s * SB_S9_1)}, w2 = V{(T)SB_C9_2, (T)(s * SB_S9_2)};
+      const V w4 = V{(T)SB_C9_4, (T)(s * SB_S9_4)};
+      b1 = cmul(b1, w1);
+      b2 = cmul(b2, w2);
+      c1 = cmul(c1, w2);
+      c2 = cmul(c2, w4);
+      dft3<T, V>(a0, b0, c0, s);
+      dft3<T, V>(a1, b1, c1, s);
+      dft3<T, V>(a2, b2, c2, s);
+      v[0] = a0; v[3] = b0; v[6] = c0;
+      v[1] = a1; v[4] = b1; v[7] = c1;
+      v[2] = a2; v[5] = b2; v[8] = c2;
+      return;
+    }
+  }
+  dft_small<T, V>(v, R, s);
 }
 
 // One Stockham pass: src -> dst, sub-transform length Ns -> Ns*R.  B (the
@@ -385,6 +430,32 @@ constexpr CPlanData cplan_make(int n) {
   return p;
 }
 
+// The 3/2 zero padding of the step-2 transforms (n = 3/2 of the stored
+// modes): an inverse transform's input is zero on the band [n/3, 2n/3] of
+// padded indices, a forward transform's output is dropped on [n/3, 2n/3).
+// pad_zero_mask: bit r set when input block r of the first pass (indices
+// [r n/R, (r+1) n/R)) lies in the zero band; pad_drop_mask: bit r set when
+// output block r of the last pass (indices [r Ns, (r+1) Ns)) lies in the
+// dropped band.
+template <int N>
+constexpr unsigned pad_zero_mask() {
+  constexpr CPlanData p = cplan_make(N);
+  const int R = p.radix[0], nb = N / R;
+  unsigned m = 0;
+  for (int r = 0; r < R; ++r)
+    if (3 * r * nb >= N && 3 * ((r + 1) * nb - 1) <= 2 * N) m |= 1u << r;
+  return m;
+}
+template <int N>
+constexpr unsigned pad_drop_mask() {
+  constexpr CPlanData p = cplan_make(N);
+  const int R = p.radix[p.npass - 1], ns = p.ns[p.npass - 1];
+  unsigned m = 0;
+  for (int r = 0; r < R; ++r)
+    if (3 * r * ns >= N && 3 * (r + 1) * ns <= 2 * N) m |= 1u << r;
+  return m;
+}
+
 // largest number of butterflies of one column in any pass (n / smallest radix)
 constexpr int cplan_max_nb(int n) {
   const CPlanData p = cplan_make(n);
@@ -395,7 +466,8 @@ constexpr int cplan_max_nb(int n) {
 
 // One radix-R pass of an N-point transform over B interleaved columns; work
 // items t0, t0 + NT, ...
-template <class T, int B, int N, int R, int NS, int S, int NT>
+// DM: outputs of the blocks in the mask are not stored (pad_drop_mask).
+template <class T, int B, int N, int R, int NS, int S, int NT, unsigned DM = 0>
 SB_HD __forceinline__ void cpass(const typename C2<T>::type* __restrict__ src, typename C2<T>::type* __restrict__ dst,
                                  const typename C2<T>::type* __restrict__ tw, int t0) {
   typedef typename C2<T>::type V;
@@ -418,14 +490,17 @@ SB_HD __forceinline__ void cpass(const typename C2<T>::type* __restrict__ src, t
     dft_small<T, V>(v, R, S);
     V* __restrict__ d = dst + (size_t)((jg * NS * R + jm) * B + b);
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[r * NS * B] = v[r];
+    for (int r = 0; r < R; ++r)
+      if (!(DM & (1u << r))) d[r * NS * B] = v[r];
   }
 }
 
 // All passes of the N-point transform of the B columns in src (dst is
 // scratch); returns the buffer holding the result.  On the device every pass
 // ends with a barrier (the caller syncs before the first).
-template <class T, int B, int N, int S, int NT, int P = 0>
+// DOUT: the output band that pad_drop_mask names is left unwritten (the
+// caller reads only the kept modes).
+template <class T, int B, int N, int S, int NT, int P = 0, bool DOUT = false>
 SB_HD __forceinline__ typename C2<T>::type* cfft(typename C2<T>::type* src, typename C2<T>::type* dst,
                                                  const typename C2<T>::type* __restrict__ tw, int t0) {
   constexpr CPlanData pl = cplan_make(N);
@@ -433,11 +508,12 @@ SB_HD __forceinline__ typename C2<T>::type* cfft(typename C2<T>::type* src, type
   if constexpr (P >= pl.npass) {
     return src;
   } else {
-    cpass<T, B, N, pl.radix[P], pl.ns[P], S, NT>(src, dst, tw, t0);
+    constexpr unsigned dm = (DOUT && P == pl.npass - 1) ? pad_drop_mask<N>() : 0u;
+    cpass<T, B, N, pl.radix[P], pl.ns[P], S, NT, dm>(src, dst, tw, t0);
 #ifdef __CUDA_ARCH__
     __syncthreads();
 #endif
-    return cfft<T, B, N, S, NT, P + 1>(dst, src, tw, t0);
+    return cfft<T, B, N, S, NT, P + 1, DOUT>(dst, src, tw, t0);
   }
 }
 
@@ -446,7 +522,11 @@ SB_HD __forceinline__ typename C2<T>::type* cfft(typename C2<T>::type* src, type
 // column b of its output.  The first pass of cfft_io reads the global arrays
 // through ld and its last pass writes them through st, so the data crosses
 // shared memory only between passes.
-template <class T, int B, int N, int R, int NS, int S, int NT, class Ld, class St>
+// ZM: inputs of the blocks in the mask are zero and not loaded
+// (pad_zero_mask, first pass); DM: outputs of the blocks in the mask are not
+// stored (pad_drop_mask, last pass).
+template <class T, int B, int N, int R, int NS, int S, int NT, unsigned ZM = 0, unsigned DM = 0, class Ld,
+          class St>
 SB_HD __forceinline__ void cpass_io(Ld ld, St st, const typename C2<T>::type* __restrict__ tw, int t0) {
   typedef typename C2<T>::type V;
   constexpr int nb = N / R;
@@ -463,12 +543,13 @@ SB_HD __forceinline__ void cpass_io(Ld ld, St st, const typename C2<T>::type* __
     const unsigned jm = j - jg * NS;
     V v[9];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = ld((int)(j + r * nb), (int)b);
+    for (int r = 0; r < R; ++r) v[r] = (ZM & (1u << r)) ? V{(T)0, (T)0} : ld((int)(j + r * nb), (int)b);
     if (NS > 1 && jm != 0) twiddle<T, R, S>(v, tw, (int)(jm * tstep));
-    dft_small<T, V>(v, R, S);
+    dft_small_z<T, V, ZM>(v, R, S);
     const int k0 = (int)(jg * NS * R + jm);
 #pragma unroll
-    for (int r = 0; r < R; ++r) st(k0 + r * NS, (int)b, v[r]);
+    for (int r = 0; r < R; ++r)
+      if (!(DM & (1u << r))) st(k0 + r * NS, (int)b, v[r]);
   }
 }
 
@@ -486,50 +567,56 @@ struct SmemSt {
 // N-point transform of B columns from ld to st (at least two passes);
 // buf0/buf1 hold the intermediate passes.  The caller syncs before reusing
 // the buffers.
-template <class T, int B, int N, int S, int NT, int P = 0, class Ld, class St>
+// ZIN: the input is zero on the band of pad_zero_mask (never loaded); DOUT:
+// st is never called on the band of pad_drop_mask.
+template <class T, int B, int N, int S, int NT, int P = 0, bool ZIN = false, bool DOUT = false, class Ld,
+          class St>
 SB_HD __forceinline__ void cfft_io(Ld ld, St st, typename C2<T>::type* buf0, typename C2<T>::type* buf1,
                                    const typename C2<T>::type* __restrict__ tw, int t0) {
   constexpr CPlanData pl = cplan_make(N);
   static_assert(pl.npass >= 2, "cfft_io needs at least two passes");
   if constexpr (P == 0) {
-    cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT>(ld, SmemSt<T, B>{buf0}, tw, t0);
+    cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT, ZIN ? pad_zero_mask<N>() : 0u>(ld, SmemSt<T, B>{buf0}, tw,
+                                                                                  t0);
 #ifdef __CUDA_ARCH__
     __syncthreads();
 #endif
-    cfft_io<T, B, N, S, NT, 1>(ld, st, buf0, buf1, tw, t0);
+    cfft_io<T, B, N, S, NT, 1, ZIN, DOUT>(ld, st, buf0, buf1, tw, t0);
   } else if constexpr (P == pl.npass - 1) {
-    cpass_io<T, B, N, pl.radix[P], pl.ns[P], S, NT>(SmemLd<T, B>{buf0}, st, tw, t0);
+    cpass_io<T, B, N, pl.radix[P], pl.ns[P], S, NT, 0u, DOUT ? pad_drop_mask<N>() : 0u>(SmemLd<T, B>{buf0}, st,
+                                                                                       tw, t0);
   } else {
     cpass_io<T, B, N, pl.radix[P], pl.ns[P], S, NT>(SmemLd<T, B>{buf0}, SmemSt<T, B>{buf1}, tw, t0);
 #ifdef __CUDA_ARCH__
     __syncthreads();
 #endif
-    cfft_io<T, B, N, S, NT, P + 1>(ld, st, buf1, buf0, tw, t0);
+    cfft_io<T, B, N, S, NT, P + 1, ZIN, DOUT>(ld, st, buf1, buf0, tw, t0);
   }
 }
 
 // First pass from ld, the others in shared memory; returns the buffer that
 // holds the result (ends with a barrier on the device).
-template <class T, int B, int N, int S, int NT, class Ld>
+template <class T, int B, int N, int S, int NT, bool ZIN = false, class Ld>
 SB_HD __forceinline__ typename C2<T>::type* cfft_ld(Ld ld, typename C2<T>::type* buf0, typename C2<T>::type* buf1,
                                                     const typename C2<T>::type* __restrict__ tw, int t0) {
   constexpr CPlanData pl = cplan_make(N);
-  cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT>(ld, SmemSt<T, B>{buf0}, tw, t0);
+  cpass_io<T, B, N, pl.radix[0], pl.ns[0], S, NT, ZIN ? pad_zero_mask<N>() : 0u>(ld, SmemSt<T, B>{buf0}, tw, t0);
 #ifdef __CUDA_ARCH__
   __syncthreads();
 #endif
   return cfft<T, B, N, S, NT, 1>(buf0, buf1, tw, t0);
 }
 
-// runtime plan (N == 0) or compile-time plan, same interface
-template <class T, int B, int N, int NT, int S>
+// runtime plan (N == 0) or compile-time plan, same interface (DOUT: as cfft,
+// compile-time plans only)
+template <class T, int B, int N, int NT, int S, bool DOUT = false>
 __device__ __forceinline__ typename C2<T>::type* fft_any(typename C2<T>::type* buf0, typename C2<T>::type* buf1,
                                                         const FFTPlan& plan,
                                                         const typename C2<T>::type* __restrict__ tw) {
   if constexpr (N == 0)
     return fft_columns_s<T, B, S>(buf0, buf1, plan, tw);
   else
-    return cfft<T, B, N, S, NT>(buf0, buf1, tw, threadIdx.x);
+    return cfft<T, B, N, S, NT, 0, DOUT>(buf0, buf1, tw, threadIdx.x);
 }
 
 }  // namespace sb

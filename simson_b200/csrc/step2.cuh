@@ -94,8 +94,10 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256,
     V* __restrict__ out = zb + ((size_t)f * g.nyp + y) * nzp * g.nx2;
     if constexpr (N > 0) {
       // the first pass reads the state, the last writes zb: shared memory
-      // only between passes
-      cfft_io<T, KB, N, 1, NT>([&](int m, int b) { return load_elem(f, m, b); },
+      // only between passes; FP32: the zero band of the padding (nz/2 <= m
+      // <= nzp - nz/2, nzp = N = 3 nz / 2) is not loaded (FP64 measured 1 %
+      // slower with it)
+      cfft_io<T, KB, N, 1, NT, 0, sizeof(T) == 4>([&](int m, int b) { return load_elem(f, m, b); },
                                [&](int m, int b, V v) {
                                  if (kx0 + b < g.nx2) out[(size_t)m * g.nx2 + kx0 + b] = v;
                                },
@@ -194,8 +196,9 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256,
   };
   V* res;
   if constexpr (N > 0) {
-    // the first inverse pass reads the spectra itself
-    res = cfft_ld<T, B, N, 1, NT>(herm, bA, bB, tw, threadIdx.x);
+    // the first inverse pass reads the spectra itself, except the zero band
+    // nx/2 <= k <= nxp - nx/2 of the padding (nxp = N = 3 nx / 2)
+    res = cfft_ld<T, B, N, 1, NT, true>(herm, bA, bB, tw, threadIdx.x);
   } else {
     for (int t = threadIdx.x; t < n * B; t += nthr) {
       const int k = t / B;
@@ -260,7 +263,9 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256,
   }
   double cmax = (double)cmaxt;
   __syncthreads();
-  V* fres = fft_any<T, B2, N, NT, -1>(oth, res, plan, tw);
+  // (the band nx/2 <= k <= nxp - nx/2 of the spectra, which the loop below
+  // never reads, is not written)
+  V* fres = fft_any<T, B2, N, NT, -1, true>(oth, res, plan, tw);
   for (int t = threadIdx.x; t < g.nx2 * RB; t += nthr) {
     const int k = t / RB;
     const int r = t - k * RB;
@@ -338,7 +343,7 @@ __global__ void __launch_bounds__(NT > 0 ? NT : 256,
       dst[iz * g.nx2 + kx] = typename C2<S>::type{(S)hx, (S)hy};
     };
     if constexpr (N > 0) {
-      cfft_io<T, KB, N, -1, NT>(
+      cfft_io<T, KB, N, -1, NT, 0, false, true>(
           [&](int m, int b) { return (kx0 + b < g.nx2) ? in[(size_t)m * g.nx2 + kx0 + b] : V{(T)0, (T)0}; },
           [&](int m, int b, V v) {
             // keep the nz stored modes (truncation folded into the store)
