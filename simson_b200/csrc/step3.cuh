@@ -187,9 +187,10 @@ SB_HD __forceinline__ double tau_rhs(const Col& f, int i, int n) {
 // fewer per solution; the same arithmetic in a different summation order.
 //
 // pre (optional): called at the top of backward row i as pre(i, fnew) and
-// returns in fnew[q] the right-hand side f(i-3) of every column (0-based
-// rows; the caller has produced rows n-1 and n-2 itself), so a right-hand
-// side assembled row by row never goes through memory; f[] is then unused.
+// returns in fnew[q] (type FS, the forcing's storage type) the right-hand
+// side f(i-3) of every column (0-based rows; the caller has produced rows n-1
+// and n-2 itself), so a right-hand side assembled row by row never goes
+// through memory; f[] is then unused.
 struct NoPre {};
 
 //
@@ -218,21 +219,24 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   S xa[M], xb[M];  // x computed 1 and 2 rows ago (x(i+1), x(i+2))
   S q1 = (S)0.0, q2 = (S)0.0;  // c' computed 1 and 2 rows ago: q2 = c'(i) at row i
   S w1 = (S)0.0, w2 = (S)0.0;  // W computed 1 and 2 rows ago: w2 = W(i+2) at row i
-  S bs_odd[M], bs_even[M], xn[M], xn1[M];  // FAST: boundary sums, x(n), x(n-1)
+  S bs_odd[M], bs_even[M];  // FAST: boundary sums
 #pragma unroll
-  for (int q = 0; q < M; ++q) xa[q] = xb[q] = bs_odd[q] = bs_even[q] = xn[q] = xn1[q] = (S)0.0;
+  for (int q = 0; q < M; ++q) xa[q] = xb[q] = bs_odd[q] = bs_even[q] = (S)0.0;
   // right-hand-side window: row i reads f(i-3), f(i-1), f(i+1) (0-based);
   // per row parity the last two stay in registers, so each row loads one
   // value per column (row i-2 reuses f(i-1) and f(i-3)). Used by the FP64
   // path and with pre; in the reordered (FAST) variant without pre the extra
-  // registers spill and the plain three loads are faster.
+  // registers spill and the plain three loads are faster.  The window holds
+  // the values in the forcing's storage type FS: they come from FS columns or
+  // from pre, which rounds them to FS, so this is exact (and halves the
+  // window's registers when FS is float).
   constexpr bool WIN = !FAST || HOOK;
-  S wlo0[M], whi0[M], wlo1[M], whi1[M];  // even / odd rows (selects keep them in registers)
+  FS wlo0[M], whi0[M], wlo1[M], whi1[M];  // even / odd rows (selects keep them in registers)
 #pragma unroll
-  for (int q = 0; q < M; ++q) wlo0[q] = wlo1[q] = whi0[q] = whi1[q] = (S)0.0;
+  for (int q = 0; q < M; ++q) wlo0[q] = wlo1[q] = whi0[q] = whi1[q] = (FS)0.0;
   for (int i = n; i >= 3; --i) {
     const int pr = i & 1;
-    S fh[M];
+    FS fh[M];
     if constexpr (HOOK) pre(i, fh);
     S dinv = (S)1.0, cnew = (S)0.0, wnew = (S)0.0;
     if (i <= n - 2) {
@@ -262,11 +266,11 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       if ((HOOK || fp[q] != nullptr) && WIN) {
         S fnew;  // f(i-3)
         if constexpr (HOOK)
-          fnew = fh[q];
+          fnew = (S)fh[q];
         else
           fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];
-        const S fm = pr ? wlo1[q] : wlo0[q];               // f(i-1)
-        const S fpl = pr ? whi1[q] : whi0[q];              // f(i+1)
+        const S fm = (S)(pr ? wlo1[q] : wlo0[q]);          // f(i-1)
+        const S fpl = (S)(pr ? whi1[q] : whi0[q]);         // f(i+1)
         if (i == 3) {
           r = (S)0.25 * fnew + fpl / (S)24.0 - fm / (S)6.0;
         } else {
@@ -275,11 +279,11 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
           if (i <= n - 4) r += cc * fpl;
         }
         if (pr) {
-          whi1[q] = fm;
-          wlo1[q] = fnew;
+          whi1[q] = (FS)fm;
+          wlo1[q] = (FS)fnew;
         } else {
-          whi0[q] = fm;
-          wlo0[q] = fnew;
+          whi0[q] = (FS)fm;
+          wlo0[q] = (FS)fnew;
         }
       } else if (fp[q] != nullptr) {
         const FS* __restrict__ F = fp[q];
@@ -298,8 +302,6 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
         r = r * dinv;
       xp[q][(size_t)(i - 1) * xs[q]] = r;
       if (FAST) {
-        if (i == n) xn[q] = r;
-        if (i == n - 1) xn1[q] = r;
         if (i <= n - 2) {
           if (i & 1)
             bs_odd[q] = bs_odd[q] + r * wnew;
@@ -328,8 +330,11 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     for (int q = 0; q < M; ++q) {
       S* __restrict__ X = xp[q];
       const size_t st = xs[q];
-      xa[q] = (bc1[q] - xn[q] - bs_odd[q]) * d1;   // x(1)
-      xb[q] = (bc2[q] - xn1[q] - bs_even[q]) * d2;  // x(2)
+      // x(n), x(n-1): the sweep's first two rows, read back from the column
+      // rather than held in registers through the sweep
+      const S xn = X[(size_t)(n - 1) * st], xn1 = X[(size_t)(n - 2) * st];
+      xa[q] = (bc1[q] - xn - bs_odd[q]) * d1;   // x(1)
+      xb[q] = (bc2[q] - xn1 - bs_even[q]) * d2;  // x(2)
       X[0] = xa[q];
       X[st] = xb[q];
     }
@@ -608,7 +613,7 @@ __global__ void __launch_bounds__(128, SB_PENCIL_MINB) k_pencil(PencilBufs B, Di
   // forcing never goes through memory.
   double2 g1 = double2{0.0, 0.0};                           // g_{j+1}
   double2 d1 = double2{0.0, 0.0}, d2 = double2{0.0, 0.0};  // dg_{j+1}, dg_{j+2}
-  auto assemble = [&](int j, SC* fr) {
+  auto assemble = [&](int j, FC* fr) {
     const size_t o = j * NP;
     if (j >= SB_PF_ROWS) {
       const size_t op = o - (size_t)SB_PF_ROWS * NP;
@@ -636,17 +641,17 @@ __global__ void __launch_bounds__(128, SB_PENCIL_MINB) k_pencil(PencilBufs B, Di
     const FC2 hvs = FC2{(FC)hv.x, (FC)hv.y};
     HV[o] = hvs;
     // f_v, f_omega rounded to the forcing storage type as when they were stored
-    fr[0] = (SC)(FC)(pv.x - c1 * hv.x);
-    fr[1] = (SC)(FC)(pv.y - c1 * hv.y);
-    fr[2] = (SC)(FC)(pw.x - c1 * hom.x);
-    fr[3] = (SC)(FC)(pw.y - c1 * hom.y);
+    fr[0] = (FC)(pv.x - c1 * hv.x);
+    fr[1] = (FC)(pv.y - c1 * hv.y);
+    fr[2] = (FC)(pw.x - c1 * hom.x);
+    fr[3] = (FC)(pw.y - c1 * hom.y);
   };
   // phi (particular) and omega_y: (D^2 - lam) psi = f  (linearbl.f:625-626)
   {
     auto cre = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p, 2 * NP}; };
     auto cim = [&](double2* arr) { return ColT<SC>{reinterpret_cast<SC*>(arr) + 2 * (size_t)p + 1, 2 * NP}; };
     // rows n-1 and n-2 first; the solve asks for row i-3 at its row i
-    SC fdummy[4];
+    FC fdummy[4];
     assemble(n - 1, fdummy);
     assemble(n - 2, fdummy);
     const ColT<FC> f[4] = {};
@@ -656,7 +661,7 @@ __global__ void __launch_bounds__(128, SB_PENCIL_MINB) k_pencil(PencilBufs B, Di
     const size_t fr = (size_t)n * NP;
     tau_solve<4, SC, FC, FAST, true>((SC)lam, n, f, x, bc0, bc0, ColT<SC>{reinterpret_cast<SC*>(CF) + p, NP},
                                      ColT<SC>{reinterpret_cast<SC*>(CF + fr) + p, NP}, nullptr,
-                                     [&](int i, SC* fo) { assemble(i - 3, fo); });
+                                     [&](int i, FC* fo) { assemble(i - 3, fo); });
     // v from phi: (D^2 - k^2) v = phi  (linearbl.f:1000-1001), FP64
     const ColT<SC> fv[2] = {cre(B.PHI), cim(B.PHI)};
     const Col xv[2] = {col_re(B.V, p, NP), col_im(B.V, p, NP)};
