@@ -489,7 +489,7 @@ def main():
     # from ncu captures of these kernels at this workload, summarised in
     # profiles/: the pencil kernel captured at 384x193x384 (one pass), the x
     # pass at 384x33x384 scaled by ny (its traffic grows with the planes)
-    measured_traffic = {("mixed", "pencil"): 2.64e9 + 2.53e9, ("mixed", "xpass"): (175.25e6 + 60.25e6) * 193 / 33}
+    measured_traffic = {("mixed", "pencil"): 2.65e9 + 2.51e9, ("mixed", "xpass"): (175.25e6 + 60.25e6) * 193 / 33}
     roof = {"kernel": dom, "bound": "hbm", "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
             "traffic": measured_traffic.get((head, dom)), "launch_ms": dom_ms}
     if dom_bytes:
