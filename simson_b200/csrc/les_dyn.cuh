@@ -548,9 +548,11 @@ __global__ void __launch_bounds__(128) k_sgs_sigma(const double2* __restrict__ t
   const int j0 = min(n, lane * per), j1 = min(n, j0 + per);
   // sigma_1 = i a tau11 + i b tau13 + D tau12; sigma_2 = i a tau12 + i b tau23
   // + D tau22; sigma_3 = i a tau13 + i b tau33 + D tau23
-  const int cx[3] = {0, 1, 2}, cz[3] = {2, 4, 5}, cy[3] = {1, 3, 4};
+  // tau slots: i a tau_(i,1), i b tau_(i,3), D tau_(i,2) of row i (selects,
+  // so no index table goes to local memory)
   for (int i = 0; i < 3; ++i) {
-    const double2* ty = tc + (size_t)cy[i] * fld + p;
+    const int cx = i, cy = (i == 0) ? 1 : (i == 1 ? 3 : 4), cz = (i == 0) ? 2 : (i == 1 ? 4 : 5);
+    const double2* ty = tc + (size_t)cy * fld + p;
     // this lane's block sums of 2 k a_k, k even / k odd
     double2 se{0.0, 0.0}, so{0.0, 0.0};
     for (int k = j0; k < j1; ++k) {
@@ -582,8 +584,8 @@ __global__ void __launch_bounds__(128) k_sgs_sigma(const double2* __restrict__ t
       const double2 v = ty[(size_t)j * G.NP];
       double2 d = (j & 1) ? Se : So;  // k > j of the other parity
       if (j == 0) d = double2{0.5 * d.x, 0.5 * d.y};
-      const double2 tx = tc[(size_t)cx[i] * fld + o];
-      const double2 tz = tc[(size_t)cz[i] * fld + o];
+      const double2 tx = tc[(size_t)cx * fld + o];
+      const double2 tz = tc[(size_t)cz * fld + o];
       sc[(size_t)i * fld + o] = double2{-a * tx.y - b * tz.y + d.x, a * tx.x + b * tz.x + d.y};
       const double f = 2.0 * (double)j;
       if (j & 1) {

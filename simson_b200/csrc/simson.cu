@@ -1578,6 +1578,8 @@ static int xys_setup(sgpu_ctx* c) {
   cudaFuncSetAttribute(k_xys_zinv<float2, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
   cudaFuncSetAttribute(k_xys_acc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
   cudaFuncSetAttribute(k_xys_acc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  cudaFuncSetAttribute(k_xys_acc<false, 384>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+  cudaFuncSetAttribute(k_xys_acc<true, 384>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
   cudaFuncSetAttribute(k_box_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
   return SGPU_OK;
 }
@@ -1642,12 +1644,21 @@ extern "C" int sgpu_xys_sample(sgpu_ctx* c, double dtn) {
   const bool pres = c->press_valid && c->press;
   xys_fields(c, pres ? c->press : nullptr);
   const int nt = (g.nx + 31) / 32 * 32;
-  if (pres)
-    k_xys_acc<true><<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
-                                                                    c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
+  const dim3 gr(XYS_GROUPS, g.nyp);
+  const double cw = dtn / (double)g.nz;
+  // the 384-thread instances (more registers per thread) whenever nx fits
+  if (pres && nt <= 384)
+    k_xys_acc<true, 384><<<gr, nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G, c->xys_twx.plan,
+                                                    c->xys_twx.d, cw);
+  else if (pres)
+    k_xys_acc<true><<<gr, nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G, c->xys_twx.plan, c->xys_twx.d,
+                                               cw);
+  else if (nt <= 384)
+    k_xys_acc<false, 384><<<gr, nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G, c->xys_twx.plan,
+                                                     c->xys_twx.d, cw);
   else
-    k_xys_acc<false><<<dim3(XYS_GROUPS, g.nyp), nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G,
-                                                                     c->xys_twx.plan, c->xys_twx.d, dtn / (double)g.nz);
+    k_xys_acc<false><<<gr, nt, sx, c->stream>>>(c->xys_spec, c->xys_part, c->xys_u, G, c->xys_twx.plan, c->xys_twx.d,
+                                                cw);
   const size_t plane = (size_t)g.nyp * g.nx;
   const int nb = (int)((plane + 255) / 256);
   k_xys_add<<<nb, 256, 0, c->stream>>>(c->xys_part, c->xys, G, pres ? XYS_NACC_P : XYS_NACC);

@@ -105,12 +105,16 @@ __global__ void k_xys_zinv(const V* __restrict__ st, const double2* __restrict__
   }
 }
 
-// blockDim.x >= nx (nx <= 512); thread j owns x = j.  part: [XYS_GROUPS][XYS_NACC_P][nyp][nx];
+// blockDim.x >= nx (nx <= MAXT <= 512); thread j owns x = j.  part: [XYS_GROUPS][XYS_NACC_P][nyp][nx];
 // PRES: the pressure entries too (field 15 holds p).
 // uphys: [nyp][nz][nx].  c = dtn / nz, the weight of one point
 // (boxxys.f:556, nfzsym = 0).
-template <bool PRES>
-__global__ void __launch_bounds__(512) k_xys_acc(const double2* __restrict__ spec, double* __restrict__ part,
+// MAXT: the block size the register budget is sized for.  The accumulators
+// stay in registers across the z rows: at 512 threads (128 registers) 512
+// bytes of them spill (240 without the pressure entries), at 384 threads
+// (168 registers, grids with nx <= 384) 160 bytes (16).
+template <bool PRES, int MAXT = 512>
+__global__ void __launch_bounds__(MAXT) k_xys_acc(const double2* __restrict__ spec, double* __restrict__ part,
                                                   double* __restrict__ uphys, SgsGrid G, FFTPlan plan,
                                                   const double2* __restrict__ tw, double c) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
