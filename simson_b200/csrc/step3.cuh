@@ -344,16 +344,29 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       ds0[q] = xb[q];  // k = 1 (odd): 1^2 x_1
       ds1[q] = (S)0.0;
     }
+    // row i's inputs are loaded during row i-1, before its stores (which
+    // the compiler cannot move them past): the loads overlap a row's work
+    S cn = cpp[0], xnx[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) xnx[q] = xp[q][2 * xs[q]];
 #pragma unroll 4
     for (int i = 3; i <= n; ++i) {
       if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(cpp + (size_t)(i - 3 + SB_PF_ROWS) * cs);
-      const S c = cpp[(size_t)(i - 3) * cs];
+      const S c = cn;
+      S xc[M];
+#pragma unroll
+      for (int q = 0; q < M; ++q) xc[q] = xnx[q];
+      if (i < n) {
+        cn = cpp[(size_t)(i - 2) * cs];
+#pragma unroll
+        for (int q = 0; q < M; ++q) xnx[q] = xp[q][(size_t)i * xs[q]];
+      }
       const S kk = (S)(i - 1) * (S)(i - 1);
 #pragma unroll
       for (int q = 0; q < M; ++q) {
         const size_t o = (size_t)(i - 1) * xs[q];
         if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(xp[q] + o + (size_t)SB_PF_ROWS * xs[q]);
-        const S v = xp[q][o] - c * xa[q];
+        const S v = xc[q] - c * xa[q];
         xp[q][o] = v;
         xa[q] = xb[q];
         xb[q] = v;
@@ -389,15 +402,27 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
     X[0] = xa[q];
     X[st] = xb[q];
   }
+  // row i's inputs loaded during row i-1, as in the reordered variant
+  S cn = cpp[0], xnx[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) xnx[q] = xp[q][2 * xs[q]];
 #pragma unroll 4
   for (int i = 3; i <= n; ++i) {
     if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(cpp + (size_t)(i - 3 + SB_PF_ROWS) * cs);
-    const S c = cpp[(size_t)(i - 3) * cs];
+    const S c = cn;
+    S xc[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) xc[q] = xnx[q];
+    if (i < n) {
+      cn = cpp[(size_t)(i - 2) * cs];
+#pragma unroll
+      for (int q = 0; q < M; ++q) xnx[q] = xp[q][(size_t)i * xs[q]];
+    }
 #pragma unroll
     for (int q = 0; q < M; ++q) {
       const size_t o = (size_t)(i - 1) * xs[q];
       if (i - 1 + SB_PF_ROWS <= n - 1) pf_l2(xp[q] + o + (size_t)SB_PF_ROWS * xs[q]);
-      const S v = xp[q][o] - c * xa[q];
+      const S v = xc[q] - c * xa[q];
       xp[q][o] = v;
       xa[q] = xb[q];
       xb[q] = v;
