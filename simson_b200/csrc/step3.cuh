@@ -225,15 +225,25 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
   // right-hand-side window: row i reads f(i-3), f(i-1), f(i+1) (0-based);
   // per row parity the last two stay in registers, so each row loads one
   // value per column (row i-2 reuses f(i-1) and f(i-3)). Used by the FP64
-  // path and with pre; in the reordered (FAST) variant without pre the extra
-  // registers spill and the plain three loads are faster.  The window holds
+  // path, with pre and (SB_TAU_WIN_ALL) in the reordered (FAST) variant: one
+  // load per row instead of three (mixed pencil kernel 1.02 -> 1.005 ms, no
+  // spill at its 128-register cap).  The window holds
   // the values in the forcing's storage type FS: they come from FS columns or
   // from pre, which rounds them to FS, so this is exact (and halves the
   // window's registers when FS is float).
-  constexpr bool WIN = !FAST || HOOK;
+#ifndef SB_TAU_WIN_ALL
+#define SB_TAU_WIN_ALL 1
+#endif
+  constexpr bool WIN = !FAST || HOOK || SB_TAU_WIN_ALL;
   FS wlo0[M], whi0[M], wlo1[M], whi1[M];  // even / odd rows (selects keep them in registers)
 #pragma unroll
   for (int q = 0; q < M; ++q) wlo0[q] = wlo1[q] = whi0[q] = whi1[q] = (FS)0.0;
+  // FAST: f(i-3) of the window read one row early, before the row's stores
+  // (the FP64 order keeps the plain load: one more live value spills there)
+  constexpr bool EARLY = FAST && !HOOK;
+  FS fpre[M];
+#pragma unroll
+  for (int q = 0; q < M; ++q) fpre[q] = (EARLY && fp[q] != nullptr) ? fp[q][(size_t)(n - 3) * fs[q]] : (FS)0.0;
   for (int i = n; i >= 3; --i) {
     const int pr = i & 1;
     FS fh[M];
@@ -265,10 +275,14 @@ SB_HD void tau_solve(S lam, int n, const ColT<FS>* f, const ColT<S>* x, const S*
       if (fp[q] != nullptr && i - 3 - SB_PF_ROWS >= 0) pf_l2(fp[q] + (size_t)(i - 3 - SB_PF_ROWS) * fs[q]);
       if ((HOOK || fp[q] != nullptr) && WIN) {
         S fnew;  // f(i-3)
-        if constexpr (HOOK)
+        if constexpr (HOOK) {
           fnew = (S)fh[q];
-        else
+        } else if constexpr (EARLY) {
+          fnew = (S)fpre[q];
+          if (i >= 4) fpre[q] = fp[q][(size_t)(i - 4) * fs[q]];
+        } else {
           fnew = (S)fp[q][(size_t)(i - 3) * fs[q]];
+        }
         const S fm = (S)(pr ? wlo1[q] : wlo0[q]);          // f(i-1)
         const S fpl = (S)(pr ? whi1[q] : whi0[q]);         // f(i+1)
         if (i == 3) {
