@@ -252,12 +252,20 @@ SB_HD __forceinline__ unsigned umulhi_(unsigned a, unsigned b) {
 }
 
 // v[r] *= w^(r e), w = exp(S 2 pi i / n), from the table tw[m] = exp(-2 pi i m / n).
+// Twiddle powers w^r, r = 1..R-1: two table loads (w, w^2) and products of
+// depth <= 2 for the rest (a few ulp), in FP32 and, with SB_TW_PRODUCTS64, in
+// FP64 too: the FP64 transforms were stalled on the R - 1 table loads per
+// butterfly (x pass 2.25 -> 1.91 ms, z-inverse 1.02 -> 0.96, z-forward 0.55 ->
+// 0.51 at 384x193x384; the parity gates against the reference unchanged)
+#ifndef SB_TW_PRODUCTS64
+#define SB_TW_PRODUCTS64 1
+#endif
 template <class T, int R, int S>
 SB_HD __forceinline__ void twiddle(typename C2<T>::type* v, const typename C2<T>::type* __restrict__ tw, int e) {
   typedef typename C2<T>::type V;
-  if constexpr (std::is_same<T, float>::value) {
-    // FP32: two table loads, the other powers by products of depth <= 2
-    // (w^k for k <= 8 from w, w^2: a few ulp), fewer load-pipe requests
+  if constexpr (std::is_same<T, float>::value || SB_TW_PRODUCTS64) {
+    // two table loads, the other powers by products of depth <= 2 (w^k for
+    // k <= 8 from w, w^2: a few ulp), fewer load-pipe requests
     V w[9];
     w[1] = tw[e];
     w[2] = tw[2 * e];
